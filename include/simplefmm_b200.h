@@ -1,0 +1,136 @@
+/*
+ * simplefmm_b200 -- C ABI of the B200 (sm_100a) 3D Laplace FMM.
+ *
+ * The reference library (SimpleFMM) is header-only C++ templates; its
+ * evaluation path is the sequence
+ *     Box(positions, vertical_axis, phideg)                 box.hpp:84-107
+ *     OctreePartitioner(positions, box).refine(L, ppn)       partition.hpp:397-446
+ *     FMM3D<double, N, p, Vector, grad>(partitioner, comm)   fmm.hpp:204-427
+ *     fmm.rinv(Q, U) / fmm.rinv<true>(Q, U)                  fmm.hpp:864-881
+ * Each entry point below replaces one step of that sequence (cited per
+ * function).  Arguments are plain pointers and sizes; no C++ or CUDA types
+ * cross the boundary (a cudaStream_t is passed as void*).
+ *
+ * Conventions
+ *  - Every function returns an fmm_status (0 = FMM_OK).  fmm_last_error()
+ *    returns a message for the calling thread's last failure.
+ *  - Positions are n x 3 doubles, row-major (x0 y0 z0 x1 ...), exactly the
+ *    memory of the reference's std::vector<Vector<double,3>>.
+ *  - Charges Q are n x qdim doubles (the reference's Vector<double,N>*);
+ *    outputs are accumulated (U += ...), as the reference's rinv does.
+ *  - `where` says whether pointers are host (FMM_HOST) or device
+ *    (FMM_DEVICE) memory.
+ *  - The library keeps the tree, lists and expansions resident on the
+ *    device; one context = one device + one stream.  Calls on one context
+ *    are not re-entrant (like the reference's mutable _M/_L, fmm.hpp:178-179).
+ */
+#ifndef SIMPLEFMM_B200_H
+#define SIMPLEFMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum fmm_status {
+    FMM_OK = 0,
+    FMM_ERR_INVALID_ARGUMENT = 1,
+    FMM_ERR_UNSUPPORTED = 2,
+    FMM_ERR_CUDA = 3,
+    FMM_ERR_OUT_OF_MEMORY = 4,
+    /* All points share the vertical coordinate: the reference's Box loops
+       forever doubling a zero width (box.hpp:101-105); rejected here. */
+    FMM_ERR_DEGENERATE_INPUT = 5,
+    FMM_ERR_OVER_BUDGET = 6,
+    FMM_ERR_TIMEOUT = 7
+} fmm_status;
+
+enum { FMM_HOST = 0, FMM_DEVICE = 1 };
+
+/* Plan precision: FP64 throughout (matches the reference to 1e-12), or the
+   mixed-precision form. */
+enum { FMM_PRECISION_FP64 = 0, FMM_PRECISION_MIXED = 1 };
+
+/* Tree export selectors for fmm_tree_export (one level at a time). */
+enum {
+    FMM_EXPORT_NODE_KEYS = 0,   /* int64[n_node]  OctreeLevel::_c_node      partition.hpp:158 */
+    FMM_EXPORT_LEAF_NODES = 1,  /* int32[n_leaf]  OctreeLevel::_i_leaf      partition.hpp:159 */
+    FMM_EXPORT_INDEX_PTR = 2,   /* int32[n_leaf+1] _indices row pointers    partition.hpp:160 */
+    FMM_EXPORT_INDEX = 3,       /* int32[nnz]     _indices (original ids)  */
+    FMM_EXPORT_ILIST_PTR = 4,   /* int32[n_node+1] _ilist rows (level>=2)   partition.hpp:283-297 */
+    FMM_EXPORT_ILIST = 5,       /* int32[4*nnz]   (src node, di, dj, dk)   */
+    FMM_EXPORT_CLIST_PTR = 6,   /* int32[n_node+1] _clist rows (level<depth) partition.hpp:299-313 */
+    FMM_EXPORT_CLIST = 7,       /* int64[2*nnz]   (child node, child key)  */
+    FMM_EXPORT_PLIST = 8,       /* int64[2*n_node] (parent node, own key), level>=1  partition.hpp:315-322 */
+    FMM_EXPORT_NLIST_PTR = 9,   /* int32[n_leaf+1] _nlist rows              partition.hpp:343-366 */
+    FMM_EXPORT_NLIST = 10,      /* int32[2*nnz]   (level, leaf)            */
+    FMM_EXPORT_PARTITIONS = 11  /* int32[2*n]     point -> (level, leaf)   partition.hpp:436-445 */
+};
+
+typedef struct fmm_context fmm_context;
+typedef struct fmm_tree fmm_tree;
+typedef struct fmm_plan fmm_plan;
+
+const char* fmm_status_string(int status);
+const char* fmm_last_error(void);
+/* Library version, e.g. "0.1.0". */
+const char* fmm_version(void);
+
+/* Create a context on `device` with its own stream. */
+int fmm_context_create(int device, fmm_context** out);
+int fmm_context_destroy(fmm_context* ctx);
+/* Use the caller's stream (a cudaStream_t) for all work of this context. */
+int fmm_context_set_stream(fmm_context* ctx, void* stream);
+int fmm_context_synchronize(fmm_context* ctx);
+/* Page-lock host memory so host<->device copies run at full speed. */
+int fmm_host_register(void* ptr, size_t bytes);
+int fmm_host_unregister(void* ptr);
+
+/* Box(positions, vertical_axis, phideg) + OctreePartitioner::refine(max_level,
+   max_particles_per_node): box.hpp:84-107, partition.hpp:397-446.  The tree
+   (nodes, leaf point lists, interaction/neighbour lists) is built on the
+   device and stays resident.  max_level is clamped to 20 (box.hpp:26).
+   The tree copies the positions it needs; the caller's array may be freed. */
+int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level,
+                   int max_particles_per_node, int vertical_axis, double phideg, fmm_tree** out);
+int fmm_tree_destroy(fmm_tree* tree);
+/* Deepest level (OctreePartitioner::level(), partition.hpp:463-466). */
+int fmm_tree_depth(const fmm_tree* tree, int* depth);
+/* Box::width() and Box::corner() (box.hpp:109-117). */
+int fmm_tree_box(const fmm_tree* tree, double* width, double* corner3);
+/* Element count of an export (see FMM_EXPORT_*), or -1 if not defined at this level. */
+int fmm_tree_export_size(const fmm_tree* tree, int level, int what, int64_t* count);
+/* Copy one export to host memory sized by fmm_tree_export_size. */
+int fmm_tree_export(const fmm_tree* tree, int level, int what, void* host_out);
+/* Total element counts of the device lists: [0] nodes, [1] leaves, [2] ilist
+   pairs, [3] near-field point pairs (self excluded), [4] near-field ranges. */
+int fmm_tree_stats(const fmm_tree* tree, int64_t* stats5);
+
+/* FMM3D<double, qdim, p, Vector, support_gradient>(partitioner, comm):
+   fmm.hpp:204-427.  Builds the operator tables for order p (0..16) and
+   allocates device expansions.  qdim is the number of charge components N. */
+int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** out);
+int fmm_plan_destroy(fmm_plan* plan);
+
+/* fmm.rinv(Q, U) (gradient = 0) or fmm.rinv<true>(Q, U) (gradient = 1,
+   qdim must be 3): fmm.hpp:864-881.  U (n x qdim, or n x 3) is accumulated. */
+int fmm_rinv(fmm_plan* plan, const double* Q, double* U, int gradient, int where);
+
+/* One pass computing any of: pot (n x qdim) += sum_j Q_j/|x_i-x_j|, and
+   field (n x 3) += sum_j q_j R/|R|^3 for qdim = 1, or sum_j Q_j x R/|R|^3 for
+   qdim = 3 (the reference's rinv<true>).  NULL skips an output.  Both are
+   accumulated.  The far field of the field uses source-gradient moments, the
+   formulation of fmm.hpp:234-253 and 549-551. */
+int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, int where);
+
+/* Device time (ms) of each phase of the last evaluation: [0] P2M+M2M,
+   [1] M2L, [2] L2L+L2P, [3] P2P, [4] total; and of the last tree build [5]. */
+int fmm_plan_timings(const fmm_plan* plan, double* ms6);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,198 @@
+// Internal declarations of the B200 FMM library (not part of the C ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "fmm_ops.cuh"
+#include "simplefmm_b200.h"
+
+namespace sfmm {
+
+// ------------------------------------------------------------------ errors
+struct Error : std::runtime_error {
+    int status;
+    Error(int s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+
+#define SFMM_CUDA(x)                                                     \
+    do {                                                                 \
+        cudaError_t e_ = (x);                                            \
+        if (e_ != cudaSuccess) ::sfmm::throw_cuda(e_, #x, __FILE__, __LINE__); \
+    } while (0)
+
+#define SFMM_CHECK_LAUNCH() SFMM_CUDA(cudaGetLastError())
+
+#define SFMM_REQUIRE(cond, status, msg)                 \
+    do {                                                \
+        if (!(cond)) throw ::sfmm::Error((status), (msg)); \
+    } while (0)
+
+// ------------------------------------------------------------------ device memory
+// Stream-ordered device allocation (cudaMallocAsync from the device pool,
+// whose release threshold is raised at context creation so repeated
+// evaluations reuse memory instead of returning it to the driver).
+template<typename T>
+struct DevBuf {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaStream_t stream = nullptr;
+
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) { o.ptr = nullptr; o.count = 0; }
+    DevBuf& operator=(DevBuf&& o) noexcept
+    {
+        if (this != &o) {
+            release();
+            ptr = o.ptr; count = o.count; stream = o.stream;
+            o.ptr = nullptr; o.count = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+
+    void alloc(size_t n, cudaStream_t s)
+    {
+        release();
+        stream = s;
+        count = n;
+        if (n) {
+            cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s);
+            if (e == cudaErrorMemoryAllocation) {
+                (void)cudaGetLastError();
+                ptr = nullptr;
+                count = 0;
+                throw Error(FMM_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed");
+            }
+            SFMM_CUDA(e);
+        }
+    }
+    // grow keeping the first `keep` elements
+    void grow(size_t n, size_t keep, cudaStream_t s)
+    {
+        if (n <= count) return;
+        DevBuf<T> nb;
+        nb.alloc(n, s);
+        if (keep && ptr) SFMM_CUDA(cudaMemcpyAsync(nb.ptr, ptr, keep * sizeof(T), cudaMemcpyDeviceToDevice, s));
+        *this = std::move(nb);
+    }
+    void release() noexcept
+    {
+        if (ptr) cudaFreeAsync(ptr, stream);
+        ptr = nullptr;
+        count = 0;
+    }
+    size_t bytes() const { return count * sizeof(T); }
+};
+
+constexpr int kKeyLevel = 20;             // box.hpp:26 -- deepest keyed level
+
+// Root cube (box.hpp:24-31, 84-107) as used on the device.
+struct BoxDev {
+    double width;
+    double corner[3];
+    double cphi, sphi;                    // cos / sin of the rotation about the vertical axis
+    int X, Y, Z;                          // axis permutation (box.hpp:74-76)
+    int rotated;                          // phideg != 0
+    int status;                           // FMM_OK or FMM_ERR_DEGENERATE_INPUT
+};
+
+// rotate(v) of box.hpp:152-157, without contraction so the rounding is the
+// plain product/sum sequence of the source.
+__host__ __device__ inline void box_rotate(const BoxDev& b, const double* v, double* r)
+{
+    if (!b.rotated) {
+        r[0] = v[b.X];
+        r[1] = v[b.Y];
+        r[2] = v[b.Z];
+        return;
+    }
+#ifdef __CUDA_ARCH__
+    r[0] = __dsub_rn(__dmul_rn(b.cphi, v[b.X]), __dmul_rn(b.sphi, v[b.Y]));
+    r[1] = __dadd_rn(__dmul_rn(b.sphi, v[b.X]), __dmul_rn(b.cphi, v[b.Y]));
+#else
+    r[0] = b.cphi * v[b.X] - b.sphi * v[b.Y];
+    r[1] = b.sphi * v[b.X] + b.cphi * v[b.Y];
+#endif
+    r[2] = v[b.Z];
+}
+
+// ------------------------------------------------------------------ objects
+struct Context {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+};
+
+// Device-resident octree: nodes of all levels concatenated level by level
+// (within a level in key order, the reference's _c_node order), points in
+// leaf order (leaves in Morton order, each leaf's points by ascending
+// original index -- the order OctreeNode::subdivide leaves them in).
+struct Tree {
+    Context* ctx = nullptr;
+    int64_t n = 0;
+    int depth = 0;
+    int max_level = 20, max_ppn = 64, vertical_axis = 2;
+    double phideg = 0;
+    BoxDev box{};                         // host copy
+    DevBuf<BoxDev> d_box;
+
+    std::vector<int64_t> lvl_off;         // node offset per level (depth + 2)
+    std::vector<int64_t> leaf_off;        // leaf offset per level (depth + 2)
+    int64_t n_nodes = 0, n_leaves = 0;
+
+    // points (sorted order)
+    DevBuf<int32_t> order;                // sorted position -> original index
+    DevBuf<double> pts;                   // 3 x n SoA: x | y | z, original frame (near field)
+    DevBuf<double> rpts;                  // 3 x n SoA rotated frame, only when box.rotated
+    const double* far_x = nullptr;        // rotated-frame coordinates used by the far field
+    const double* far_y = nullptr;
+    const double* far_z = nullptr;
+
+    // nodes
+    DevBuf<uint64_t> key;
+    DevBuf<int32_t> pbeg, pend, parent, child_beg, nchild, leaf_id;
+    DevBuf<int32_t> leaf_node;            // global leaf id -> global node id
+    DevBuf<int32_t> colleague;            // 27 per node: same-level neighbours (tree.hpp:66-119)
+
+    // interaction list (partition.hpp:283-297), rows = all nodes, sorted by source
+    DevBuf<int32_t> il_ptr, il_src, il_code;
+    int64_t il_nnz = 0;
+
+    // near-field source point ranges per leaf (the point sets of _nlist rows)
+    DevBuf<int32_t> nr_ptr;
+    DevBuf<int2> nr;
+    int64_t nr_nnz = 0;
+    int64_t near_pairs = 0;
+
+    float build_ms = 0;
+};
+
+struct Plan;
+
+// tree.cu
+void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg);
+int64_t tree_export(const Tree& t, int level, int what, void* host_out);
+
+// scan.cu
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+
+inline unsigned blocks_for(int64_t n, int threads, int64_t cap = 1 << 20)
+{
+    int64_t b = (n + threads - 1) / threads;
+    if (b < 1) b = 1;
+    if (b > cap) b = cap;
+    return static_cast<unsigned>(b);
+}
+
+}  // namespace sfmm

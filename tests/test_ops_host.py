@@ -1,0 +1,103 @@
+"""CPU check of the device operator math.
+
+tests/native/emu.cpp runs the library's m >= 0 formulation (fmm_ops.cuh +
+tables.cpp -- the code the kernels execute) serially over the oracle's tree;
+its potential and field must agree with the reference (golden fixtures) to the
+same 1e-12 per-target bar the GPU path is held to.  This isolates the math
+from the GPU parallelisation."""
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import load_golden, rel_err_per_target
+from oracle import pyoracle
+from simplefmm_b200 import workloads as W
+
+ROOT = Path(__file__).resolve().parents[1]
+CSRC = ROOT / "simplefmm_b200" / "csrc"
+
+
+@pytest.fixture(scope="module")
+def emu(tmp_path_factory):
+    out = tmp_path_factory.mktemp("emu") / "libemu.so"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", f"-I{CSRC}", str(ROOT / "tests/native/emu.cpp"),
+                    str(CSRC / "tables.cpp"), "-o", str(out)], check=True)
+    lib = C.CDLL(str(out))
+    lib.emu_fmm.restype = C.c_int
+    return lib
+
+
+def run_emu(lib, dump, pos, Q, p, va=2, phideg=0.0, want_pot=True, want_field=True):
+    depth = int(dump["DEPTH"][0])
+    keep = []
+
+    def arr(key, dtype, l):
+        a = np.ascontiguousarray(dump.get(f"{key}{l}", np.zeros(1, dtype)), dtype=dtype)
+        if a.size == 0:
+            a = np.zeros(1, dtype)
+        keep.append(a)
+        return a.ctypes.data_as(C.c_void_p)
+
+    def ptrs(key, dtype):
+        return (C.c_void_p * (depth + 1))(*[arr(key, dtype, l) for l in range(depth + 1)])
+
+    nnode = np.array([dump[f"CNODE{l}"].size for l in range(depth + 1)], np.int64)
+    nleaf = np.array([dump[f"ILEAF{l}"].size for l in range(depth + 1)], np.int64)
+    pos = np.ascontiguousarray(pos, np.float64)
+    Q = np.ascontiguousarray(Q, np.float64)
+    qdim = 1 if Q.ndim == 1 else Q.shape[1]
+    pot = np.zeros((pos.shape[0], qdim)) if qdim > 1 else np.zeros(pos.shape[0])
+    field = np.zeros((pos.shape[0], 3))
+    box = np.ascontiguousarray(dump["BOX"], np.float64)
+    dp = lambda a: a.ctypes.data_as(C.POINTER(C.c_double))  # noqa: E731
+    rc = lib.emu_fmm(depth, nnode.ctypes.data_as(C.c_void_p), nleaf.ctypes.data_as(C.c_void_p),
+                     ptrs("CNODE", np.int64), ptrs("ILEAF", np.int32), ptrs("IDXP", np.int32), ptrs("IDXV", np.int32),
+                     ptrs("ILP", np.int32), ptrs("ILV", np.int32), ptrs("CLP", np.int32), ptrs("CLV", np.int64),
+                     ptrs("PL", np.int64), ptrs("NLP", np.int32), ptrs("NLV", np.int32), dp(box), va,
+                     C.c_double(phideg), dp(pos), C.c_int64(pos.shape[0]), p, qdim, int(want_pot), int(want_field),
+                     dp(Q), dp(pot), dp(field))
+    assert rc == 0
+    return pot, field
+
+
+@pytest.mark.parametrize("name", ["uniform_n3000_p6", "plummer_n6000_p5_ppn32", "gauss2_n4000_p8",
+                                  "uniform_n2500_p10_maxlevel3", "shell_n4000_p4_ppn16", "uniform_n400_p4_depth1"])
+def test_emulated_math_matches_reference(emu, name):
+    g = load_golden(name)
+    t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"])
+    sp, sf = pyoracle.error_scales(g["pos"], g["q"])
+    assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
+    assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
+
+
+def test_emulated_vector_charges(emu):
+    g = load_golden("vector_n2000_p8_ppn128")
+    t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"])
+    sp, sf = pyoracle.error_scales(g["pos"], g["q"])
+    assert rel_err_per_target(pot, g["VECPOT"], sp) < 1e-12
+    assert rel_err_per_target(field, g["BIOT"], sf) < 1e-12
+
+
+@pytest.mark.parametrize("va,phideg", [(0, 0.0), (1, 0.0), (2, 30.0)])
+def test_emulated_box_frames(emu, va, phideg):
+    pos = W.plummer(2500, 31)
+    q = W.charges(2500, 31)
+    t = pyoracle.Tree(pos, 20, 32, va, phideg)
+    pot, _ = run_emu(emu, t.dump(), pos, q, 6, va, phideg, want_field=False)
+    ref = t.rinv(6, q)
+    sp, _ = pyoracle.error_scales(pos, q)
+    assert rel_err_per_target(pot, ref, sp) < 1e-12
+
+
+def test_emulated_p12_against_direct(emu):
+    g = load_golden("uniform_n3000_p12")
+    t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], 12)
+    sp, sf = pyoracle.error_scales(g["pos"], g["q"])
+    assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
+    assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
