@@ -129,6 +129,16 @@ int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, in
    [1] M2L, [2] L2L+L2P, [3] P2P, [4] total; and of the last tree build [5]. */
 int fmm_plan_timings(const fmm_plan* plan, double* ms6);
 
+/* Direct O(n * nt) FP64 sums at nt target indices (the reference's own
+   accuracy check, main.cpp:70-111): pot (nt x qdim) = sum_{j != i} Q_j/|R|,
+   field (nt x 3) = sum_j q_j R/|R|^3 (qdim 1) or sum_j Q_j x R/|R|^3 (qdim 3).
+   Outputs are overwritten.  Synchronous. */
+int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
+               int64_t nt, double* pot, double* field, int where);
+
+/* Number of kernels this library has launched in this process. */
+int fmm_launch_count(int64_t* count);
+
 #ifdef __cplusplus
 }
 #endif

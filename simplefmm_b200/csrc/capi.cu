@@ -1,0 +1,364 @@
+// C ABI of the library (include/simplefmm_b200.h).  Every entry point
+// converts exceptions to an fmm_status and records a per-thread message.
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "fmm_eval.cuh"
+
+namespace sfmm {
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line)
+{
+    const int st = e == cudaErrorMemoryAllocation ? FMM_ERR_OUT_OF_MEMORY : FMM_ERR_CUDA;
+    throw Error(st, std::string(cudaGetErrorString(e)) + " in " + what + " (" + file + ":" + std::to_string(line) + ")");
+}
+
+}  // namespace sfmm
+
+struct fmm_context {
+    sfmm::Context c;
+};
+
+struct fmm_tree {
+    sfmm::Tree t;
+};
+
+struct fmm_plan {
+    sfmm::Plan pl;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int status, const std::string& msg)
+{
+    g_last_error = msg;
+    return status;
+}
+
+#define API_TRY try {
+#define API_CATCH                                                              \
+    }                                                                          \
+    catch (const sfmm::Error& e) { return fail(e.status, e.what()); }          \
+    catch (const std::bad_alloc&) { return fail(FMM_ERR_OUT_OF_MEMORY, "host allocation failed"); } \
+    catch (const std::exception& e) { return fail(FMM_ERR_CUDA, e.what()); }   \
+    return FMM_OK;
+
+void bind(const sfmm::Context& c) { SFMM_CUDA(cudaSetDevice(c.device)); }
+
+}  // namespace
+
+extern "C" {
+
+const char* fmm_status_string(int s)
+{
+    switch (s) {
+    case FMM_OK: return "ok";
+    case FMM_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case FMM_ERR_UNSUPPORTED: return "unsupported";
+    case FMM_ERR_CUDA: return "CUDA error";
+    case FMM_ERR_OUT_OF_MEMORY: return "out of memory";
+    case FMM_ERR_DEGENERATE_INPUT: return "degenerate input";
+    case FMM_ERR_OVER_BUDGET: return "over memory budget";
+    case FMM_ERR_TIMEOUT: return "timeout";
+    default: return "unknown status";
+    }
+}
+
+const char* fmm_last_error(void) { return g_last_error.c_str(); }
+
+const char* fmm_version(void) { return "0.1.0"; }
+
+int fmm_context_create(int device, fmm_context** out)
+{
+    API_TRY
+    if (!out) return fail(FMM_ERR_INVALID_ARGUMENT, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    SFMM_CUDA(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return fail(FMM_ERR_INVALID_ARGUMENT, "no such device");
+    auto* ctx = new fmm_context;
+    ctx->c.device = device;
+    try {
+        SFMM_CUDA(cudaSetDevice(device));
+        SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
+        ctx->c.own_stream = true;
+        SFMM_CUDA(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
+        cudaMemPool_t pool;
+        SFMM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
+        uint64_t thr = UINT64_MAX;
+        SFMM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    } catch (...) {
+        if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+        delete ctx;
+        throw;
+    }
+    *out = ctx;
+    API_CATCH
+}
+
+int fmm_context_destroy(fmm_context* ctx)
+{
+    API_TRY
+    if (!ctx) return FMM_OK;
+    bind(ctx->c);
+    SFMM_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    API_CATCH
+}
+
+int fmm_context_set_stream(fmm_context* ctx, void* stream)
+{
+    API_TRY
+    if (!ctx) return fail(FMM_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    bind(ctx->c);
+    SFMM_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+    ctx->c.stream = static_cast<cudaStream_t>(stream);
+    ctx->c.own_stream = false;
+    API_CATCH
+}
+
+int fmm_context_synchronize(fmm_context* ctx)
+{
+    API_TRY
+    if (!ctx) return fail(FMM_ERR_INVALID_ARGUMENT, "ctx is NULL");
+    bind(ctx->c);
+    SFMM_CUDA(cudaStreamSynchronize(ctx->c.stream));
+    API_CATCH
+}
+
+int fmm_host_register(void* ptr, size_t bytes)
+{
+    API_TRY
+    if (!ptr || !bytes) return fail(FMM_ERR_INVALID_ARGUMENT, "empty range");
+    SFMM_CUDA(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    API_CATCH
+}
+
+int fmm_host_unregister(void* ptr)
+{
+    API_TRY
+    SFMM_CUDA(cudaHostUnregister(ptr));
+    API_CATCH
+}
+
+int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level, int max_ppn,
+                   int vertical_axis, double phideg, fmm_tree** out)
+{
+    API_TRY
+    if (!ctx || !out || !xyz) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (where != FMM_HOST && where != FMM_DEVICE) return fail(FMM_ERR_INVALID_ARGUMENT, "where must be FMM_HOST or FMM_DEVICE");
+    *out = nullptr;
+    bind(ctx->c);
+    auto* tr = new fmm_tree;
+    try {
+        tr->t.ctx = &ctx->c;
+        tr->t.n = n;
+        if (n <= 0) throw sfmm::Error(FMM_ERR_INVALID_ARGUMENT, "n must be positive");
+        sfmm::DevBuf<double> staged;
+        const double* dxyz = xyz;
+        if (where == FMM_HOST) {
+            staged.alloc(size_t(3) * n, ctx->c.stream);
+            SFMM_CUDA(cudaMemcpyAsync(staged.ptr, xyz, size_t(3) * n * sizeof(double), cudaMemcpyHostToDevice, ctx->c.stream));
+            dxyz = staged.ptr;
+        }
+        sfmm::build_tree(tr->t, dxyz, max_level, max_ppn, vertical_axis, phideg);
+    } catch (...) {
+        delete tr;
+        throw;
+    }
+    *out = tr;
+    API_CATCH
+}
+
+int fmm_tree_destroy(fmm_tree* tree)
+{
+    API_TRY
+    if (!tree) return FMM_OK;
+    bind(*tree->t.ctx);
+    delete tree;
+    API_CATCH
+}
+
+int fmm_tree_depth(const fmm_tree* tree, int* depth)
+{
+    if (!tree || !depth) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *depth = tree->t.depth;
+    return FMM_OK;
+}
+
+int fmm_tree_box(const fmm_tree* tree, double* width, double* corner3)
+{
+    if (!tree || !width || !corner3) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *width = tree->t.box.width;
+    for (int a = 0; a < 3; ++a) corner3[a] = tree->t.box.corner[a];
+    return FMM_OK;
+}
+
+int fmm_tree_export_size(const fmm_tree* tree, int level, int what, int64_t* count)
+{
+    API_TRY
+    if (!tree || !count) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    bind(*tree->t.ctx);
+    *count = sfmm::tree_export(tree->t, level, what, nullptr);
+    API_CATCH
+}
+
+int fmm_tree_export(const fmm_tree* tree, int level, int what, void* host_out)
+{
+    API_TRY
+    if (!tree || !host_out) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    bind(*tree->t.ctx);
+    if (sfmm::tree_export(tree->t, level, what, host_out) < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "export not defined at this level");
+    API_CATCH
+}
+
+int fmm_tree_stats(const fmm_tree* tree, int64_t* s)
+{
+    if (!tree || !s) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    s[0] = tree->t.n_nodes;
+    s[1] = tree->t.n_leaves;
+    s[2] = tree->t.il_nnz;
+    s[3] = tree->t.near_pairs;
+    s[4] = tree->t.nr_nnz;
+    return FMM_OK;
+}
+
+int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** out)
+{
+    API_TRY
+    if (!tree || !out) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *out = nullptr;
+    if (p < 0 || p > sfmm::kMaxOrder) return fail(FMM_ERR_UNSUPPORTED, "expansion order must be in [0, 16]");
+    if (qdim < 1 || qdim > 3) return fail(FMM_ERR_UNSUPPORTED, "charge components N must be 1, 2 or 3");
+    if (precision != FMM_PRECISION_FP64) return fail(FMM_ERR_UNSUPPORTED, "only the FP64 precision is available");
+    bind(*tree->t.ctx);
+    auto* pl = new fmm_plan;
+    try {
+        pl->pl.tree = &tree->t;
+        pl->pl.p = p;
+        pl->pl.qdim = qdim;
+        pl->pl.precision = precision;
+        for (auto& e : pl->pl.ev) SFMM_CUDA(cudaEventCreate(&e));
+        sfmm::plan_init(pl->pl);
+        SFMM_CUDA(cudaStreamSynchronize(tree->t.ctx->stream));
+    } catch (...) {
+        for (auto& e : pl->pl.ev)
+            if (e) cudaEventDestroy(e);
+        delete pl;
+        throw;
+    }
+    *out = pl;
+    API_CATCH
+}
+
+int fmm_plan_destroy(fmm_plan* plan)
+{
+    API_TRY
+    if (!plan) return FMM_OK;
+    bind(*plan->pl.tree->ctx);
+    SFMM_CUDA(cudaStreamSynchronize(plan->pl.tree->ctx->stream));
+    for (auto& e : plan->pl.ev)
+        if (e) cudaEventDestroy(e);
+    delete plan;
+    API_CATCH
+}
+
+int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, int where)
+{
+    API_TRY
+    if (!plan || !Q) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (where != FMM_HOST && where != FMM_DEVICE) return fail(FMM_ERR_INVALID_ARGUMENT, "where must be FMM_HOST or FMM_DEVICE");
+    sfmm::Plan& pl = plan->pl;
+    if (field && pl.qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs N = 1 or N = 3 charges");
+    if (!pot && !field) return FMM_OK;
+    sfmm::Context& c = *pl.tree->ctx;
+    bind(c);
+    const int64_t n = pl.tree->n;
+    if (where == FMM_DEVICE) {
+        sfmm::plan_evaluate(pl, Q, pot, field);
+        return FMM_OK;
+    }
+    cudaStream_t st = c.stream;
+    const size_t qb = size_t(n) * pl.qdim * sizeof(double);
+    if (pl.qin.count < size_t(n) * pl.qdim) pl.qin.alloc(size_t(n) * pl.qdim, st);
+    SFMM_CUDA(cudaMemcpyAsync(pl.qin.ptr, Q, qb, cudaMemcpyHostToDevice, st));
+    double* dpot = nullptr;
+    double* dfield = nullptr;
+    if (pot) {
+        if (pl.uio_pot.count < size_t(n) * pl.qdim) pl.uio_pot.alloc(size_t(n) * pl.qdim, st);
+        SFMM_CUDA(cudaMemcpyAsync(pl.uio_pot.ptr, pot, qb, cudaMemcpyHostToDevice, st));
+        dpot = pl.uio_pot.ptr;
+    }
+    if (field) {
+        if (pl.uio_field.count < size_t(n) * 3) pl.uio_field.alloc(size_t(n) * 3, st);
+        SFMM_CUDA(cudaMemcpyAsync(pl.uio_field.ptr, field, size_t(n) * 3 * sizeof(double), cudaMemcpyHostToDevice, st));
+        dfield = pl.uio_field.ptr;
+    }
+    sfmm::plan_evaluate(pl, pl.qin.ptr, dpot, dfield);
+    if (pot) SFMM_CUDA(cudaMemcpyAsync(pot, dpot, qb, cudaMemcpyDeviceToHost, st));
+    if (field) SFMM_CUDA(cudaMemcpyAsync(field, dfield, size_t(n) * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    API_CATCH
+}
+
+int fmm_rinv(fmm_plan* plan, const double* Q, double* U, int gradient, int where)
+{
+    if (!plan) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (gradient && plan->pl.qdim != 3) return fail(FMM_ERR_UNSUPPORTED, "rinv<true> needs N = 3 (fmm.hpp:550)");
+    return gradient ? fmm_evaluate(plan, Q, nullptr, U, where) : fmm_evaluate(plan, Q, U, nullptr, where);
+}
+
+int fmm_plan_timings(const fmm_plan* plan, double* ms6)
+{
+    API_TRY
+    if (!plan || !ms6) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    bind(*plan->pl.tree->ctx);
+    sfmm::plan_read_timings(const_cast<sfmm::Plan&>(plan->pl), ms6);
+    API_CATCH
+}
+
+int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
+               int64_t nt, double* pot, double* field, int where)
+{
+    API_TRY
+    if (!ctx || !xyz || !Q || !targets) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (qdim < 1 || qdim > 3) return fail(FMM_ERR_UNSUPPORTED, "qdim must be 1, 2 or 3");
+    if (field && qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs qdim 1 or 3");
+    if (n <= 0 || nt < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "bad sizes");
+    bind(ctx->c);
+    cudaStream_t st = ctx->c.stream;
+    if (where == FMM_DEVICE) {
+        sfmm::direct_sum(ctx->c, xyz, n, Q, qdim, targets, nt, pot, field);
+        SFMM_CUDA(cudaStreamSynchronize(st));
+        return FMM_OK;
+    }
+    sfmm::DevBuf<double> dx, dq, dp, df;
+    sfmm::DevBuf<int64_t> dt;
+    dx.alloc(size_t(3) * n, st);
+    dq.alloc(size_t(qdim) * n, st);
+    dt.alloc(std::max<int64_t>(nt, 1), st);
+    SFMM_CUDA(cudaMemcpyAsync(dx.ptr, xyz, size_t(3) * n * 8, cudaMemcpyHostToDevice, st));
+    SFMM_CUDA(cudaMemcpyAsync(dq.ptr, Q, size_t(qdim) * n * 8, cudaMemcpyHostToDevice, st));
+    SFMM_CUDA(cudaMemcpyAsync(dt.ptr, targets, size_t(nt) * 8, cudaMemcpyHostToDevice, st));
+    if (pot) dp.alloc(size_t(qdim) * std::max<int64_t>(nt, 1), st);
+    if (field) df.alloc(size_t(3) * std::max<int64_t>(nt, 1), st);
+    sfmm::direct_sum(ctx->c, dx.ptr, n, dq.ptr, qdim, dt.ptr, nt, pot ? dp.ptr : nullptr, field ? df.ptr : nullptr);
+    if (pot) SFMM_CUDA(cudaMemcpyAsync(pot, dp.ptr, size_t(qdim) * nt * 8, cudaMemcpyDeviceToHost, st));
+    if (field) SFMM_CUDA(cudaMemcpyAsync(field, df.ptr, size_t(3) * nt * 8, cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    API_CATCH
+}
+
+int fmm_launch_count(int64_t* count)
+{
+    if (!count) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *count = sfmm::g_launches.load();
+    return FMM_OK;
+}
+
+}  // extern "C"

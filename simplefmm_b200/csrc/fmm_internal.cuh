@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <stdexcept>
 #include <string>
@@ -27,7 +28,13 @@ struct Error : std::runtime_error {
         if (e_ != cudaSuccess) ::sfmm::throw_cuda(e_, #x, __FILE__, __LINE__); \
     } while (0)
 
-#define SFMM_CHECK_LAUNCH() SFMM_CUDA(cudaGetLastError())
+extern std::atomic<long long> g_launches;
+
+#define SFMM_CHECK_LAUNCH()                   \
+    do {                                      \
+        ::sfmm::g_launches.fetch_add(1);      \
+        SFMM_CUDA(cudaGetLastError());        \
+    } while (0)
 
 #define SFMM_REQUIRE(cond, status, msg)                 \
     do {                                                \
@@ -182,6 +189,10 @@ struct Plan;
 // tree.cu
 void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg);
 int64_t tree_export(const Tree& t, int level, int what, void* host_out);
+
+// direct.cu
+void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets, int64_t nt,
+                double* pot, double* field);
 
 // scan.cu
 void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);

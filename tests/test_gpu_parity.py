@@ -1,0 +1,162 @@
+"""Parity of the CUDA path with the reference.
+
+Trees and lists are compared bit for bit against the reference's own dumps
+(tests/golden, generated by tests/golden/make_golden.py from the compiled
+reference).  Potentials and fields must agree per target to 1e-12 relative
+to the magnitude sum S_i = sum_j |Q_j|/r_ij (potential) or sum_j |Q_j|/r_ij^2
+(field): the size of the terms summed at target i, which FP64 rounding is
+proportional to.  Every call goes through the C ABI (libsimplefmm_b200.so).
+"""
+import numpy as np
+import pytest
+
+import simplefmm_b200 as sf
+from conftest import golden_cases, load_golden, rel_err_per_target, rel_l2, tree_keys
+from oracle import pyoracle
+from simplefmm_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-12
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    return sf.Context(0)
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_tree_bit_exact(ctx, name):
+    g = load_golden(name)
+    t = sf.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"], ctx=ctx)
+    d = t.dump()
+    assert t.depth == int(g["DEPTH"][0])
+    if "CNODE0" not in g:
+        return
+    assert np.array_equal(d["BOX"], g["BOX"])
+    for k in tree_keys(g):
+        assert np.array_equal(d[k], g[k]), k
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_results_match_reference(ctx, name):
+    g = load_golden(name)
+    t = sf.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"], ctx=ctx)
+    plan = sf.Plan(t, g["p"], g["qdim"])
+    sp, sf_ = pyoracle.error_scales(g["pos"], g["q"])
+    n = g["n"]
+    if g["qdim"] == 1:
+        pot = np.zeros(n)
+        field = np.zeros((n, 3)) if "FIELD" in g else None
+        plan.evaluate(g["q"], pot, field)
+        assert rel_err_per_target(pot, g["POT"], sp) < TOL
+        if field is not None:
+            assert rel_err_per_target(field, g["FIELD"], sf_) < TOL
+    else:
+        vp = np.zeros((n, 3))
+        bi = np.zeros((n, 3))
+        plan.rinv(g["q"], vp)
+        plan.rinv(g["q"], bi, gradient=True)
+        assert rel_err_per_target(vp, g["VECPOT"], sp) < TOL
+        assert rel_err_per_target(bi, g["BIOT"], sf_) < TOL
+
+
+def test_one_pass_equals_separate_calls(ctx):
+    g = load_golden("plummer_n6000_p5_ppn32")
+    t = sf.Tree(g["pos"], 20, 32, ctx=ctx)
+    plan = sf.Plan(t, 5, 1)
+    n = g["n"]
+    pot, field = np.zeros(n), np.zeros((n, 3))
+    plan.evaluate(g["q"], pot, field)
+    pot2, field2 = np.zeros(n), np.zeros((n, 3))
+    plan.evaluate(g["q"], pot2, None)
+    plan.evaluate(g["q"], None, field2)
+    assert np.array_equal(pot, pot2)
+    assert np.array_equal(field, field2)
+
+
+def test_outputs_accumulate(ctx):
+    """U is accumulated, never overwritten (fmm.hpp:767, 788; main.cpp:57-61)."""
+    g = load_golden("uniform_n3000_p6")
+    t = sf.Tree(g["pos"], 20, 64, ctx=ctx)
+    plan = sf.Plan(t, 6, 1)
+    U = np.full(g["n"], 5.0)
+    plan.rinv(g["q"], U)
+    plan.rinv(g["q"], U)
+    sp, _ = pyoracle.error_scales(g["pos"], g["q"])
+    assert rel_err_per_target(U - 5.0, 2 * g["POT"], 2 * sp) < TOL
+
+
+@pytest.mark.parametrize("dist,n,p,ppn", [("plummer", 40000, 10, 64), ("uniform", 50000, 8, 64),
+                                          ("gauss2", 20000, 12, 64), ("shell", 30000, 6, 32)])
+def test_medium_against_restatement(ctx, dist, n, p, ppn):
+    pos = W.points(dist, n, 101)
+    q = W.charges(n, 101)
+    ot = pyoracle.Tree(pos, 20, ppn)
+    t = sf.Tree(pos, 20, ppn, ctx=ctx)
+    d, od = t.dump(), ot.dump()
+    for k in tree_keys(od):
+        assert np.array_equal(d[k], od[k]), k
+    pot, field = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, p, 1).evaluate(q, pot, field)
+    opot, ofield = ot.potential_field(p, q)
+    tg = np.arange(0, n, 37)
+    sp, sfl = pyoracle.error_scales(pos, q, tg)
+    assert rel_err_per_target(pot[tg], opot[tg], sp) < TOL
+    assert rel_err_per_target(field[tg], ofield[tg], sfl) < TOL
+
+
+def test_large_plummer_against_direct_sum(ctx):
+    """Configuration-size check: N = 4M Plummer, p = 10, leaf 64, against the
+    FP64 direct sum on seeded sample targets (truncation error only)."""
+    n = 4_000_000
+    pos = W.plummer(n, 7)
+    q = W.charges(n, 7)
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    pot, field = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, 10, 1).evaluate(q, pot, field)
+    tg = np.random.default_rng(7).choice(n, 1000, replace=False)
+    dpot = pyoracle.direct(pos, q, tg)
+    dfield = pyoracle.direct(pos, q, tg, mode="field")
+    assert rel_l2(pot[tg], dpot) < 1e-5
+    assert rel_l2(field[tg], dfield) < 1e-4
+
+
+def test_edge_cases(ctx):
+    # one point: nothing to sum
+    t = sf.Tree(np.array([[0.1, 0.2, 0.3]]), ctx=ctx)
+    U = np.zeros(1)
+    sf.Plan(t, 4, 1).rinv(np.array([1.0]), U)
+    assert U[0] == 0.0
+    # two points: direct only
+    pos = np.array([[0.0, 0.0, 0.0], [1.0, 2.0, 2.0]])
+    t = sf.Tree(pos, ctx=ctx)
+    U = np.zeros(2)
+    sf.Plan(t, 4, 1).rinv(np.array([2.0, -1.0]), U)
+    assert np.allclose(U, [-1.0 / 3.0, 2.0 / 3.0], rtol=0, atol=1e-15)
+    # coplanar vertical extent: the reference would never leave its box loop
+    flat = np.random.default_rng(0).random((100, 3))
+    flat[:, 2] = 0.5
+    with pytest.raises(sf.FMMError) as e:
+        sf.Tree(flat, ctx=ctx)
+    assert e.value.status == 5
+    # max_level caps refinement: leaves may exceed max_particles_per_node
+    pos = W.uniform_cube(5000, 3)
+    t = sf.Tree(pos, max_level=2, max_particles_per_node=8, ctx=ctx)
+    assert t.depth == 2
+    ot = pyoracle.Tree(pos, 2, 8)
+    d, od = t.dump(), ot.dump()
+    for k in tree_keys(od):
+        assert np.array_equal(d[k], od[k]), k
+
+
+def test_invalid_arguments(ctx):
+    t = sf.Tree(W.uniform_cube(1000, 1), ctx=ctx)
+    with pytest.raises(sf.FMMError) as e:
+        sf.Plan(t, 17, 1)
+    assert e.value.status == 2
+    with pytest.raises(sf.FMMError):
+        sf.Plan(t, 8, 4)
+    p1 = sf.Plan(t, 4, 1)
+    with pytest.raises(sf.FMMError) as e:
+        p1.rinv(np.zeros(1000), np.zeros((1000, 3)), gradient=True)
+    assert e.value.status == 2
