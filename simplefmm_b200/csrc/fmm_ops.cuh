@@ -162,6 +162,43 @@ SFMM_HD void grad_moment(const cplx* M, int n, int m, cplx* gx, cplx* gy, cplx* 
     *gz = z;
 }
 
+// Target-side gradient of a local expansion.  With
+//   U(x) = sum_{j, |k| <= j} Re(B_j^k conj(S_j^k(x - c)))      (fmm.hpp:765-768)
+// and the ladder relations above extended to k < 0 through
+// S_j^{-k} = conj(S_j^k), dU/dx_c = sum_{n,m} Re(G_c[n,m] conj(S_n^m)) with
+//   G_z[n,m] = sqrt((n+1-m)(n+1+m)) B_{n+1}^m
+//   G_x[n,m] = (t1 + t2)/2,   G_y[n,m] = (i/2)(t1 - t2)
+//   t1 = -sqrt((n+m+2)(n+m+1)) B_{n+1}^{m+1}
+//   t2 =  sqrt((n-m+2)(n-m+1)) B_{n+1}^{m-1}   (m >= 1)
+//   t2 = -sqrt((n+2)(n+1)) conj(B_{n+1}^1)      (m = 0).
+// The source-gradient M2L of the reference (moments of Q x Zgrho, order p,
+// from plain moments of order p - 1) equals, term by term, minus this
+// gradient of the order-(p+1) local expansion of the order-(p-1) plain
+// moments: grad_s 1/|t - s| = -grad_t 1/|t - s| matches every coefficient of
+// the two-centre expansion.  B is stored with order p + 1 (tri indexing).
+SFMM_HD void grad_local(const cplx* B, int n, int m, cplx* gx, cplx* gy, cplx* gz)
+{
+    const cplx b0 = B[tri(n + 1, m)];
+    const double cz = sqrt(double(n + 1 - m) * double(n + 1 + m));
+    *gz = {cz * b0.re, cz * b0.im};
+    const cplx bp = B[tri(n + 1, m + 1)];
+    const double c1 = -sqrt(double(n + m + 2) * double(n + m + 1));
+    const cplx t1{c1 * bp.re, c1 * bp.im};
+    cplx t2;
+    if (m >= 1) {
+        const cplx bm = B[tri(n + 1, m - 1)];
+        const double c2 = sqrt(double(n - m + 2) * double(n - m + 1));
+        t2 = {c2 * bm.re, c2 * bm.im};
+    } else {
+        const cplx b1 = B[tri(n + 1, 1)];
+        const double c2 = -sqrt(double(n + 2) * double(n + 1));
+        t2 = {c2 * b1.re, -c2 * b1.im};
+    }
+    *gx = {0.5 * (t1.re + t2.re), 0.5 * (t1.im + t2.im)};
+    // (i/2)(t1 - t2)
+    *gy = {-0.5 * (t1.im - t2.im), 0.5 * (t1.re - t2.re)};
+}
+
 // Component layout of an evaluation: `qdim` plain-moment components come
 // out of P2M/M2M; `K` components go through M2L/L2L/L2P:
 //   [0, qdim)      potential of each charge component (if want_pot)

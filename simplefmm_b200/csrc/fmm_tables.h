@@ -22,6 +22,10 @@ struct HostTables {
     std::vector<double> rot;             // kRotClasses x rot_len
     std::vector<int> tz_off;             // per k >= 0
     std::vector<double> tz;
+    // z-translation with target orders j <= p+1 and source orders n <= p
+    // (rows j = k..p+1, columns n = k..p), for the field's order-(p+1) local
+    std::vector<int> tzx_off;
+    std::vector<double> tzx;
     std::vector<double> eil;             // 49 x (p+1) complex (re, im)
     std::vector<double> echild, eparent; // 4 x (2p+1) complex
     std::vector<int> m2m_ptr, m2m_code;  // per output (tri order) term ranges

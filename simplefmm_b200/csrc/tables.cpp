@@ -16,6 +16,7 @@
 //   M2M / L2L (fmm.hpp:558-576, 714-733) -> per-output term lists whose
 //       octant-independent factor is precomputed; the octant enters through
 //       a sign (-1)^(n-|m|) and a phase e^{i q phi}.
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <vector>
@@ -66,8 +67,8 @@ HostTables make_tables(int p)
     t.p = p;
     t.T = (p + 1) * (p + 2) / 2;
     const double th_diag = std::acos(1 / std::sqrt(3.0));
-    std::vector<double> A((2 * p + 1) * (2 * p + 2) / 2);
-    for (int n = 0; n <= 2 * p; ++n)
+    std::vector<double> A((2 * p + 3) * (2 * p + 4) / 2);
+    for (int n = 0; n <= 2 * p + 2; ++n)
         for (int m = 0; m <= n; ++m) A[tri(n, m)] = Afun(n, m);
     auto a = [&](int n, int m) { return A[tri(n, std::abs(m))]; };
     std::vector<double> Znear(t.T);
@@ -130,6 +131,17 @@ HostTables make_tables(int p)
         for (int j = k; j <= p; ++j)
             for (int n = k; n <= p; ++n)
                 t.tz[t.tz_off[k] + (j - k) * w + (n - k)] = sgn_pow(n + k) * a(n, k) * a(j, k) / a(j + n, 0);
+    }
+
+    t.tzx_off.resize(p + 3);
+    t.tzx_off[0] = 0;
+    for (int k = 0; k <= p + 1; ++k) t.tzx_off[k + 1] = t.tzx_off[k] + (p + 2 - k) * std::max(p + 1 - k, 0);
+    t.tzx.resize(std::max(t.tzx_off[p + 2], 1));
+    for (int k = 0; k <= p + 1; ++k) {
+        const int w = p + 1 - k;
+        for (int j = k; j <= p + 1; ++j)
+            for (int n = k; n <= p; ++n)
+                t.tzx[t.tzx_off[k] + (j - k) * w + (n - k)] = sgn_pow(n + k) * a(n, k) * a(j, k) / a(j + n, 0);
     }
 
     // ---- M2L phases e^{i q atan2(dj, di)}, q = 0..p (fmm.hpp:285-292)
