@@ -3,11 +3,21 @@
 // Phase structure of FMM3D::rinv (fmm.hpp:811-881): far field only when the
 // tree is at least 2 levels deep; multipoles at every leaf of level >= 2;
 // M2M up to level 2; M2L on levels 2..depth; L2L down; L2P at every leaf of
-// level >= 2; near field over the neighbour lists.  All per-coefficient
-// math is in fmm_ops.cuh; expansions keep only m >= 0.
+// level >= 2; near field over the neighbour lists.  Per-coefficient math is
+// in fmm_ops.cuh; expansions keep only m >= 0.
+//
+// Potential and field share one M2L: for every (target, source) pair the
+// source multipole is rotated once, z-translated into both the order-p
+// potential local LA and the order-(p+1) field local LB (source orders
+// <= p-1), and the two are rotated back.  The field is minus the gradient of
+// LB at the target, identical term by term to the reference's
+// source-gradient moments (fmm.hpp:234-253, 549-551).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 
 #include "fmm_eval.cuh"
 #include "fmm_tables.h"
@@ -18,7 +28,10 @@ __constant__ HarmCoef c_harm;
 
 namespace {
 
-constexpr int kMaxWarps = 4;              // warps per block in the per-box kernels (fewer when shared memory is short)
+constexpr int kMaxWarps = 8;
+constexpr int kCols = 4;                  // M2L columns (pair x charge component) per warp chunk
+constexpr int kMaxGroupPairs = 8 * 189;   // <= 8 siblings x n_ilist_max (partition.hpp:149)
+constexpr int kNumClasses = 70;           // rotation classes (fmm.hpp:169)
 
 __device__ __forceinline__ int level_of(const EvalArgs& a, int64_t g)
 {
@@ -145,167 +158,388 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_m2m(EvalArgs a, int lp, int6
     }
 }
 
-// M2L (fmm.hpp:620-712) first version: warp per target node, pairs in
-// ilist order; rotate -> z-translate -> rotate back in warp-private shared
-// buffers, accumulation in shared memory, one store per target.
-__global__ void __launch_bounds__(kMaxWarps * 32) k_m2l(EvalArgs a, int64_t off, int64_t cnt)
+// ------------------------------------------------------------------ M2L
+// Shared-memory plan of k_m2l (same arithmetic on host and device).
+struct M2LLayout {
+    int ent_src, ent_code, cls, sorted, cls_cnt, cls_off, chunk_off, colinfo, eil, accA, accB, warps, total;
+    int per_warp;
+};
+
+__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
+
+__host__ __device__ inline M2LLayout m2l_layout(int p, int qdim, int warps)
 {
-    extern __shared__ double smem[];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int p = a.p, T = a.T, K = a.cs.K, KT = K * T;
-    double* tz = smem;                                           // tz_len
-    cplx* eil = reinterpret_cast<cplx*>(smem + a.tz_len);        // 49 x (p+1)
-    cplx* wbase = eil + 49 * (p + 1) + w * (3 * KT + a.qdim * T);
-    cplx* A = wbase;
-    cplx* B = A + KT;
-    cplx* acc = B + KT;
-    cplx* src = acc + KT;
-    for (int t = threadIdx.x; t < a.tz_len; t += blockDim.x) tz[t] = a.tz[t];
-    for (int t = threadIdx.x; t < 49 * (p + 1); t += blockDim.x) eil[t] = a.eil[t];
+    const int T = (p + 1) * (p + 2) / 2, T1 = (p + 2) * (p + 3) / 2;
+    M2LLayout L;
+    int o = 0;
+    L.ent_src = o; o = align16(o + 4 * kMaxGroupPairs);
+    L.ent_code = o; o = align16(o + 4 * kMaxGroupPairs);
+    L.cls = o; o = align16(o + 4 * kMaxGroupPairs);
+    L.sorted = o; o = align16(o + 4 * kMaxGroupPairs);
+    L.cls_cnt = o; o = align16(o + 4 * 72);
+    L.cls_off = o; o = align16(o + 4 * 72);
+    L.chunk_off = o; o = align16(o + 4 * 72);
+    L.colinfo = o; o = align16(o + 4 * kMaxWarps * kCols);
+    L.eil = o; o = align16(o + 16 * 49 * (p + 2));
+    L.accA = o; o = align16(o + 16 * 8 * qdim * T);
+    L.accB = o; o = align16(o + 16 * 8 * qdim * T1);
+    L.per_warp = align16(16 * 4 * kCols * T1);
+    L.warps = warps;
+    L.total = o + warps * L.per_warp;
+    return L;
+}
+
+// M2L (fmm.hpp:620-712): one block per sibling group (the children of one
+// node), all their interaction pairs sorted by rotation class and processed
+// in chunks of kCols same-class columns per warp, so every rotation-matrix
+// element read feeds kCols pairs.  Per chunk: phase + rotate (P/Q), split
+// z-translation into LA (orders <= p) and LB (orders <= p+1, sources <= p-1),
+// inverse rotation (PB/QB) + phase.  Warp outputs are added to per-target
+// shared accumulators in a fixed order after every round, and each target's
+// locals are stored once.
+__global__ void __launch_bounds__(kMaxWarps * 32) k_m2l(EvalArgs a, int64_t g0, int64_t g1)
+{
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int p = a.p, T = a.T, T1 = a.T1, qd = a.qdim;
+    const M2LLayout Ly = m2l_layout(p, qd, nw);
+    int* ent_src = reinterpret_cast<int*>(sm + Ly.ent_src);
+    int* ent_code = reinterpret_cast<int*>(sm + Ly.ent_code);
+    int* cls = reinterpret_cast<int*>(sm + Ly.cls);
+    int* sorted = reinterpret_cast<int*>(sm + Ly.sorted);
+    int* cls_cnt = reinterpret_cast<int*>(sm + Ly.cls_cnt);
+    int* cls_off = reinterpret_cast<int*>(sm + Ly.cls_off);
+    int* chunk_off = reinterpret_cast<int*>(sm + Ly.chunk_off);
+    int* colinfo = reinterpret_cast<int*>(sm + Ly.colinfo);
+    cplx* eil = reinterpret_cast<cplx*>(sm + Ly.eil);
+    cplx* accA = reinterpret_cast<cplx*>(sm + Ly.accA);
+    cplx* accB = reinterpret_cast<cplx*>(sm + Ly.accB);
+    cplx* X = reinterpret_cast<cplx*>(sm + Ly.total - (nw - w) * Ly.per_warp);
+    cplx* Y = X + kCols * T1;
+    cplx* Z = Y + kCols * T1;
+    cplx* O = Z + kCols * T1;
+
+    for (int t = threadIdx.x; t < 49 * (p + 2); t += blockDim.x) eil[t] = a.eil[t];
     __syncthreads();
-    for (int64_t i = blockIdx.x * int64_t(nw) + w; i < cnt; i += int64_t(gridDim.x) * nw) {
-        const int64_t g = off + i;
-        const int e0 = a.il_ptr[g], e1 = a.il_ptr[g + 1];
-        const int l = level_of(a, g);
-        for (int t = lane; t < KT; t += 32) acc[t] = cplx{0, 0};
-        for (int e = e0; e < e1; ++e) {
-            const int s = a.il_src[e];
-            const int code = a.il_code[e];
-            const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
-            const double* R = a.rot + int64_t(rot_class(di, dj, dk)) * a.rot_len;
-            const cplx* ph = eil + (7 * (dj + 3) + (di + 3)) * (p + 1);
-            const double* ipw = a.ipow + (int64_t(l) * 28 + (di * di + dj * dj + dk * dk)) * (2 * p + 2);
-            const cplx* Ms = a.M + int64_t(s) * a.qdim * T;
-            for (int t = lane; t < a.qdim * T; t += 32) src[t] = Ms[t];
-            __syncwarp();
-            // derive + phase: Mt = e^{i m phi} X
-            for (int o = lane; o < KT; o += 32) {
-                const int k = o / T, t = o - k * T;
-                int n, m;
-                tri_nm(t, n, m);
-                A[o] = cmul(ph[m], derive_component(a.cs, src, T, k, n, m));
+
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        const int nc = a.nchild[g];
+        if (nc == 0) continue;
+        const int cb = a.child_beg[g];
+        const int l = level_of(a, g) + 1;                       // level of the targets
+        const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
+        // ---- gather the group's pairs, classify
+        for (int s = 0; s < nc; ++s) {
+            const int r0 = a.il_ptr[cb + s] - e0, r1 = a.il_ptr[cb + s + 1] - e0;
+            for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
+                const int code = a.il_code[e0 + e];
+                ent_src[e] = a.il_src[e0 + e];
+                ent_code[e] = code | (s << 9);
+                cls[e] = rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3);
             }
-            __syncwarp();
-            // rotation: W_n = (P Re Mt_n, Q Im Mt_n) rho^{-n}
-            for (int o = lane; o < KT; o += 32) {
-                const int k = o / T, t = o - k * T;
-                int n, aa;
-                tri_nm(t, n, aa);
-                const double* P = R + a.rot_off[n] + aa * (n + 1);
-                const double* Qm = P + (n + 1) * (n + 1);
-                const cplx* x = A + k * T + n * (n + 1) / 2;
-                double re = 0, im = 0;
-                for (int b = 0; b <= n; ++b) {
-                    re += __ldg(P + b) * x[b].re;
-                    im += __ldg(Qm + b) * x[b].im;
-                }
-                const double sc = n ? ipw[n - 1] : 1.0;
-                B[o] = cplx{re * sc, im * sc};
-            }
-            __syncwarp();
-            // z-translation: Lz_j^k = rho^{-(j+1)} sum_n tz[k][j][n] W_n^k
-            for (int o = lane; o < KT; o += 32) {
-                const int k = o / T, t = o - k * T;
-                int j, kk;
-                tri_nm(t, j, kk);
-                const int wd = p + 1 - kk;
-                const double* row = tz + a.tz_off[kk] + (j - kk) * wd;
-                const cplx* x = B + k * T;
-                double re = 0, im = 0;
-                for (int n = kk; n <= p; ++n) {
-                    const cplx v = x[n * (n + 1) / 2 + kk];
-                    re += row[n - kk] * v.re;
-                    im += row[n - kk] * v.im;
-                }
-                const double sc = ipw[j];
-                A[o] = cplx{re * sc, im * sc};
-            }
-            __syncwarp();
-            // rotate back + phase, accumulate
-            for (int o = lane; o < KT; o += 32) {
-                const int k = o / T, t = o - k * T;
-                int j, aa;
-                tri_nm(t, j, aa);
-                const int wd = (j + 1) * (j + 1);
-                const double* PB = R + a.rot_off[j] + 2 * wd + aa * (j + 1);
-                const double* QB = PB + wd;
-                const cplx* x = A + k * T + j * (j + 1) / 2;
-                double re = 0, im = 0;
-                for (int b = 0; b <= j; ++b) {
-                    re += __ldg(PB + b) * x[b].re;
-                    im += __ldg(QB + b) * x[b].im;
-                }
-                const cplx v = cmul(cconj(ph[aa]), cplx{re, im});
-                acc[o].re += v.re;
-                acc[o].im += v.im;
-            }
-            __syncwarp();
         }
-        cplx* Lt = a.L + g * KT;
-        for (int t = lane; t < KT; t += 32) Lt[t] = acc[t];
-        __syncwarp();
+        for (int t = threadIdx.x; t < 8 * qd * T; t += blockDim.x) accA[t] = cplx{0, 0};
+        for (int t = threadIdx.x; t < 8 * qd * T1; t += blockDim.x) accB[t] = cplx{0, 0};
+        __syncthreads();
+        // stable counting sort by class: thread c collects class c in order
+        if (threadIdx.x < kNumClasses) {
+            int cnt = 0;
+            for (int e = 0; e < E; ++e) cnt += cls[e] == int(threadIdx.x);
+            cls_cnt[threadIdx.x] = cnt;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int s = 0, k = 0;
+            for (int c = 0; c < kNumClasses; ++c) {
+                cls_off[c] = s;
+                chunk_off[c] = k;
+                s += cls_cnt[c];
+                k += (cls_cnt[c] * qd + kCols - 1) / kCols;
+            }
+            cls_off[kNumClasses] = s;
+            chunk_off[kNumClasses] = k;
+        }
+        __syncthreads();
+        if (threadIdx.x < kNumClasses) {
+            int pos = cls_off[threadIdx.x];
+            for (int e = 0; e < E; ++e)
+                if (cls[e] == int(threadIdx.x)) sorted[pos++] = e;
+        }
+        __syncthreads();
+        const int nchunk = chunk_off[kNumClasses];
+        for (int r0 = 0; r0 < nchunk; r0 += nw) {
+            const int k = r0 + w;
+            if (k < nchunk) {
+                // ---- locate the chunk
+                int c = 0;
+                while (chunk_off[c + 1] <= k) ++c;
+                const int col0 = (k - chunk_off[c]) * kCols;
+                const int ncols_c = cls_cnt[c] * qd;
+                const int ncol = min(kCols, ncols_c - col0);
+                int src[kCols], bq[kCols], pidx[kCols];
+                int dsq = 0;
+#pragma unroll
+                for (int cc = 0; cc < kCols; ++cc) {
+                    src[cc] = 0;
+                    bq[cc] = 0;
+                    pidx[cc] = 24;
+                    if (cc < ncol) {
+                        const int col = col0 + cc;
+                        const int e = sorted[cls_off[c] + col / qd];
+                        const int code = ent_code[e];
+                        const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
+                        src[cc] = ent_src[e];
+                        bq[cc] = col % qd;
+                        pidx[cc] = 7 * (dj + 3) + (di + 3);
+                        dsq = di * di + dj * dj + dk * dk;
+                        if (lane == 0) colinfo[w * kCols + cc] = ((code >> 9) & 7) * 8 + bq[cc];
+                    } else if (lane == 0) {
+                        colinfo[w * kCols + cc] = -1;
+                    }
+                }
+                const double* R = a.rot + int64_t(c) * a.rot_len;
+                const double* ipw = a.ipow + (int64_t(l) * 28 + dsq) * a.ipow_w;
+                // (a) phase: X = e^{i m phi} M
+#pragma unroll
+                for (int cc = 0; cc < kCols; ++cc) {
+                    if (cc < ncol) {
+                        const cplx* Ms = a.M + (int64_t(src[cc]) * qd + bq[cc]) * T;
+                        const cplx* ph = eil + pidx[cc] * (p + 2);
+                        for (int t = lane; t < T; t += 32) {
+                            int n, m;
+                            tri_nm(t, n, m);
+                            X[cc * T1 + t] = cmul(ph[m], Ms[t]);
+                        }
+                    } else {
+                        for (int t = lane; t < T; t += 32) X[cc * T1 + t] = cplx{0, 0};
+                    }
+                }
+                __syncwarp();
+                // (b) rotation: Y_n = (P_n Re X_n, Q_n Im X_n) rho^{-n}
+                for (int r = lane; r < T; r += 32) {
+                    int n, aa;
+                    tri_nm(r, n, aa);
+                    const double* P = R + a.rot_off[n] + aa * (n + 1);
+                    const double* Qm = P + (n + 1) * (n + 1);
+                    const int base = n * (n + 1) / 2;
+                    double re[kCols], im[kCols];
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) re[cc] = im[cc] = 0;
+                    for (int b = 0; b <= n; ++b) {
+                        const double pb = __ldg(P + b), qb = __ldg(Qm + b);
+#pragma unroll
+                        for (int cc = 0; cc < kCols; ++cc) {
+                            const cplx x = X[cc * T1 + base + b];
+                            re[cc] += pb * x.re;
+                            im[cc] += qb * x.im;
+                        }
+                    }
+                    const double sc = n ? ipw[n - 1] : 1.0;
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) Y[cc * T1 + r] = cplx{re[cc] * sc, im[cc] * sc};
+                }
+                __syncwarp();
+                // (c) z-translation: Z = LB (sources n <= p-1, targets j <= p+1), X = LA
+                for (int r = lane; r < T1; r += 32) {
+                    int j, kk;
+                    tri_nm(r, j, kk);
+                    const int wd = p + 1 - kk;
+                    const double* row = a.tzx + a.tzx_off[kk] + (j - kk) * wd;
+                    double bre[kCols], bim[kCols];
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) bre[cc] = bim[cc] = 0;
+                    for (int n = kk; n <= p - 1; ++n) {
+                        const double tv = __ldg(row + n - kk);
+                        const int tn = n * (n + 1) / 2 + kk;
+#pragma unroll
+                        for (int cc = 0; cc < kCols; ++cc) {
+                            const cplx y = Y[cc * T1 + tn];
+                            bre[cc] += tv * y.re;
+                            bim[cc] += tv * y.im;
+                        }
+                    }
+                    const double sc = ipw[j];
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) Z[cc * T1 + r] = cplx{bre[cc] * sc, bim[cc] * sc};
+                    if (j <= p) {
+                        const double tv = __ldg(row + p - kk);
+                        const int tn = p * (p + 1) / 2 + kk;
+#pragma unroll
+                        for (int cc = 0; cc < kCols; ++cc) {
+                            const cplx y = Y[cc * T1 + tn];
+                            X[cc * T1 + r] = cplx{(bre[cc] + tv * y.re) * sc, (bim[cc] + tv * y.im) * sc};
+                        }
+                    }
+                }
+                __syncwarp();
+                // (d) inverse rotation + phase: Y = LA contribution, O = LB contribution
+                for (int r = lane; r < T1; r += 32) {
+                    int j, aa;
+                    tri_nm(r, j, aa);
+                    const int wd = (j + 1) * (j + 1);
+                    const double* PB = R + a.rot_off[j] + 2 * wd + aa * (j + 1);
+                    const double* QB = PB + wd;
+                    const int base = j * (j + 1) / 2;
+                    const bool doA = a.want_pot && j <= p;
+                    double are[kCols], aim[kCols], bre[kCols], bim[kCols];
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) are[cc] = aim[cc] = bre[cc] = bim[cc] = 0;
+                    for (int b = 0; b <= j; ++b) {
+                        const double pb = __ldg(PB + b), qb = __ldg(QB + b);
+#pragma unroll
+                        for (int cc = 0; cc < kCols; ++cc) {
+                            if (a.want_field) {
+                                const cplx z = Z[cc * T1 + base + b];
+                                bre[cc] += pb * z.re;
+                                bim[cc] += qb * z.im;
+                            }
+                            if (doA) {
+                                const cplx x = X[cc * T1 + base + b];
+                                are[cc] += pb * x.re;
+                                aim[cc] += qb * x.im;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int cc = 0; cc < kCols; ++cc) {
+                        const cplx e = cconj(eil[pidx[cc] * (p + 2) + aa]);
+                        if (a.want_field) O[cc * T1 + r] = cmul(e, cplx{bre[cc], bim[cc]});
+                        if (doA) Y[cc * T1 + r] = cmul(e, cplx{are[cc], aim[cc]});
+                    }
+                }
+            } else if (lane < kCols) {
+                colinfo[w * kCols + lane] = -1;
+            }
+            __syncthreads();
+            // ---- fixed-order accumulation of this round's warp outputs
+            const int nA = a.want_pot ? nc * qd * T : 0;
+            const int nB = a.want_field ? nc * qd * T1 : 0;
+            for (int e = threadIdx.x; e < nA + nB; e += blockDim.x) {
+                const bool isA = e < nA;
+                const int ee = isA ? e : e - nA;
+                const int TT = isA ? T : T1;
+                const int sb = ee / TT, t = ee - sb * TT;      // sb = slot * qd + b
+                const int tag = (sb / qd) * 8 + sb % qd;
+                cplx s{0, 0};
+                for (int ww = 0; ww < nw; ++ww) {
+                    const cplx* Xw = reinterpret_cast<const cplx*>(sm + Ly.total - (nw - ww) * Ly.per_warp);
+                    const cplx* src_buf = isA ? Xw + kCols * T1 : Xw + 3 * kCols * T1;
+                    for (int cc = 0; cc < kCols; ++cc)
+                        if (colinfo[ww * kCols + cc] == tag) {
+                            s.re += src_buf[cc * T1 + t].re;
+                            s.im += src_buf[cc * T1 + t].im;
+                        }
+                }
+                cplx* acc = isA ? accA : accB;
+                acc[ee].re += s.re;
+                acc[ee].im += s.im;
+            }
+            __syncthreads();
+        }
+        // ---- store the group's locals (M2L is their first contribution)
+        if (a.want_pot)
+            for (int e = threadIdx.x; e < nc * qd * T; e += blockDim.x) a.LA[int64_t(cb) * qd * T + e] = accA[e];
+        if (a.want_field)
+            for (int e = threadIdx.x; e < nc * qd * T1; e += blockDim.x) a.LB[int64_t(cb) * qd * T1 + e] = accB[e];
+        __syncthreads();
     }
 }
 
-// L2L (fmm.hpp:714-745): warp per child node at level lc.
+// L2L (fmm.hpp:714-745): warp per child node at level lc; LA at order p,
+// LB at order p + 1 (exact: a polynomial of degree p + 1 re-expanded).
 __global__ void __launch_bounds__(kMaxWarps * 32) k_l2l(EvalArgs a, int lc, int64_t off, int64_t cnt)
 {
     extern __shared__ double smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int p = a.p, T = a.T, K = a.cs.K, KT = K * T;
-    double* rpow = smem;
-    cplx* phase = reinterpret_cast<cplx*>(smem + 32);
-    cplx* par = reinterpret_cast<cplx*>(smem + 32) + 4 * (2 * kMaxOrder + 1) + w * KT;
+    const int p = a.p, T = a.T, T1 = a.T1, qd = a.qdim;
+    double* rpow = smem;                                                   // p + 2
+    cplx* ph = reinterpret_cast<cplx*>(smem + 32);                         // 4 x (2p+1)
+    cplx* ph1 = ph + 4 * (2 * kMaxOrder + 1);                              // 4 x (2p+3)
+    cplx* parA = ph1 + 4 * (2 * kMaxOrder + 3) + w * qd * (T + T1);
+    cplx* parB = parA + qd * T;
     if (threadIdx.x == 0) {
         const double rho = sqrt(0.75) * a.box->width / (1 << lc);
         rpow[0] = 1;
-        for (int k = 1; k <= p; ++k) rpow[k] = rpow[k - 1] * rho;
+        for (int k = 1; k <= p + 1; ++k) rpow[k] = rpow[k - 1] * rho;
     }
-    for (int t = threadIdx.x; t < 4 * (2 * p + 1); t += blockDim.x) phase[t] = a.eparent[t];
+    for (int t = threadIdx.x; t < 4 * (2 * p + 1); t += blockDim.x) ph[t] = a.eparent[t];
+    for (int t = threadIdx.x; t < 4 * (2 * p + 3); t += blockDim.x) ph1[t] = a.eparent1[t];
     __syncthreads();
     for (int64_t i = blockIdx.x * int64_t(nw) + w; i < cnt; i += int64_t(gridDim.x) * nw) {
         const int64_t g = off + i;
-        const int pg = a.parent[g];
-        const cplx* Lp = a.L + int64_t(pg) * KT;
-        for (int t = lane; t < KT; t += 32) par[t] = Lp[t];
+        const int64_t pg = a.parent[g];
+        if (a.want_pot)
+            for (int t = lane; t < qd * T; t += 32) parA[t] = a.LA[pg * qd * T + t];
+        if (a.want_field)
+            for (int t = lane; t < qd * T1; t += 32) parB[t] = a.LB[pg * qd * T1 + t];
         __syncwarp();
         const int oct = static_cast<int>(a.key[g] & 7);
-        cplx* Lc = a.L + g * KT;
-        for (int o = lane; o < KT; o += 32) {
-            const int k = o / T, t = o - k * T;
-            const cplx v = shift_output<false>(t, a.l2l_ptr, a.l2l_code, a.l2l_g, par + k * T, oct, rpow,
-                                               phase + (oct & 3) * (2 * p + 1), p);
-            Lc[o].re += v.re;
-            Lc[o].im += v.im;
-        }
+        if (a.want_pot)
+            for (int o = lane; o < qd * T; o += 32) {
+                const int b = o / T, t = o - b * T;
+                const cplx v = shift_output<false>(t, a.l2l_ptr, a.l2l_code, a.l2l_g, parA + b * T, oct, rpow,
+                                                   ph + (oct & 3) * (2 * p + 1), p);
+                cplx& d = a.LA[g * qd * T + o];
+                d.re += v.re;
+                d.im += v.im;
+            }
+        if (a.want_field)
+            for (int o = lane; o < qd * T1; o += 32) {
+                const int b = o / T1, t = o - b * T1;
+                const cplx v = shift_output<false>(t, a.l2l1_ptr, a.l2l1_code, a.l2l1_g, parB + b * T1, oct, rpow,
+                                                   ph1 + (oct & 3) * (2 * p + 3), p + 1);
+                cplx& d = a.LB[g * qd * T1 + o];
+                d.re += v.re;
+                d.im += v.im;
+            }
         __syncwarp();
     }
 }
 
-// L2P (fmm.hpp:747-771): warp per leaf of level >= 2, lanes over points.
+// L2P (fmm.hpp:747-771): warp per leaf of level >= 2.  The leaf's output
+// locals (potential: LA; field: minus grad of LB for scalar charges, curl
+// of LB for vector charges) are formed in shared memory, then lanes
+// evaluate them at the leaf's points.
 __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
 {
     extern __shared__ double smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int T = a.T, K = a.cs.K, KT = K * T;
-    cplx* loc = reinterpret_cast<cplx*>(smem) + w * KT;
+    const int T = a.T, T1 = a.T1, qd = a.qdim, K = a.K;
+    cplx* loc = reinterpret_cast<cplx*>(smem) + w * K * T;
     const int64_t nfar = a.n_leaves - a.far_leaf0;
     for (int64_t f = blockIdx.x * int64_t(nw) + w; f < nfar; f += int64_t(gridDim.x) * nw) {
-        const int g = a.leaf_node[a.far_leaf0 + f];
+        const int64_t g = a.leaf_node[a.far_leaf0 + f];
         const int l = level_of(a, g);
         double c[3];
         node_center(*a.box, a.key[g], l, c);
-        const cplx* Lg = a.L + int64_t(g) * KT;
-        for (int t = lane; t < KT; t += 32) loc[t] = Lg[t];
+        if (a.want_pot)
+            for (int t = lane; t < qd * T; t += 32) loc[t] = a.LA[g * qd * T + t];
+        if (a.want_field)
+            for (int t = lane; t < T; t += 32) {
+                int n, m;
+                tri_nm(t, n, m);
+                cplx G[3][3];
+                for (int b = 0; b < qd; ++b) grad_local(a.LB + (g * qd + b) * T1, n, m, &G[b][0], &G[b][1], &G[b][2]);
+                for (int ax = 0; ax < 3; ++ax) {
+                    cplx v;
+                    if (qd == 1) {
+                        v = cplx{-G[0][ax].re, -G[0][ax].im};
+                    } else {
+                        const int b1 = (ax + 1) % 3, c1 = (ax + 2) % 3;
+                        v = cplx{G[c1][b1].re - G[b1][c1].re, G[c1][b1].im - G[b1][c1].im};
+                    }
+                    loc[(a.kf + ax) * T + t] = v;
+                }
+            }
         __syncwarp();
         const int b0 = a.pbeg[g], b1 = a.pend[g];
         for (int i = b0 + lane; i < b1; i += 32) {
-            double u[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+            double u[6] = {0, 0, 0, 0, 0, 0};
             for_each_harmonic(a.p, a.fx[i] - c[0], a.fy[i] - c[1], a.fz[i] - c[2], c_harm, [&](int n, int m, cplx s) {
                 const int t = tri(n, m);
                 const double wt = m == 0 ? 1.0 : 2.0;
 #pragma unroll
-                for (int k = 0; k < 8; ++k)
+                for (int k = 0; k < 6; ++k)
                     if (k < K) u[k] += wt * (loc[k * T + t].re * s.re + loc[k * T + t].im * s.im);
             });
             for (int k = 0; k < K; ++k) a.out[int64_t(k) * a.n + i] += u[k];
@@ -314,65 +548,98 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
     }
 }
 
-// P2P (fmm.hpp:773-809): block per leaf, thread per target, source tiles
-// staged in shared memory from the leaf's near-field point ranges.
-constexpr int kP2PThreads = 64;
+// P2P (fmm.hpp:773-809): warp per target leaf.  Lanes are split into
+// (target, source slice) so leaves of ~20 points still use the whole warp;
+// sources are staged 32 at a time in shared memory from the leaf's
+// near-field point ranges; slices are summed in shared memory at the end.
+constexpr int kP2PWarps = 8;
 
-__global__ void __launch_bounds__(kP2PThreads) k_p2p(EvalArgs a)
+template<int QD, bool POT, bool FLD>
+__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(EvalArgs a)
 {
-    __shared__ double sx[kP2PThreads], sy[kP2PThreads], sz[kP2PThreads], sq[3][kP2PThreads];
-    const int64_t f = blockIdx.x;
-    const int g = a.leaf_node[f];
-    const int t0 = a.pbeg[g], t1 = a.pend[g];
-    const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
-    const int qd = a.qdim;
-    for (int tb = t0; tb < t1; tb += kP2PThreads) {
-        const int i = tb + threadIdx.x;
-        const bool on = i < t1;
-        const double xi = on ? a.px[i] : 0, yi = on ? a.py[i] : 0, zi = on ? a.pz[i] : 0;
-        double pot[3] = {0, 0, 0}, fld[3] = {0, 0, 0};
-        for (int r = r0; r < r1; ++r) {
-            const int2 rg = a.nr[r];
-            for (int sb = rg.x; sb < rg.y; sb += kP2PThreads) {
-                const int j = sb + threadIdx.x;
-                __syncthreads();
-                if (j < rg.y) {
-                    sx[threadIdx.x] = a.px[j];
-                    sy[threadIdx.x] = a.py[j];
-                    sz[threadIdx.x] = a.pz[j];
-                    for (int b = 0; b < qd; ++b) sq[b][threadIdx.x] = a.qs[b * a.n + j];
-                }
-                __syncthreads();
-                const int ns = min(kP2PThreads, rg.y - sb);
-                if (!on) continue;
-                for (int s = 0; s < ns; ++s) {
-                    if (sb + s == i) continue;
-                    const double dx = xi - sx[s], dy = yi - sy[s], dz = zi - sz[s];
-                    const double r2 = dx * dx + dy * dy + dz * dz;
-                    const double ir = 1.0 / sqrt(r2);
-                    if (a.cs.want_pot)
-                        for (int b = 0; b < qd; ++b) pot[b] += sq[b][s] * ir;
-                    if (a.cs.want_field) {
-                        const double ir3 = ir * ir * ir;
-                        if (qd == 1) {
-                            const double c = sq[0][s] * ir3;
-                            fld[0] += c * dx;
-                            fld[1] += c * dy;
-                            fld[2] += c * dz;
-                        } else {
-                            fld[0] += (sq[1][s] * dz - sq[2][s] * dy) * ir3;
-                            fld[1] += (sq[2][s] * dx - sq[0][s] * dz) * ir3;
-                            fld[2] += (sq[0][s] * dy - sq[1][s] * dx) * ir3;
+    constexpr int NV = 3 + QD;
+    __shared__ double tile[kP2PWarps][NV][32];
+    __shared__ double red[kP2PWarps][6][32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int64_t f = blockIdx.x * int64_t(kP2PWarps) + w; f < a.n_leaves; f += int64_t(gridDim.x) * kP2PWarps) {
+        const int g = a.leaf_node[f];
+        const int t0 = a.pbeg[g], t1 = a.pend[g];
+        const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
+        for (int tb = t0; tb < t1; tb += 32) {
+            const int ntc = min(32, t1 - tb);
+            const int lpt = max(1, 32 / ntc);
+            const int mt = lane / lpt, ms = lane - mt * lpt;
+            const bool on = mt < ntc;
+            const int i = tb + (on ? mt : 0);
+            const double xi = a.px[i], yi = a.py[i], zi = a.pz[i];
+            double pot[QD], fld[3] = {0, 0, 0};
+#pragma unroll
+            for (int b = 0; b < QD; ++b) pot[b] = 0;
+            for (int r = r0; r < r1; ++r) {
+                const int2 rg = a.nr[r];
+                for (int sb = rg.x; sb < rg.y; sb += 32) {
+                    const int j = sb + lane;
+                    if (j < rg.y) {
+                        tile[w][0][lane] = a.px[j];
+                        tile[w][1][lane] = a.py[j];
+                        tile[w][2][lane] = a.pz[j];
+#pragma unroll
+                        for (int b = 0; b < QD; ++b) tile[w][3 + b][lane] = a.qs[b * a.n + j];
+                    }
+                    __syncwarp();
+                    const int ns = min(32, rg.y - sb);
+                    if (on) {
+                        for (int k = ms; k < ns; k += lpt) {
+                            const double dx = xi - tile[w][0][k], dy = yi - tile[w][1][k], dz = zi - tile[w][2][k];
+                            const double r2 = dx * dx + dy * dy + dz * dz;
+                            const double ir = (sb + k == i) ? 0.0 : rsqrt(r2);
+                            if (POT) {
+#pragma unroll
+                                for (int b = 0; b < QD; ++b) pot[b] += tile[w][3 + b][k] * ir;
+                            }
+                            if (FLD) {
+                                const double ir3 = ir * ir * ir;
+                                if (QD == 1) {
+                                    const double cq = tile[w][3][k] * ir3;
+                                    fld[0] += cq * dx;
+                                    fld[1] += cq * dy;
+                                    fld[2] += cq * dz;
+                                } else {
+                                    const double q0 = tile[w][3][k], q1 = tile[w][3 + (QD > 1 ? 1 : 0)][k],
+                                                 q2 = tile[w][3 + (QD > 2 ? 2 : 0)][k];
+                                    fld[0] += (q1 * dz - q2 * dy) * ir3;
+                                    fld[1] += (q2 * dx - q0 * dz) * ir3;
+                                    fld[2] += (q0 * dy - q1 * dx) * ir3;
+                                }
+                            }
                         }
                     }
+                    __syncwarp();
                 }
             }
-        }
-        if (on) {
-            if (a.cs.want_pot)
-                for (int b = 0; b < qd; ++b) a.out2[int64_t(b) * a.n + i] = pot[b];
-            if (a.cs.want_field)
-                for (int c = 0; c < 3; ++c) a.out2[int64_t(a.cs.kf + c) * a.n + i] = fld[c];
+            // sum the slices of each target
+            int nv = 0;
+            if (POT)
+                for (int b = 0; b < QD; ++b) red[w][nv++][lane] = pot[b];
+            if (FLD)
+                for (int c = 0; c < 3; ++c) red[w][nv++][lane] = fld[c];
+            __syncwarp();
+            if (on && ms == 0) {
+                int v = 0;
+                if (POT)
+                    for (int b = 0; b < QD; ++b, ++v) {
+                        double s = 0;
+                        for (int k = 0; k < lpt; ++k) s += red[w][v][lane + k];
+                        a.out2[int64_t(b) * a.n + i] = s;
+                    }
+                if (FLD)
+                    for (int c = 0; c < 3; ++c, ++v) {
+                        double s = 0;
+                        for (int k = 0; k < lpt; ++k) s += red[w][v][lane + k];
+                        a.out2[int64_t(a.kf + c) * a.n + i] = s;
+                    }
+            }
+            __syncwarp();
         }
     }
 }
@@ -386,24 +653,46 @@ __global__ void k_finalize(EvalArgs a, double* __restrict__ pot, double* __restr
             for (int b = 0; b < a.qdim; ++b) pot[o * a.qdim + b] += a.out[b * a.n + i] + a.out2[b * a.n + i];
         if (field)
             for (int c = 0; c < 3; ++c)
-                field[o * 3 + c] += a.out[(a.cs.kf + c) * a.n + i] + a.out2[(a.cs.kf + c) * a.n + i];
+                field[o * 3 + c] += a.out[(a.kf + c) * a.n + i] + a.out2[(a.kf + c) * a.n + i];
     }
 }
 
-constexpr size_t kSmemBudget = 200 * 1024;
+size_t g_smem_optin = 227 * 1024;
 
 // Warps per block such that head + warps * per_warp shared bytes fits.
-int warps_for(size_t head, size_t per_warp)
+int warps_for(size_t head, size_t per_warp, int maxw = 4)
 {
-    int w = kMaxWarps;
-    while (w > 1 && head + per_warp * w > kSmemBudget) --w;
+    int w = maxw;
+    while (w > 1 && head + per_warp * w > g_smem_optin) --w;
     return w;
 }
 
 template<typename KernelT>
-void launch_cfg(KernelT k, int, size_t smem)
+void allow_smem(KernelT k, size_t smem)
 {
     SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+}
+
+template<int QD, bool POT, bool FLD>
+void launch_p2p(const EvalArgs& a, int sms, cudaStream_t st)
+{
+    k_p2p<QD, POT, FLD><<<blocks_for(a.n_leaves, kP2PWarps, int64_t(sms) * 16), kP2PWarps * 32, 0, st>>>(a);
+    SFMM_CHECK_LAUNCH();
+}
+
+void p2p_dispatch(const EvalArgs& a, int sms, cudaStream_t st)
+{
+    const int mode = (a.want_pot ? 1 : 0) | (a.want_field ? 2 : 0);
+#define SFMM_P2P(Q)                                                    \
+    if (a.qdim == Q) {                                                 \
+        if (mode == 1) return launch_p2p<Q, true, false>(a, sms, st);  \
+        if (mode == 2) return launch_p2p<Q, false, true>(a, sms, st);  \
+        return launch_p2p<Q, true, true>(a, sms, st);                  \
+    }
+    SFMM_P2P(1)
+    SFMM_P2P(2)
+    SFMM_P2P(3)
+#undef SFMM_P2P
 }
 
 }  // namespace
@@ -411,12 +700,30 @@ void launch_cfg(KernelT k, int, size_t smem)
 // ------------------------------------------------------------------ plan
 void upload_harm_coef(int device)
 {
+    static std::mutex mu;
     static bool done[64] = {false};
+    std::lock_guard<std::mutex> lk(mu);
     if (device >= 0 && device < 64 && done[device]) return;
     HarmCoef h;
     fill_harm_coef(h);
     SFMM_CUDA(cudaMemcpyToSymbol(c_harm, &h, sizeof(h)));
+    int v = 0;
+    if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device) == cudaSuccess && v > 0)
+        g_smem_optin = static_cast<size_t>(v);
     if (device >= 0 && device < 64) done[device] = true;
+}
+
+// Host tables depend on p only; built once per order and shared.
+static std::shared_ptr<const HostTables> tables_for(int p)
+{
+    static std::mutex mu;
+    static std::map<int, std::shared_ptr<const HostTables>> cache;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(p);
+    if (it != cache.end()) return it->second;
+    auto t = std::make_shared<const HostTables>(make_tables(p));
+    cache[p] = t;
+    return t;
 }
 
 template<typename T>
@@ -431,36 +738,44 @@ void plan_init(Plan& pl)
     Tree& t = *pl.tree;
     cudaStream_t st = t.ctx->stream;
     upload_harm_coef(t.ctx->device);
-    const HostTables tb = make_tables(pl.p);
-    pl.T = tb.T;
-    pl.rot_len = tb.rot_len;
-    pl.tz_len = static_cast<int>(tb.tz.size());
-    upload(pl.rot, tb.rot, st);
-    upload(pl.rot_off, tb.rot_off, st);
-    upload(pl.tz, tb.tz, st);
-    upload(pl.tz_off, tb.tz_off, st);
-    upload(pl.eil, tb.eil, st);
-    upload(pl.echild, tb.echild, st);
-    upload(pl.eparent, tb.eparent, st);
-    upload(pl.m2m_ptr, tb.m2m_ptr, st);
-    upload(pl.m2m_code, tb.m2m_code, st);
-    upload(pl.m2m_g, tb.m2m_g, st);
-    upload(pl.l2l_ptr, tb.l2l_ptr, st);
-    upload(pl.l2l_code, tb.l2l_code, st);
-    upload(pl.l2l_g, tb.l2l_g, st);
-    // rho^{-(k+1)} per (level, |d|^2), k = 0..2p, as fmm.hpp:629-633 forms them
-    std::vector<double> ipw(size_t(t.depth + 1) * 28 * (2 * pl.p + 2), 0.0);
+    const auto tb = tables_for(pl.p);
+    const auto tb1 = tables_for(pl.p + 1);
+    pl.T = tb->T;
+    pl.T1 = tb1->T;
+    pl.rot_len = tb1->rot_len;
+    pl.tzx_len = static_cast<int>(tb->tzx.size());
+    upload(pl.rot, tb1->rot, st);
+    upload(pl.rot_off, tb1->rot_off, st);
+    upload(pl.tzx, tb->tzx, st);
+    upload(pl.tzx_off, tb->tzx_off, st);
+    upload(pl.eil, tb1->eil, st);
+    upload(pl.echild, tb->echild, st);
+    upload(pl.eparent, tb->eparent, st);
+    upload(pl.eparent1, tb1->eparent, st);
+    upload(pl.m2m_ptr, tb->m2m_ptr, st);
+    upload(pl.m2m_code, tb->m2m_code, st);
+    upload(pl.m2m_g, tb->m2m_g, st);
+    upload(pl.l2l_ptr, tb->l2l_ptr, st);
+    upload(pl.l2l_code, tb->l2l_code, st);
+    upload(pl.l2l_g, tb->l2l_g, st);
+    upload(pl.l2l1_ptr, tb1->l2l_ptr, st);
+    upload(pl.l2l1_code, tb1->l2l_code, st);
+    upload(pl.l2l1_g, tb1->l2l_g, st);
+    // rho^{-(k+1)} per (level, |d|^2), k = 0..2p+2, formed as fmm.hpp:629-633 does
+    pl.ipow_w = 2 * pl.p + 3;
+    std::vector<double> ipw(size_t(t.depth + 1) * 28 * pl.ipow_w, 0.0);
     for (int l = 0; l <= t.depth; ++l)
         for (int d2 = 1; d2 < 28; ++d2) {
             const double rho = t.box.width / (1 << l) * std::sqrt(double(d2));
-            double* r = &ipw[(size_t(l) * 28 + d2) * (2 * pl.p + 2)];
+            double* r = &ipw[(size_t(l) * 28 + d2) * pl.ipow_w];
             r[0] = 1 / rho;
-            for (int k = 0; k < 2 * pl.p + 1; ++k) r[k + 1] = r[k] / rho;
+            for (int k = 0; k + 1 < pl.ipow_w; ++k) r[k + 1] = r[k] / rho;
         }
     upload(pl.ipow, ipw, st);
-    const int kmax = pl.qdim + 3;
     pl.M.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
-    pl.L.alloc(size_t(t.n_nodes) * kmax * pl.T, st);
+    pl.LA.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
+    pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
+    const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     pl.out.alloc(size_t(t.n) * kmax, st);
     pl.out2.alloc(size_t(t.n) * kmax, st);
@@ -498,82 +813,88 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.nr = t.nr.ptr;
     a.p = pl.p;
     a.T = pl.T;
+    a.T1 = pl.T1;
     a.qdim = pl.qdim;
-    a.cs.qdim = pl.qdim;
-    a.cs.want_pot = pot != nullptr;
-    a.cs.want_field = field != nullptr;
-    a.cs.kf = a.cs.want_pot ? pl.qdim : 0;
-    a.cs.K = a.cs.kf + (a.cs.want_field ? 3 : 0);
+    a.want_pot = pot != nullptr;
+    a.want_field = field != nullptr;
+    a.kf = a.want_pot ? pl.qdim : 0;
+    a.K = a.kf + (a.want_field ? 3 : 0);
     a.rot = pl.rot.ptr;
     a.rot_off = pl.rot_off.ptr;
     a.rot_len = pl.rot_len;
-    a.tz = pl.tz.ptr;
-    a.tz_off = pl.tz_off.ptr;
-    a.tz_len = pl.tz_len;
+    a.tzx = pl.tzx.ptr;
+    a.tzx_off = pl.tzx_off.ptr;
+    a.tzx_len = pl.tzx_len;
     a.eil = reinterpret_cast<const cplx*>(pl.eil.ptr);
     a.echild = reinterpret_cast<const cplx*>(pl.echild.ptr);
     a.eparent = reinterpret_cast<const cplx*>(pl.eparent.ptr);
+    a.eparent1 = reinterpret_cast<const cplx*>(pl.eparent1.ptr);
     a.m2m_ptr = pl.m2m_ptr.ptr;
     a.m2m_code = pl.m2m_code.ptr;
     a.m2m_g = pl.m2m_g.ptr;
     a.l2l_ptr = pl.l2l_ptr.ptr;
     a.l2l_code = pl.l2l_code.ptr;
     a.l2l_g = pl.l2l_g.ptr;
+    a.l2l1_ptr = pl.l2l1_ptr.ptr;
+    a.l2l1_code = pl.l2l1_code.ptr;
+    a.l2l1_g = pl.l2l1_g.ptr;
     a.ipow = pl.ipow.ptr;
+    a.ipow_w = pl.ipow_w;
     a.M = reinterpret_cast<cplx*>(pl.M.ptr);
-    a.L = reinterpret_cast<cplx*>(pl.L.ptr);
+    a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
+    a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);
     a.qs = pl.qs.ptr;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;
-    if (a.cs.K == 0) return;
-    SFMM_REQUIRE(!(a.cs.want_field && pl.qdim != 1 && pl.qdim != 3), FMM_ERR_UNSUPPORTED,
+    if (a.K == 0) return;
+    SFMM_REQUIRE(!(a.want_field && pl.qdim == 2), FMM_ERR_UNSUPPORTED,
                  "the field needs scalar (qdim 1) or vector (qdim 3) charges");
-    const int K = a.cs.K, T = pl.T;
+    const int K = a.K, T = pl.T, T1 = pl.T1, qd = pl.qdim;
     const int sms = t.ctx->sm_count;
 
     SFMM_CUDA(cudaEventRecord(pl.ev[0], st));
-    k_gather_q<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(Q, t.order.ptr, t.n, pl.qdim, pl.qs.ptr);
+    k_gather_q<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(Q, t.order.ptr, t.n, qd, pl.qs.ptr);
     SFMM_CHECK_LAUNCH();
     SFMM_CUDA(cudaMemsetAsync(pl.out.ptr, 0, size_t(t.n) * K * sizeof(double), st));
-    SFMM_CUDA(cudaMemsetAsync(pl.out2.ptr, 0, size_t(t.n) * K * sizeof(double), st));
     const bool far = t.depth >= 2;
     if (far) {
-        SFMM_CUDA(cudaMemsetAsync(pl.M.ptr, 0, size_t(t.n_nodes) * pl.qdim * T * sizeof(cplx), st));
         const int64_t nfar = t.n_leaves - a.far_leaf0;
-        const size_t head = (32 + 2 * 4 * (2 * kMaxOrder + 1)) * sizeof(double);
-        const size_t sm_p2m_w = size_t(pl.qdim) * T * sizeof(cplx);
+        const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx);
         const int w_p2m = warps_for(0, sm_p2m_w);
-        launch_cfg(k_p2m, w_p2m, sm_p2m_w * w_p2m);
+        allow_smem(k_p2m, sm_p2m_w * w_p2m);
         k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
         SFMM_CHECK_LAUNCH();
-        const size_t sm_m2m_w = 2 * size_t(pl.qdim) * T * sizeof(cplx);
+        const size_t head = (32 + 2 * 4 * (2 * kMaxOrder + 1)) * sizeof(double);
+        const size_t sm_m2m_w = 2 * size_t(qd) * T * sizeof(cplx);
         const int w_m2m = warps_for(head, sm_m2m_w);
-        launch_cfg(k_m2m, w_m2m, head + sm_m2m_w * w_m2m);
+        allow_smem(k_m2m, head + sm_m2m_w * w_m2m);
         for (int l = t.depth - 1; l >= 2; --l) {
             const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
             k_m2m<<<blocks_for(c, w_m2m, 65535), w_m2m * 32, head + sm_m2m_w * w_m2m, st>>>(a, l, t.lvl_off[l], c);
             SFMM_CHECK_LAUNCH();
         }
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
-        const size_t head_m2l = pl.tz_len * sizeof(double) + 49 * (pl.p + 1) * sizeof(cplx);
-        const size_t sm_m2l_w = size_t(3 * K * T + pl.qdim * T) * sizeof(cplx);
-        const int w_m2l = warps_for(head_m2l, sm_m2l_w);
-        launch_cfg(k_m2l, w_m2l, head_m2l + sm_m2l_w * w_m2l);
-        const int64_t c2 = t.n_nodes - t.lvl_off[2];
-        k_m2l<<<blocks_for(c2, w_m2l, int64_t(sms) * 64), w_m2l * 32, head_m2l + sm_m2l_w * w_m2l, st>>>(a, t.lvl_off[2], c2);
+        int w_m2l = kMaxWarps;
+        while (w_m2l > 1 && size_t(m2l_layout(pl.p, qd, w_m2l).total) > g_smem_optin) --w_m2l;
+        const size_t sm_m2l = m2l_layout(pl.p, qd, w_m2l).total;
+        SFMM_REQUIRE(sm_m2l <= g_smem_optin, FMM_ERR_UNSUPPORTED, "M2L working set exceeds shared memory");
+        allow_smem(k_m2l, sm_m2l);
+        const int64_t gcount = t.lvl_off[t.depth] - t.lvl_off[1];
+        k_m2l<<<blocks_for(gcount, 1, int64_t(sms) * 8), w_m2l * 32, sm_m2l, st>>>(a, t.lvl_off[1], t.lvl_off[t.depth]);
         SFMM_CHECK_LAUNCH();
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
-        const size_t sm_l2l_w = size_t(K) * T * sizeof(cplx);
-        const int w_l2l = warps_for(head, sm_l2l_w);
-        launch_cfg(k_l2l, w_l2l, head + sm_l2l_w * w_l2l);
+        const size_t head2 = (32 + 2 * 4 * (2 * kMaxOrder + 1) + 2 * 4 * (2 * kMaxOrder + 3)) * sizeof(double);
+        const size_t sm_l2l_w = size_t(qd) * (T + T1) * sizeof(cplx);
+        const int w_l2l = warps_for(head2, sm_l2l_w);
+        allow_smem(k_l2l, head2 + sm_l2l_w * w_l2l);
         for (int l = 3; l <= t.depth; ++l) {
             const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
-            k_l2l<<<blocks_for(c, w_l2l, 65535), w_l2l * 32, head + sm_l2l_w * w_l2l, st>>>(a, l, t.lvl_off[l], c);
+            k_l2l<<<blocks_for(c, w_l2l, 65535), w_l2l * 32, head2 + sm_l2l_w * w_l2l, st>>>(a, l, t.lvl_off[l], c);
             SFMM_CHECK_LAUNCH();
         }
         const size_t sm_l2p_w = size_t(K) * T * sizeof(cplx);
         const int w_l2p = warps_for(0, sm_l2p_w);
-        launch_cfg(k_l2p, w_l2p, sm_l2p_w * w_l2p);
+        allow_smem(k_l2p, sm_l2p_w * w_l2p);
         k_l2p<<<blocks_for(nfar, w_l2p, 65535), w_l2p * 32, sm_l2p_w * w_l2p, st>>>(a);
         SFMM_CHECK_LAUNCH();
     } else {
@@ -581,8 +902,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
     }
     SFMM_CUDA(cudaEventRecord(pl.ev[3], st));
-    k_p2p<<<static_cast<unsigned>(t.n_leaves), kP2PThreads, 0, st>>>(a);
-    SFMM_CHECK_LAUNCH();
+    p2p_dispatch(a, sms, st);
     SFMM_CUDA(cudaEventRecord(pl.ev[4], st));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
     SFMM_CHECK_LAUNCH();

@@ -6,6 +6,13 @@
 namespace sfmm {
 
 // Everything a kernel of one evaluation reads, passed by value.
+//
+// Far-field expansions per node and charge component b:
+//   M   plain multipoles of order p (P2M/M2M)
+//   LA  potential local of order p  (M2L of M, orders <= p)
+//   LB  field local of order p + 1  (M2L of M restricted to orders <= p - 1);
+//       the field at a target is minus its gradient (fmm_ops.cuh grad_local),
+//       which equals the reference's source-gradient moments term by term.
 struct EvalArgs {
     int64_t n;
     int depth;
@@ -19,22 +26,31 @@ struct EvalArgs {
     const int32_t *il_ptr, *il_src, *il_code;
     const int32_t* nr_ptr;
     const int2* nr;
-    int p, T, qdim;
-    CompSpec cs;
-    const double* rot;
+    int p, T, T1, qdim;
+    int want_pot, want_field;
+    int K;                                // output components: qdim (if pot) + 3 (if field)
+    int kf;                               // first field output component
+    const double* rot;                    // rotation classes up to order p + 1
     const int* rot_off;
     int rot_len;
-    const double* tz;
-    const int* tz_off;
-    int tz_len;
-    const cplx *eil, *echild, *eparent;
+    const double* tzx;                    // z-translation, target orders <= p+1, source orders <= p
+    const int* tzx_off;
+    int tzx_len;
+    const cplx* eil;                      // 49 x (p + 2)
+    const cplx* echild;                   // 4 x (2p + 1)
+    const cplx* eparent;                  // 4 x (2p + 1)
+    const cplx* eparent1;                 // 4 x (2p + 3)
     const int *m2m_ptr, *m2m_code;
     const double* m2m_g;
-    const int *l2l_ptr, *l2l_code;
+    const int *l2l_ptr, *l2l_code;        // order p
     const double* l2l_g;
-    const double* ipow;
+    const int *l2l1_ptr, *l2l1_code;      // order p + 1
+    const double* l2l1_g;
+    const double* ipow;                   // rho^{-(k+1)} per (level, |d|^2), k = 0..2p+2
+    int ipow_w;
     cplx* M;
-    cplx* L;
+    cplx* LA;
+    cplx* LB;
     const double* qs;
     double* out;                         // far field per component, sorted order
     double* out2;                        // near field per component, sorted order
@@ -42,11 +58,11 @@ struct EvalArgs {
 
 struct Plan {
     Tree* tree = nullptr;
-    int p = 0, T = 0, qdim = 1, precision = FMM_PRECISION_FP64;
-    int rot_len = 0, tz_len = 0;
-    DevBuf<double> rot, tz, eil, echild, eparent, m2m_g, l2l_g, ipow;
-    DevBuf<int> rot_off, tz_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code;
-    DevBuf<double2> M, L;
+    int p = 0, T = 0, T1 = 0, qdim = 1, precision = FMM_PRECISION_FP64;
+    int rot_len = 0, tzx_len = 0, ipow_w = 0;
+    DevBuf<double> rot, tzx, eil, echild, eparent, eparent1, m2m_g, l2l_g, l2l1_g, ipow;
+    DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
+    DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
     cudaEvent_t ev[6] = {};

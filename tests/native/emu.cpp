@@ -42,7 +42,7 @@ void ijk(int64_t k, int* o)
 extern "C" int emu_fmm(int depth, const int64_t* nnode, const int64_t* nleaf, void** keys, void** leafnode, void** idxp,
                        void** idxv, void** ilp, void** ilv, void** clp, void** clv, void** pl, void** nlp, void** nlv,
                        const double* box4, int va, double phideg, const double* pos, int64_t n, int p, int qdim,
-                       int want_pot, int want_field, const double* Q, double* pot, double* field)
+                       int want_pot, int want_field, const double* Q, double* pot, double* field, int split)
 {
     if (p < 0 || p > kMaxOrder) return -1;
     std::vector<Lv> L(depth + 1);
@@ -131,6 +131,158 @@ extern "C" int emu_fmm(int depth, const int64_t* nnode, const int64_t* nleaf, vo
                     }
                 }
         }
+        if (split) {
+            // Field through the order-(p+1) local B of the order-(p-1) moments
+            // (grad_local), sharing rotation and translation with the potential.
+            const HostTables tb1 = make_tables(p + 1);
+            const int T1 = tb1.T;
+            std::vector<std::vector<cplx>> LA(depth + 1), LB(depth + 1);
+            for (int l = 0; l <= depth; ++l) {
+                LA[l].assign(size_t(L[l].nn) * qdim * T, cplx{0, 0});
+                LB[l].assign(size_t(L[l].nn) * qdim * T1, cplx{0, 0});
+            }
+            std::vector<cplx> Mt(T), W(T), LzA(T), LzB(T1);
+            for (int l = 2; l <= depth; ++l)
+                for (int64_t it = 0; it < L[l].nn; ++it)
+                    for (int e = L[l].ilp[it]; e < L[l].ilp[it + 1]; ++e) {
+                        const int src = L[l].ilv[4 * e];
+                        const int di = L[l].ilv[4 * e + 1], dj = L[l].ilv[4 * e + 2], dk = L[l].ilv[4 * e + 3];
+                        const double rho = width / (1 << l) * std::sqrt(double(di * di + dj * dj + dk * dk));
+                        const double* R = tb1.rot.data() + size_t(rot_class(di, dj, dk)) * tb1.rot_len;
+                        const cplx* ph = &eil[(7 * (dj + 3) + (di + 3)) * (p + 1)];
+                        double ip[2 * kMaxOrder + 4];
+                        ip[0] = 1;
+                        for (int k = 1; k <= 2 * p + 3; ++k) ip[k] = ip[k - 1] / rho;
+                        for (int b = 0; b < qdim; ++b) {
+                            const cplx* Ms = &M[l][(size_t(src) * qdim + b) * T];
+                            for (int nn = 0; nn <= p; ++nn)
+                                for (int m = 0; m <= nn; ++m) Mt[tri(nn, m)] = cmul(ph[m], Ms[tri(nn, m)]);
+                            for (int nn = 0; nn <= p; ++nn) {
+                                const double* P = R + tb1.rot_off[nn];
+                                const double* Qm = P + (nn + 1) * (nn + 1);
+                                for (int a = 0; a <= nn; ++a) {
+                                    double re = 0, im = 0;
+                                    for (int bb = 0; bb <= nn; ++bb) {
+                                        re += P[a * (nn + 1) + bb] * Mt[tri(nn, bb)].re;
+                                        im += Qm[a * (nn + 1) + bb] * Mt[tri(nn, bb)].im;
+                                    }
+                                    W[tri(nn, a)] = {re * ip[nn], im * ip[nn]};
+                                }
+                            }
+                            for (int kk = 0; kk <= p + 1; ++kk) {
+                                const int w = p + 1 - kk;
+                                const double* tz = tb.tzx.data() + tb.tzx_off[kk];
+                                for (int j = kk; j <= p + 1; ++j) {
+                                    double re = 0, im = 0;
+                                    for (int nn = kk; nn <= p - 1; ++nn) {
+                                        re += tz[(j - kk) * w + (nn - kk)] * W[tri(nn, kk)].re;
+                                        im += tz[(j - kk) * w + (nn - kk)] * W[tri(nn, kk)].im;
+                                    }
+                                    LzB[tri(j, kk)] = {re * ip[j + 1], im * ip[j + 1]};
+                                    if (j <= p && kk <= p) {
+                                        const double c = tz[(j - kk) * w + (p - kk)];
+                                        LzA[tri(j, kk)] = {(re + c * W[tri(p, kk)].re) * ip[j + 1], (im + c * W[tri(p, kk)].im) * ip[j + 1]};
+                                    }
+                                }
+                            }
+                            auto back = [&](const std::vector<cplx>& Lz, int order, cplx* out) {
+                                for (int j = 0; j <= order; ++j) {
+                                    const int w = (j + 1) * (j + 1);
+                                    const double* PB = R + tb1.rot_off[j] + 2 * w;
+                                    const double* QB = PB + w;
+                                    for (int a = 0; a <= j; ++a) {
+                                        double re = 0, im = 0;
+                                        for (int bb = 0; bb <= j; ++bb) {
+                                            re += PB[a * (j + 1) + bb] * Lz[tri(j, bb)].re;
+                                            im += QB[a * (j + 1) + bb] * Lz[tri(j, bb)].im;
+                                        }
+                                        const cplx e2 = a <= p ? ph[a] : cmul(ph[a - 1], ph[1]);
+                                        const cplx v = cmul(cconj(e2), cplx{re, im});
+                                        out[tri(j, a)].re += v.re;
+                                        out[tri(j, a)].im += v.im;
+                                    }
+                                }
+                            };
+                            if (want_pot) back(LzA, p, &LA[l][(size_t(it) * qdim + b) * T]);
+                            if (want_field) back(LzB, p + 1, &LB[l][(size_t(it) * qdim + b) * T1]);
+                        }
+                    }
+            // L2L: A at order p, B at order p + 1
+            for (int l = 3; l <= depth; ++l) {
+                const double rho = std::sqrt(0.75) * width / (1 << l);
+                double rp[kMaxOrder + 2];
+                rp[0] = 1;
+                for (int k = 1; k <= p + 1; ++k) rp[k] = rp[k - 1] * rho;
+                std::vector<cplx> ep1(4 * (2 * p + 3));
+                for (size_t i = 0; i < ep1.size(); ++i) ep1[i] = {tb1.eparent[2 * i], tb1.eparent[2 * i + 1]};
+                for (int64_t ic = 0; ic < L[l].nn; ++ic) {
+                    const int ipar = int(L[l].pl[2 * ic]);
+                    const int oct = int(L[l].pl[2 * ic + 1] & 7);
+                    for (int b = 0; b < qdim; ++b) {
+                        const cplx* Ap = &LA[l - 1][(size_t(ipar) * qdim + b) * T];
+                        cplx* Ac = &LA[l][(size_t(ic) * qdim + b) * T];
+                        for (int o = 0; o < T; ++o) {
+                            const cplx v = shift_output<false>(o, tb.l2l_ptr.data(), tb.l2l_code.data(), tb.l2l_g.data(), Ap,
+                                                               oct, rp, &eparent[(oct & 3) * (2 * p + 1)], p);
+                            Ac[o].re += v.re;
+                            Ac[o].im += v.im;
+                        }
+                        const cplx* Bp = &LB[l - 1][(size_t(ipar) * qdim + b) * T1];
+                        cplx* Bc = &LB[l][(size_t(ic) * qdim + b) * T1];
+                        for (int o = 0; o < T1; ++o) {
+                            const cplx v = shift_output<false>(o, tb1.l2l_ptr.data(), tb1.l2l_code.data(), tb1.l2l_g.data(), Bp,
+                                                               oct, rp, &ep1[(oct & 3) * (2 * p + 3)], p + 1);
+                            Bc[o].re += v.re;
+                            Bc[o].im += v.im;
+                        }
+                    }
+                }
+            }
+            // L2P: potential from A, field from the gradient of B
+            std::vector<cplx> F(3 * T), G(3 * size_t(qdim) * T);
+            for (int l = 2; l <= depth; ++l)
+                for (int64_t f = 0; f < L[l].nl; ++f) {
+                    const int node = L[l].leaf[f];
+                    double c[3];
+                    center(l, L[l].keys[node], c);
+                    if (want_field) {
+                        for (int b = 0; b < qdim; ++b) {
+                            const cplx* Bn = &LB[l][(size_t(node) * qdim + b) * T1];
+                            for (int nn = 0; nn <= p; ++nn)
+                                for (int m = 0; m <= nn; ++m)
+                                    grad_local(Bn, nn, m, &G[(3 * b + 0) * T + tri(nn, m)], &G[(3 * b + 1) * T + tri(nn, m)],
+                                               &G[(3 * b + 2) * T + tri(nn, m)]);
+                        }
+                        for (int t = 0; t < T; ++t)
+                            for (int a = 0; a < 3; ++a) {
+                                if (qdim == 1) {
+                                    F[a * T + t] = {-G[a * T + t].re, -G[a * T + t].im};
+                                } else {
+                                    const int b1 = (a + 1) % 3, c1 = (a + 2) % 3;
+                                    const cplx x1 = G[(3 * c1 + b1) * T + t], x2 = G[(3 * b1 + c1) * T + t];
+                                    F[a * T + t] = {x1.re - x2.re, x1.im - x2.im};
+                                }
+                            }
+                    }
+                    const cplx* An = &LA[l][size_t(node) * qdim * T];
+                    for (int e = L[l].idxp[f]; e < L[l].idxp[f + 1]; ++e) {
+                        const int i = L[l].idxv[e];
+                        double r[3];
+                        rot(pos + 3 * size_t(i), r);
+                        double up[3] = {0, 0, 0}, uf[3] = {0, 0, 0};
+                        for_each_harmonic(p, r[0] - c[0], r[1] - c[1], r[2] - c[2], hc, [&](int nn, int m, cplx sv) {
+                            const double w = m == 0 ? 1.0 : 2.0;
+                            const int t = tri(nn, m);
+                            for (int b = 0; b < qdim; ++b) up[b] += w * (An[b * T + t].re * sv.re + An[b * T + t].im * sv.im);
+                            for (int a = 0; a < 3; ++a) uf[a] += w * (F[a * T + t].re * sv.re + F[a * T + t].im * sv.im);
+                        });
+                        if (want_pot)
+                            for (int b = 0; b < qdim; ++b) pot[size_t(i) * qdim + b] += up[b];
+                        if (want_field)
+                            for (int a = 0; a < 3; ++a) field[size_t(i) * 3 + a] += uf[a];
+                    }
+                }
+        } else {
         // M2L, levels 2 .. depth
         std::vector<cplx> Mt(T), W(T), Lz(T);
         for (int l = 2; l <= depth; ++l)
@@ -236,6 +388,7 @@ extern "C" int emu_fmm(int depth, const int64_t* nnode, const int64_t* nleaf, vo
                         for (int a = 0; a < 3; ++a) field[size_t(i) * 3 + a] += u[cs.kf + a];
                 }
             }
+        }
     }
     // P2P over the nlist (fmm.hpp:773-809)
     for (int l = 0; l <= depth; ++l)

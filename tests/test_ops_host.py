@@ -30,7 +30,7 @@ def emu(tmp_path_factory):
     return lib
 
 
-def run_emu(lib, dump, pos, Q, p, va=2, phideg=0.0, want_pot=True, want_field=True):
+def run_emu(lib, dump, pos, Q, p, va=2, phideg=0.0, want_pot=True, want_field=True, split=False):
     depth = int(dump["DEPTH"][0])
     keep = []
 
@@ -58,26 +58,34 @@ def run_emu(lib, dump, pos, Q, p, va=2, phideg=0.0, want_pot=True, want_field=Tr
                      ptrs("ILP", np.int32), ptrs("ILV", np.int32), ptrs("CLP", np.int32), ptrs("CLV", np.int64),
                      ptrs("PL", np.int64), ptrs("NLP", np.int32), ptrs("NLV", np.int32), dp(box), va,
                      C.c_double(phideg), dp(pos), C.c_int64(pos.shape[0]), p, qdim, int(want_pot), int(want_field),
-                     dp(Q), dp(pot), dp(field))
+                     dp(Q), dp(pot), dp(field), int(split))
     assert rc == 0
     return pot, field
 
 
+@pytest.mark.parametrize("split", [False, True])
 @pytest.mark.parametrize("name", ["uniform_n3000_p6", "plummer_n6000_p5_ppn32", "gauss2_n4000_p8",
                                   "uniform_n2500_p10_maxlevel3", "shell_n4000_p4_ppn16", "uniform_n400_p4_depth1"])
-def test_emulated_math_matches_reference(emu, name):
+def test_emulated_math_matches_reference(emu, name, split):
+    """split=False: field through source-gradient moments (grad_moment), the
+    reference's own formulation; split=True: the library's formulation, the
+    field as minus the gradient of the order-(p+1) local of the order-(p-1)
+    moments (grad_local), sharing rotation and translation with the potential."""
     g = load_golden(name)
     t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"])
-    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"], split=split)
     sp, sf = pyoracle.error_scales(g["pos"], g["q"])
     assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
     assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
 
 
-def test_emulated_vector_charges(emu):
+@pytest.mark.parametrize("split", [False, True])
+def test_emulated_vector_charges(emu, split):
+    """rinv (vector potential) and rinv<true> (Q x grad); in split form the
+    latter is the curl of the order-(p+1) vector local."""
     g = load_golden("vector_n2000_p8_ppn128")
     t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"])
-    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], g["p"], split=split)
     sp, sf = pyoracle.error_scales(g["pos"], g["q"])
     assert rel_err_per_target(pot, g["VECPOT"], sp) < 1e-12
     assert rel_err_per_target(field, g["BIOT"], sf) < 1e-12
@@ -94,10 +102,11 @@ def test_emulated_box_frames(emu, va, phideg):
     assert rel_err_per_target(pot, ref, sp) < 1e-12
 
 
-def test_emulated_p12_against_direct(emu):
+@pytest.mark.parametrize("split", [False, True])
+def test_emulated_p12(emu, split):
     g = load_golden("uniform_n3000_p12")
     t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"])
-    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], 12)
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], 12, split=split)
     sp, sf = pyoracle.error_scales(g["pos"], g["q"])
     assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
     assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
