@@ -23,6 +23,8 @@
  *  - The library keeps the tree, lists and expansions resident on the
  *    device; one context = one device + one stream.  Calls on one context
  *    are not re-entrant (like the reference's mutable _M/_L, fmm.hpp:178-179).
+ *  - Handles may be destroyed in any order: a tree keeps its context alive
+ *    and a plan keeps its tree alive until they are destroyed themselves.
  */
 #ifndef SIMPLEFMM_B200_H
 #define SIMPLEFMM_B200_H

@@ -1,5 +1,6 @@
 // C ABI of the library (include/simplefmm_b200.h).  Every entry point
 // converts exceptions to an fmm_status and records a per-thread message.
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <string>
@@ -16,16 +17,23 @@ namespace sfmm {
 
 }  // namespace sfmm
 
+// Handles are reference counted: a tree holds its context and a plan holds
+// its tree, so the caller may destroy them in any order (garbage-collected
+// bindings finalize objects in arbitrary order).
 struct fmm_context {
     sfmm::Context c;
+    std::atomic<int> refs{1};
 };
 
 struct fmm_tree {
     sfmm::Tree t;
+    fmm_context* owner = nullptr;
+    std::atomic<int> refs{1};
 };
 
 struct fmm_plan {
     sfmm::Plan pl;
+    fmm_tree* owner = nullptr;
 };
 
 namespace {
@@ -47,6 +55,24 @@ int fail(int status, const std::string& msg)
     return FMM_OK;
 
 void bind(const sfmm::Context& c) { SFMM_CUDA(cudaSetDevice(c.device)); }
+
+void release_context(fmm_context* ctx)
+{
+    if (!ctx || --ctx->refs > 0) return;
+    cudaSetDevice(ctx->c.device);
+    cudaStreamSynchronize(ctx->c.stream);
+    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+}
+
+void release_tree(fmm_tree* tree)
+{
+    if (!tree || --tree->refs > 0) return;
+    fmm_context* ctx = tree->owner;
+    cudaSetDevice(ctx->c.device);
+    delete tree;
+    release_context(ctx);
+}
 
 }  // namespace
 
@@ -102,11 +128,7 @@ int fmm_context_create(int device, fmm_context** out)
 int fmm_context_destroy(fmm_context* ctx)
 {
     API_TRY
-    if (!ctx) return FMM_OK;
-    bind(ctx->c);
-    SFMM_CUDA(cudaStreamSynchronize(ctx->c.stream));
-    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
-    delete ctx;
+    release_context(ctx);
     API_CATCH
 }
 
@@ -155,6 +177,8 @@ int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, in
     *out = nullptr;
     bind(ctx->c);
     auto* tr = new fmm_tree;
+    tr->owner = ctx;
+    ++ctx->refs;
     try {
         tr->t.ctx = &ctx->c;
         tr->t.n = n;
@@ -168,7 +192,7 @@ int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, in
         }
         sfmm::build_tree(tr->t, dxyz, max_level, max_ppn, vertical_axis, phideg);
     } catch (...) {
-        delete tr;
+        release_tree(tr);
         throw;
     }
     *out = tr;
@@ -178,9 +202,7 @@ int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, in
 int fmm_tree_destroy(fmm_tree* tree)
 {
     API_TRY
-    if (!tree) return FMM_OK;
-    bind(*tree->t.ctx);
-    delete tree;
+    release_tree(tree);
     API_CATCH
 }
 
@@ -238,6 +260,8 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
     if (precision != FMM_PRECISION_FP64) return fail(FMM_ERR_UNSUPPORTED, "only the FP64 precision is available");
     bind(*tree->t.ctx);
     auto* pl = new fmm_plan;
+    pl->owner = tree;
+    ++tree->refs;
     try {
         pl->pl.tree = &tree->t;
         pl->pl.p = p;
@@ -250,6 +274,7 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
         for (auto& e : pl->pl.ev)
             if (e) cudaEventDestroy(e);
         delete pl;
+        release_tree(tree);
         throw;
     }
     *out = pl;
@@ -264,7 +289,9 @@ int fmm_plan_destroy(fmm_plan* plan)
     SFMM_CUDA(cudaStreamSynchronize(plan->pl.tree->ctx->stream));
     for (auto& e : plan->pl.ev)
         if (e) cudaEventDestroy(e);
+    fmm_tree* owner = plan->owner;
     delete plan;
+    release_tree(owner);
     API_CATCH
 }
 

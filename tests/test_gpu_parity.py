@@ -160,3 +160,29 @@ def test_invalid_arguments(ctx):
     with pytest.raises(sf.FMMError) as e:
         p1.rinv(np.zeros(1000), np.zeros((1000, 3)), gradient=True)
     assert e.value.status == 2
+
+
+@pytest.mark.parametrize("order", ["ctx-tree-plan", "plan-ctx-tree", "tree-plan-ctx", "ctx-plan-tree"])
+def test_handles_destroyed_in_any_order(order):
+    """A plan keeps its tree and a tree its context alive (reference counts),
+    so bindings that finalize objects in arbitrary order stay safe."""
+    import ctypes as C
+
+    L = sf.load_library()
+    ctx, tree, plan = C.c_void_p(), C.c_void_p(), C.c_void_p()
+    pos = np.ascontiguousarray(W.uniform_cube(5000, 9))
+    q = W.charges(5000, 9)
+    assert L.fmm_context_create(0, C.byref(ctx)) == 0
+    assert L.fmm_tree_build(ctx, C.c_void_p(pos.ctypes.data), 5000, 0, 20, 64, 2, 0.0, C.byref(tree)) == 0
+    assert L.fmm_plan_create(tree, 6, 1, 0, C.byref(plan)) == 0
+    handles = {"ctx": (L.fmm_context_destroy, ctx), "tree": (L.fmm_tree_destroy, tree), "plan": (L.fmm_plan_destroy, plan)}
+    first = order.split("-")[0]
+    fn, h = handles.pop(first)
+    assert fn(h) == 0
+    if first != "plan":
+        U = np.zeros(5000)
+        assert L.fmm_rinv(plan, C.c_void_p(q.ctypes.data), C.c_void_p(U.ctypes.data), 0, 0) == 0
+        assert np.isfinite(U).all() and np.abs(U).max() > 0
+    for name in order.split("-")[1:]:
+        fn, h = handles[name]
+        assert fn(h) == 0
