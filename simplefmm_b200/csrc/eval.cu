@@ -19,7 +19,7 @@
 #include <memory>
 #include <mutex>
 
-#include "fmm_eval.cuh"
+#include "eval_util.cuh"
 #include "fmm_tables.h"
 
 namespace sfmm {
@@ -29,41 +29,6 @@ __constant__ HarmCoef c_harm;
 namespace {
 
 constexpr int kMaxWarps = 8;
-constexpr int kCols = 4;                  // M2L columns (pair x charge component) per warp chunk
-constexpr int kMaxGroupPairs = 8 * 189;   // <= 8 siblings x n_ilist_max (partition.hpp:149)
-constexpr int kNumClasses = 70;           // rotation classes (fmm.hpp:169)
-
-__device__ __forceinline__ int level_of(const EvalArgs& a, int64_t g)
-{
-    int l = 0;
-    while (l < a.depth && g >= a.lvl_off[l + 1]) ++l;
-    return l;
-}
-
-// box.hpp:147-150
-__device__ __forceinline__ void node_center(const BoxDev& b, uint64_t key, int l, double* c)
-{
-    const uint32_t ix = compact3(key), iy = compact3(key >> 1), iz = compact3(key >> 2);
-    const double s = double(1 << l);
-    c[0] = b.corner[0] + b.width * ((ix + 0.5) / s);
-    c[1] = b.corner[1] + b.width * ((iy + 0.5) / s);
-    c[2] = b.corner[2] + b.width * ((iz + 0.5) / s);
-}
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__device__ __forceinline__ void tri_nm(int t, int& n, int& m)
-{
-    n = static_cast<int>((sqrtf(8.0f * t + 1.0f) - 1.0f) * 0.5f);
-    if ((n + 1) * (n + 2) / 2 <= t) ++n;
-    if (n * (n + 1) / 2 > t) --n;
-    m = t - n * (n + 1) / 2;
-}
 
 __global__ void k_gather_q(const double* __restrict__ Q, const int32_t* __restrict__ order, int64_t n, int qdim,
                            double* __restrict__ qs)
@@ -155,293 +120,6 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_m2m(EvalArgs a, int lp, int6
         }
         for (int o = lane; o < a.qdim * T; o += 32) M[o] = accs[o];
         __syncwarp();
-    }
-}
-
-// ------------------------------------------------------------------ M2L
-// Shared-memory plan of k_m2l (same arithmetic on host and device).
-struct M2LLayout {
-    int ent_src, ent_code, cls, sorted, cls_cnt, cls_off, chunk_off, colinfo, eil, accA, accB, warps, total;
-    int per_warp;
-};
-
-__host__ __device__ inline int align16(int x) { return (x + 15) & ~15; }
-
-__host__ __device__ inline M2LLayout m2l_layout(int p, int qdim, int warps)
-{
-    const int T = (p + 1) * (p + 2) / 2, T1 = (p + 2) * (p + 3) / 2;
-    M2LLayout L;
-    int o = 0;
-    L.ent_src = o; o = align16(o + 4 * kMaxGroupPairs);
-    L.ent_code = o; o = align16(o + 4 * kMaxGroupPairs);
-    L.cls = o; o = align16(o + 4 * kMaxGroupPairs);
-    L.sorted = o; o = align16(o + 4 * kMaxGroupPairs);
-    L.cls_cnt = o; o = align16(o + 4 * 72);
-    L.cls_off = o; o = align16(o + 4 * 72);
-    L.chunk_off = o; o = align16(o + 4 * 72);
-    L.colinfo = o; o = align16(o + 4 * kMaxWarps * kCols);
-    L.eil = o; o = align16(o + 16 * 49 * (p + 2));
-    L.accA = o; o = align16(o + 16 * 8 * qdim * T);
-    L.accB = o; o = align16(o + 16 * 8 * qdim * T1);
-    L.per_warp = align16(16 * 4 * kCols * T1);
-    L.warps = warps;
-    L.total = o + warps * L.per_warp;
-    return L;
-}
-
-// M2L (fmm.hpp:620-712): one block per sibling group (the children of one
-// node), all their interaction pairs sorted by rotation class and processed
-// in chunks of kCols same-class columns per warp, so every rotation-matrix
-// element read feeds kCols pairs.  Per chunk: phase + rotate (P/Q), split
-// z-translation into LA (orders <= p) and LB (orders <= p+1, sources <= p-1),
-// inverse rotation (PB/QB) + phase.  Warp outputs are added to per-target
-// shared accumulators in a fixed order after every round, and each target's
-// locals are stored once.
-__global__ void __launch_bounds__(kMaxWarps * 32) k_m2l(EvalArgs a, int64_t g0, int64_t g1)
-{
-    extern __shared__ __align__(16) unsigned char sm[];
-    const int nw = blockDim.x >> 5, w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int p = a.p, T = a.T, T1 = a.T1, qd = a.qdim;
-    const M2LLayout Ly = m2l_layout(p, qd, nw);
-    int* ent_src = reinterpret_cast<int*>(sm + Ly.ent_src);
-    int* ent_code = reinterpret_cast<int*>(sm + Ly.ent_code);
-    int* cls = reinterpret_cast<int*>(sm + Ly.cls);
-    int* sorted = reinterpret_cast<int*>(sm + Ly.sorted);
-    int* cls_cnt = reinterpret_cast<int*>(sm + Ly.cls_cnt);
-    int* cls_off = reinterpret_cast<int*>(sm + Ly.cls_off);
-    int* chunk_off = reinterpret_cast<int*>(sm + Ly.chunk_off);
-    int* colinfo = reinterpret_cast<int*>(sm + Ly.colinfo);
-    cplx* eil = reinterpret_cast<cplx*>(sm + Ly.eil);
-    cplx* accA = reinterpret_cast<cplx*>(sm + Ly.accA);
-    cplx* accB = reinterpret_cast<cplx*>(sm + Ly.accB);
-    cplx* X = reinterpret_cast<cplx*>(sm + Ly.total - (nw - w) * Ly.per_warp);
-    cplx* Y = X + kCols * T1;
-    cplx* Z = Y + kCols * T1;
-    cplx* O = Z + kCols * T1;
-
-    for (int t = threadIdx.x; t < 49 * (p + 2); t += blockDim.x) eil[t] = a.eil[t];
-    __syncthreads();
-
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
-        const int nc = a.nchild[g];
-        if (nc == 0) continue;
-        const int cb = a.child_beg[g];
-        const int l = level_of(a, g) + 1;                       // level of the targets
-        const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
-        // ---- gather the group's pairs, classify
-        for (int s = 0; s < nc; ++s) {
-            const int r0 = a.il_ptr[cb + s] - e0, r1 = a.il_ptr[cb + s + 1] - e0;
-            for (int e = r0 + threadIdx.x; e < r1; e += blockDim.x) {
-                const int code = a.il_code[e0 + e];
-                ent_src[e] = a.il_src[e0 + e];
-                ent_code[e] = code | (s << 9);
-                cls[e] = rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3);
-            }
-        }
-        for (int t = threadIdx.x; t < 8 * qd * T; t += blockDim.x) accA[t] = cplx{0, 0};
-        for (int t = threadIdx.x; t < 8 * qd * T1; t += blockDim.x) accB[t] = cplx{0, 0};
-        __syncthreads();
-        // stable counting sort by class: thread c collects class c in order
-        if (threadIdx.x < kNumClasses) {
-            int cnt = 0;
-            for (int e = 0; e < E; ++e) cnt += cls[e] == int(threadIdx.x);
-            cls_cnt[threadIdx.x] = cnt;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int s = 0, k = 0;
-            for (int c = 0; c < kNumClasses; ++c) {
-                cls_off[c] = s;
-                chunk_off[c] = k;
-                s += cls_cnt[c];
-                k += (cls_cnt[c] * qd + kCols - 1) / kCols;
-            }
-            cls_off[kNumClasses] = s;
-            chunk_off[kNumClasses] = k;
-        }
-        __syncthreads();
-        if (threadIdx.x < kNumClasses) {
-            int pos = cls_off[threadIdx.x];
-            for (int e = 0; e < E; ++e)
-                if (cls[e] == int(threadIdx.x)) sorted[pos++] = e;
-        }
-        __syncthreads();
-        const int nchunk = chunk_off[kNumClasses];
-        for (int r0 = 0; r0 < nchunk; r0 += nw) {
-            const int k = r0 + w;
-            if (k < nchunk) {
-                // ---- locate the chunk
-                int c = 0;
-                while (chunk_off[c + 1] <= k) ++c;
-                const int col0 = (k - chunk_off[c]) * kCols;
-                const int ncols_c = cls_cnt[c] * qd;
-                const int ncol = min(kCols, ncols_c - col0);
-                int src[kCols], bq[kCols], pidx[kCols];
-                int dsq = 0;
-#pragma unroll
-                for (int cc = 0; cc < kCols; ++cc) {
-                    src[cc] = 0;
-                    bq[cc] = 0;
-                    pidx[cc] = 24;
-                    if (cc < ncol) {
-                        const int col = col0 + cc;
-                        const int e = sorted[cls_off[c] + col / qd];
-                        const int code = ent_code[e];
-                        const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
-                        src[cc] = ent_src[e];
-                        bq[cc] = col % qd;
-                        pidx[cc] = 7 * (dj + 3) + (di + 3);
-                        dsq = di * di + dj * dj + dk * dk;
-                        if (lane == 0) colinfo[w * kCols + cc] = ((code >> 9) & 7) * 8 + bq[cc];
-                    } else if (lane == 0) {
-                        colinfo[w * kCols + cc] = -1;
-                    }
-                }
-                const double* R = a.rot + int64_t(c) * a.rot_len;
-                const double* ipw = a.ipow + (int64_t(l) * 28 + dsq) * a.ipow_w;
-                // (a) phase: X = e^{i m phi} M
-#pragma unroll
-                for (int cc = 0; cc < kCols; ++cc) {
-                    if (cc < ncol) {
-                        const cplx* Ms = a.M + (int64_t(src[cc]) * qd + bq[cc]) * T;
-                        const cplx* ph = eil + pidx[cc] * (p + 2);
-                        for (int t = lane; t < T; t += 32) {
-                            int n, m;
-                            tri_nm(t, n, m);
-                            X[cc * T1 + t] = cmul(ph[m], Ms[t]);
-                        }
-                    } else {
-                        for (int t = lane; t < T; t += 32) X[cc * T1 + t] = cplx{0, 0};
-                    }
-                }
-                __syncwarp();
-                // (b) rotation: Y_n = (P_n Re X_n, Q_n Im X_n) rho^{-n}
-                for (int r = lane; r < T; r += 32) {
-                    int n, aa;
-                    tri_nm(r, n, aa);
-                    const double* P = R + a.rot_off[n] + aa * (n + 1);
-                    const double* Qm = P + (n + 1) * (n + 1);
-                    const int base = n * (n + 1) / 2;
-                    double re[kCols], im[kCols];
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) re[cc] = im[cc] = 0;
-                    for (int b = 0; b <= n; ++b) {
-                        const double pb = __ldg(P + b), qb = __ldg(Qm + b);
-#pragma unroll
-                        for (int cc = 0; cc < kCols; ++cc) {
-                            const cplx x = X[cc * T1 + base + b];
-                            re[cc] += pb * x.re;
-                            im[cc] += qb * x.im;
-                        }
-                    }
-                    const double sc = n ? ipw[n - 1] : 1.0;
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) Y[cc * T1 + r] = cplx{re[cc] * sc, im[cc] * sc};
-                }
-                __syncwarp();
-                // (c) z-translation: Z = LB (sources n <= p-1, targets j <= p+1), X = LA
-                for (int r = lane; r < T1; r += 32) {
-                    int j, kk;
-                    tri_nm(r, j, kk);
-                    const int wd = p + 1 - kk;
-                    const double* row = a.tzx + a.tzx_off[kk] + (j - kk) * wd;
-                    double bre[kCols], bim[kCols];
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) bre[cc] = bim[cc] = 0;
-                    for (int n = kk; n <= p - 1; ++n) {
-                        const double tv = __ldg(row + n - kk);
-                        const int tn = n * (n + 1) / 2 + kk;
-#pragma unroll
-                        for (int cc = 0; cc < kCols; ++cc) {
-                            const cplx y = Y[cc * T1 + tn];
-                            bre[cc] += tv * y.re;
-                            bim[cc] += tv * y.im;
-                        }
-                    }
-                    const double sc = ipw[j];
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) Z[cc * T1 + r] = cplx{bre[cc] * sc, bim[cc] * sc};
-                    if (j <= p) {
-                        const double tv = __ldg(row + p - kk);
-                        const int tn = p * (p + 1) / 2 + kk;
-#pragma unroll
-                        for (int cc = 0; cc < kCols; ++cc) {
-                            const cplx y = Y[cc * T1 + tn];
-                            X[cc * T1 + r] = cplx{(bre[cc] + tv * y.re) * sc, (bim[cc] + tv * y.im) * sc};
-                        }
-                    }
-                }
-                __syncwarp();
-                // (d) inverse rotation + phase: Y = LA contribution, O = LB contribution
-                for (int r = lane; r < T1; r += 32) {
-                    int j, aa;
-                    tri_nm(r, j, aa);
-                    const int wd = (j + 1) * (j + 1);
-                    const double* PB = R + a.rot_off[j] + 2 * wd + aa * (j + 1);
-                    const double* QB = PB + wd;
-                    const int base = j * (j + 1) / 2;
-                    const bool doA = a.want_pot && j <= p;
-                    double are[kCols], aim[kCols], bre[kCols], bim[kCols];
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) are[cc] = aim[cc] = bre[cc] = bim[cc] = 0;
-                    for (int b = 0; b <= j; ++b) {
-                        const double pb = __ldg(PB + b), qb = __ldg(QB + b);
-#pragma unroll
-                        for (int cc = 0; cc < kCols; ++cc) {
-                            if (a.want_field) {
-                                const cplx z = Z[cc * T1 + base + b];
-                                bre[cc] += pb * z.re;
-                                bim[cc] += qb * z.im;
-                            }
-                            if (doA) {
-                                const cplx x = X[cc * T1 + base + b];
-                                are[cc] += pb * x.re;
-                                aim[cc] += qb * x.im;
-                            }
-                        }
-                    }
-#pragma unroll
-                    for (int cc = 0; cc < kCols; ++cc) {
-                        const cplx e = cconj(eil[pidx[cc] * (p + 2) + aa]);
-                        if (a.want_field) O[cc * T1 + r] = cmul(e, cplx{bre[cc], bim[cc]});
-                        if (doA) Y[cc * T1 + r] = cmul(e, cplx{are[cc], aim[cc]});
-                    }
-                }
-            } else if (lane < kCols) {
-                colinfo[w * kCols + lane] = -1;
-            }
-            __syncthreads();
-            // ---- fixed-order accumulation of this round's warp outputs
-            const int nA = a.want_pot ? nc * qd * T : 0;
-            const int nB = a.want_field ? nc * qd * T1 : 0;
-            for (int e = threadIdx.x; e < nA + nB; e += blockDim.x) {
-                const bool isA = e < nA;
-                const int ee = isA ? e : e - nA;
-                const int TT = isA ? T : T1;
-                const int sb = ee / TT, t = ee - sb * TT;      // sb = slot * qd + b
-                const int tag = (sb / qd) * 8 + sb % qd;
-                cplx s{0, 0};
-                for (int ww = 0; ww < nw; ++ww) {
-                    const cplx* Xw = reinterpret_cast<const cplx*>(sm + Ly.total - (nw - ww) * Ly.per_warp);
-                    const cplx* src_buf = isA ? Xw + kCols * T1 : Xw + 3 * kCols * T1;
-                    for (int cc = 0; cc < kCols; ++cc)
-                        if (colinfo[ww * kCols + cc] == tag) {
-                            s.re += src_buf[cc * T1 + t].re;
-                            s.im += src_buf[cc * T1 + t].im;
-                        }
-                }
-                cplx* acc = isA ? accA : accB;
-                acc[ee].re += s.re;
-                acc[ee].im += s.im;
-            }
-            __syncthreads();
-        }
-        // ---- store the group's locals (M2L is their first contribution)
-        if (a.want_pot)
-            for (int e = threadIdx.x; e < nc * qd * T; e += blockDim.x) a.LA[int64_t(cb) * qd * T + e] = accA[e];
-        if (a.want_field)
-            for (int e = threadIdx.x; e < nc * qd * T1; e += blockDim.x) a.LB[int64_t(cb) * qd * T1 + e] = accB[e];
-        __syncthreads();
     }
 }
 
@@ -874,14 +552,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
             SFMM_CHECK_LAUNCH();
         }
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
-        int w_m2l = kMaxWarps;
-        while (w_m2l > 1 && size_t(m2l_layout(pl.p, qd, w_m2l).total) > g_smem_optin) --w_m2l;
-        const size_t sm_m2l = m2l_layout(pl.p, qd, w_m2l).total;
-        SFMM_REQUIRE(sm_m2l <= g_smem_optin, FMM_ERR_UNSUPPORTED, "M2L working set exceeds shared memory");
-        allow_smem(k_m2l, sm_m2l);
-        const int64_t gcount = t.lvl_off[t.depth] - t.lvl_off[1];
-        k_m2l<<<blocks_for(gcount, 1, int64_t(sms) * 8), w_m2l * 32, sm_m2l, st>>>(a, t.lvl_off[1], t.lvl_off[t.depth]);
-        SFMM_CHECK_LAUNCH();
+        launch_m2l(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
         const size_t head2 = (32 + 2 * 4 * (2 * kMaxOrder + 1) + 2 * 4 * (2 * kMaxOrder + 3)) * sizeof(double);
         const size_t sm_l2l_w = size_t(qd) * (T + T1) * sizeof(cplx);
