@@ -133,10 +133,10 @@ __global__ void __launch_bounds__(RowCfg<P>::NT) k_m2l_rows(EvalArgs a, int64_t 
         for (int t = r; t < 8 * qd * T1; t += nt) accB[t] = cplx{0, 0};
         __syncthreads();
         // stable counting sort by class (thread c gathers class c in order)
-        if (r < kNumClasses) {
+        for (int cl = r; cl < kNumClasses; cl += nt) {    // blocks may be narrower than 70 threads
             int cnt = 0;
-            for (int e = 0; e < E; ++e) cnt += cls[e] == r;
-            cls_cnt[r] = cnt;
+            for (int e = 0; e < E; ++e) cnt += cls[e] == cl;
+            cls_cnt[cl] = cnt;
         }
         __syncthreads();
         if (r == 0) {
@@ -151,10 +151,10 @@ __global__ void __launch_bounds__(RowCfg<P>::NT) k_m2l_rows(EvalArgs a, int64_t 
             bat_off[kNumClasses] = k;
         }
         __syncthreads();
-        if (r < kNumClasses) {
-            int pos = cls_off[r];
+        for (int cl = r; cl < kNumClasses; cl += nt) {
+            int pos = cls_off[cl];
             for (int e = 0; e < E; ++e)
-                if (cls[e] == r) sorted[pos++] = static_cast<short>(e);
+                if (cls[e] == cl) sorted[pos++] = static_cast<short>(e);
         }
         __syncthreads();
         const int nbat = bat_off[kNumClasses];
