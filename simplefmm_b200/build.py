@@ -39,7 +39,7 @@ def _sources():
 
 
 def _headers():
-    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(INCLUDE.glob("*.h"))
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + list(INCLUDE.glob("*.h"))
 
 
 def build(verbose: bool = False, extra_flags=None) -> Path:

@@ -112,10 +112,7 @@ int fmm_context_create(int device, fmm_context** out)
         SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         ctx->c.own_stream = true;
         SFMM_CUDA(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
-        cudaMemPool_t pool;
-        SFMM_CUDA(cudaDeviceGetDefaultMemPool(&pool, device));
-        uint64_t thr = UINT64_MAX;
-        SFMM_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+        (void)sfmm::device_pool(device);
     } catch (...) {
         if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;

@@ -226,102 +226,6 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
     }
 }
 
-// P2P (fmm.hpp:773-809): warp per target leaf.  Lanes are split into
-// (target, source slice) so leaves of ~20 points still use the whole warp;
-// sources are staged 32 at a time in shared memory from the leaf's
-// near-field point ranges; slices are summed in shared memory at the end.
-constexpr int kP2PWarps = 8;
-
-template<int QD, bool POT, bool FLD>
-__global__ void __launch_bounds__(kP2PWarps * 32) k_p2p(EvalArgs a)
-{
-    constexpr int NV = 3 + QD;
-    __shared__ double tile[kP2PWarps][NV][32];
-    __shared__ double red[kP2PWarps][6][32];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int64_t f = blockIdx.x * int64_t(kP2PWarps) + w; f < a.n_leaves; f += int64_t(gridDim.x) * kP2PWarps) {
-        const int g = a.leaf_node[f];
-        const int t0 = a.pbeg[g], t1 = a.pend[g];
-        const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
-        for (int tb = t0; tb < t1; tb += 32) {
-            const int ntc = min(32, t1 - tb);
-            const int lpt = max(1, 32 / ntc);
-            const int mt = lane / lpt, ms = lane - mt * lpt;
-            const bool on = mt < ntc;
-            const int i = tb + (on ? mt : 0);
-            const double xi = a.px[i], yi = a.py[i], zi = a.pz[i];
-            double pot[QD], fld[3] = {0, 0, 0};
-#pragma unroll
-            for (int b = 0; b < QD; ++b) pot[b] = 0;
-            for (int r = r0; r < r1; ++r) {
-                const int2 rg = a.nr[r];
-                for (int sb = rg.x; sb < rg.y; sb += 32) {
-                    const int j = sb + lane;
-                    if (j < rg.y) {
-                        tile[w][0][lane] = a.px[j];
-                        tile[w][1][lane] = a.py[j];
-                        tile[w][2][lane] = a.pz[j];
-#pragma unroll
-                        for (int b = 0; b < QD; ++b) tile[w][3 + b][lane] = a.qs[b * a.n + j];
-                    }
-                    __syncwarp();
-                    const int ns = min(32, rg.y - sb);
-                    if (on) {
-                        for (int k = ms; k < ns; k += lpt) {
-                            const double dx = xi - tile[w][0][k], dy = yi - tile[w][1][k], dz = zi - tile[w][2][k];
-                            const double r2 = dx * dx + dy * dy + dz * dz;
-                            const double ir = (sb + k == i) ? 0.0 : rsqrt(r2);
-                            if (POT) {
-#pragma unroll
-                                for (int b = 0; b < QD; ++b) pot[b] += tile[w][3 + b][k] * ir;
-                            }
-                            if (FLD) {
-                                const double ir3 = ir * ir * ir;
-                                if (QD == 1) {
-                                    const double cq = tile[w][3][k] * ir3;
-                                    fld[0] += cq * dx;
-                                    fld[1] += cq * dy;
-                                    fld[2] += cq * dz;
-                                } else {
-                                    const double q0 = tile[w][3][k], q1 = tile[w][3 + (QD > 1 ? 1 : 0)][k],
-                                                 q2 = tile[w][3 + (QD > 2 ? 2 : 0)][k];
-                                    fld[0] += (q1 * dz - q2 * dy) * ir3;
-                                    fld[1] += (q2 * dx - q0 * dz) * ir3;
-                                    fld[2] += (q0 * dy - q1 * dx) * ir3;
-                                }
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-            }
-            // sum the slices of each target
-            int nv = 0;
-            if (POT)
-                for (int b = 0; b < QD; ++b) red[w][nv++][lane] = pot[b];
-            if (FLD)
-                for (int c = 0; c < 3; ++c) red[w][nv++][lane] = fld[c];
-            __syncwarp();
-            if (on && ms == 0) {
-                int v = 0;
-                if (POT)
-                    for (int b = 0; b < QD; ++b, ++v) {
-                        double s = 0;
-                        for (int k = 0; k < lpt; ++k) s += red[w][v][lane + k];
-                        a.out2[int64_t(b) * a.n + i] = s;
-                    }
-                if (FLD)
-                    for (int c = 0; c < 3; ++c, ++v) {
-                        double s = 0;
-                        for (int k = 0; k < lpt; ++k) s += red[w][v][lane + k];
-                        a.out2[int64_t(a.kf + c) * a.n + i] = s;
-                    }
-            }
-            __syncwarp();
-        }
-    }
-}
-
 // U += far + near, back in the caller's point order.
 __global__ void k_finalize(EvalArgs a, double* __restrict__ pot, double* __restrict__ field)
 {
@@ -349,28 +253,6 @@ template<typename KernelT>
 void allow_smem(KernelT k, size_t smem)
 {
     SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-}
-
-template<int QD, bool POT, bool FLD>
-void launch_p2p(const EvalArgs& a, int sms, cudaStream_t st)
-{
-    k_p2p<QD, POT, FLD><<<blocks_for(a.n_leaves, kP2PWarps, int64_t(sms) * 16), kP2PWarps * 32, 0, st>>>(a);
-    SFMM_CHECK_LAUNCH();
-}
-
-void p2p_dispatch(const EvalArgs& a, int sms, cudaStream_t st)
-{
-    const int mode = (a.want_pot ? 1 : 0) | (a.want_field ? 2 : 0);
-#define SFMM_P2P(Q)                                                    \
-    if (a.qdim == Q) {                                                 \
-        if (mode == 1) return launch_p2p<Q, true, false>(a, sms, st);  \
-        if (mode == 2) return launch_p2p<Q, false, true>(a, sms, st);  \
-        return launch_p2p<Q, true, true>(a, sms, st);                  \
-    }
-    SFMM_P2P(1)
-    SFMM_P2P(2)
-    SFMM_P2P(3)
-#undef SFMM_P2P
 }
 
 }  // namespace
@@ -573,7 +455,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
     }
     SFMM_CUDA(cudaEventRecord(pl.ev[3], st));
-    p2p_dispatch(a, sms, st);
+    launch_p2p(a, sms, st);
     SFMM_CUDA(cudaEventRecord(pl.ev[4], st));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
     SFMM_CHECK_LAUNCH();

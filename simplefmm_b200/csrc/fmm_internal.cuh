@@ -42,9 +42,12 @@ extern std::atomic<long long> g_launches;
     } while (0)
 
 // ------------------------------------------------------------------ device memory
-// Stream-ordered device allocation (cudaMallocAsync from the device pool,
-// whose release threshold is raised at context creation so repeated
-// evaluations reuse memory instead of returning it to the driver).
+// Stream-ordered device allocation from a memory pool owned by this library
+// (one per device, created on first use, kept until exit, release threshold
+// unlimited): repeated trees and plans reuse the pool's memory, and no other
+// user of the device's default pool can trim it between evaluations.
+cudaMemPool_t device_pool(int device);
+
 template<typename T>
 struct DevBuf {
     T* ptr = nullptr;
@@ -72,7 +75,9 @@ struct DevBuf {
         stream = s;
         count = n;
         if (n) {
-            cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), s);
+            int dev = 0;
+            SFMM_CUDA(cudaGetDevice(&dev));
+            cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), device_pool(dev), s);
             if (e == cudaErrorMemoryAllocation) {
                 (void)cudaGetLastError();
                 ptr = nullptr;

@@ -335,7 +335,7 @@ __global__ void __launch_bounds__(RowCfg<P>::NT) k_m2l_rows(EvalArgs a, int64_t 
 }
 
 template<int P>
-void launch_rows(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
+void launch_rows_fallback(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     constexpr int T = RowCfg<P>::T, T1 = RowCfg<P>::T1, NT = RowCfg<P>::NT;
     const size_t smem = m2l_smem(T, T1, a.qdim).total;
@@ -349,13 +349,474 @@ void launch_rows(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_
     SFMM_CHECK_LAUNCH();
 }
 
+// ------------------------------------------------------------------ role-pipelined kernel (p <= 12)
+// The same row-ownership arithmetic as k_m2l_rows, with the four operators
+// given to four disjoint thread groups (roles) so each thread keeps only one
+// operator row in registers, and pipelined over batches: in every step
+//   C  computes batch s+1's column table, loads+phases batch s (X),
+//      z-translates batch s-2 (W -> LzA, LzB);
+//   B  rotates batch s-1 (X -> W);
+//   DA rotates back the potential local of batch s-3 (LzA -> accA);
+//   DB rotates back the field local of batch s-3 (LzB -> accB);
+// with one block barrier per step and double-buffered batch vectors.  C's
+// rows are ordered by azimuth k so the translation loop length p+1-k is
+// uniform across a warp.  Roles branch once at kernel entry; the barriers are
+// the non-aligned barrier.sync so different roles may arrive from different
+// code.
+
+struct Meta {
+    int cls, ncol, dsq, pad;
+    int src[8], sb[8], pidx[8];
+};
+
+template<int P, int CB>
+struct RoleCfg {
+    static constexpr int T = (P + 1) * (P + 2) / 2;
+    static constexpr int T1 = (P + 2) * (P + 3) / 2;
+    static constexpr int NB = (T + 31) / 32 * 32;
+    static constexpr int NC = (T1 + 31) / 32 * 32;
+    static constexpr int OB = 0, OC = NB, ODA = NB + NC, ODB = 2 * NB + NC;
+    static constexpr int NT = 2 * NB + 2 * NC;
+};
+
+struct RoleSmem {
+    int ent_src, ent_code, sorted, cls, cls_cnt, cls_off, bat_off, meta, tm, X, W, LzA, LzB, accA, accB, total;
+};
+
+__host__ __device__ inline RoleSmem role_smem(int T, int T1, int qd, int CB)
+{
+    RoleSmem s;
+    int o = 0;
+    s.ent_src = o; o = al16(o + 4 * kMaxGroupPairs);
+    s.ent_code = o; o = al16(o + 4 * kMaxGroupPairs);
+    s.sorted = o; o = al16(o + 2 * kMaxGroupPairs);
+    s.cls = o; o = al16(o + kMaxGroupPairs);
+    s.cls_cnt = o; o = al16(o + 4 * 72);
+    s.cls_off = o; o = al16(o + 4 * 72);
+    s.bat_off = o; o = al16(o + 4 * 72);
+    s.meta = o; o = al16(o + int(sizeof(Meta)) * 8);
+    s.tm = o; o = al16(o + T1);
+    s.X = o; o = al16(o + 16 * 2 * CB * T);
+    s.W = o; o = al16(o + 16 * 2 * CB * T);
+    s.LzA = o; o = al16(o + 16 * 2 * CB * T);
+    s.LzB = o; o = al16(o + 16 * 2 * CB * T1);
+    s.accA = o; o = al16(o + 16 * 8 * qd * T);
+    s.accB = o; o = al16(o + 16 * 8 * qd * T1);
+    s.total = o;
+    return s;
+}
+
+__device__ __forceinline__ void block_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
+
+struct RoleShared {
+    int* ent_src;
+    int* ent_code;
+    short* sorted;
+    unsigned char* cls;
+    int* cls_cnt;
+    int* cls_off;
+    int* bat_off;
+    Meta* meta;
+    unsigned char* tm;
+    cplx* X;
+    cplx* W;
+    cplx* LzA;
+    cplx* LzB;
+    cplx* accA;
+    cplx* accB;
+};
+
+// Column table of batch b (thread k < CB of the calling group fills column k).
+// c is the class of an earlier batch (batches ascend by class) and is
+// advanced to batch b's class.
+template<int CB>
+__device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M, int& c)
+{
+    while (S.bat_off[c + 1] <= b) ++c;
+    const int col0 = (b - S.bat_off[c]) * CB;
+    const int ncol = min(CB, S.cls_cnt[c] * qd - col0);
+    if (k < ncol) {
+        const int col = col0 + k;
+        const int e = S.sorted[S.cls_off[c] + col / qd];
+        const int code = S.ent_code[e];
+        const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
+        M.src[k] = S.ent_src[e];
+        M.sb[k] = ((code >> 9) & 7) * qd + (col - (col / qd) * qd);
+        M.pidx[k] = 7 * (dj + 3) + (di + 3);
+        if (k == 0) {
+            M.cls = c;
+            M.ncol = ncol;
+            M.dsq = di * di + dj * dj + dk * dk;
+        }
+    } else if (k < CB) {
+        M.src[k] = 0;
+        M.sb[k] = 0;
+        M.pidx[k] = 24;
+    }
+}
+
+// Group set-up shared by all roles: gather, class sort, batch table, batch
+// 0's column table, zeroed accumulators.  Returns the batch count.
+template<int P, int CB>
+__device__ int group_prologue(const EvalArgs& a, const RoleShared& S, int64_t g, int tid)
+{
+    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
+    const int qd = a.qdim;
+    const int nc = a.nchild[g];
+    const int cb = a.child_beg[g];
+    const int e0 = a.il_ptr[cb];
+    const int E = a.il_ptr[cb + nc] - e0;
+    for (int s = 0; s < nc; ++s) {
+        const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
+        for (int e = q0 + tid; e < q1; e += NT) {
+            const int code = a.il_code[e0 + e];
+            S.ent_src[e] = a.il_src[e0 + e];
+            S.ent_code[e] = code | (s << 9);
+            S.cls[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
+        }
+    }
+    for (int t = tid; t < 8 * qd * T; t += NT) S.accA[t] = cplx{0, 0};
+    for (int t = tid; t < 8 * qd * T1; t += NT) S.accB[t] = cplx{0, 0};
+    block_barrier();
+    for (int cl = tid; cl < kNumClasses; cl += NT) {
+        int cnt = 0;
+        for (int e = 0; e < E; ++e) cnt += S.cls[e] == cl;
+        S.cls_cnt[cl] = cnt;
+    }
+    block_barrier();
+    if (tid == 0) {
+        int s = 0, k = 0;
+        for (int c = 0; c < kNumClasses; ++c) {
+            S.cls_off[c] = s;
+            S.bat_off[c] = k;
+            s += S.cls_cnt[c];
+            k += (S.cls_cnt[c] * qd + CB - 1) / CB;
+        }
+        S.cls_off[kNumClasses] = s;
+        S.bat_off[kNumClasses] = k;
+    }
+    block_barrier();
+    for (int cl = tid; cl < kNumClasses; cl += NT) {
+        int pos = S.cls_off[cl];
+        for (int e = 0; e < E; ++e)
+            if (S.cls[e] == cl) S.sorted[pos++] = static_cast<short>(e);
+    }
+    block_barrier();
+    if (tid < CB && S.bat_off[kNumClasses] > 0) {
+        int c = 0;
+        compute_meta<CB>(S, 0, tid, qd, S.meta[0], c);
+    }
+    block_barrier();
+    return S.bat_off[kNumClasses];
+}
+
+template<int P, int CB>
+__device__ void group_epilogue(const EvalArgs& a, const RoleShared& S, int64_t g, int tid)
+{
+    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
+    const int qd = a.qdim;
+    const int nc = a.nchild[g];
+    const int cb = a.child_beg[g];
+    if (a.want_pot)
+        for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = S.accA[e];
+    if (a.want_field)
+        for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = S.accB[e];
+    block_barrier();
+}
+
+template<int P, int CB>
+__device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
+{
+    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NC = RoleCfg<P, CB>::NC;
+    const int ci = tid - RoleCfg<P, CB>::OC;
+    const int qd = a.qdim;
+    // rows ordered by azimuth k, then target order j
+    int k = 0, rem = ci;
+    while (k <= P + 1 && rem >= P + 2 - k) {
+        rem -= P + 2 - k;
+        ++k;
+    }
+    const bool on = ci < T1;
+    const int j = on ? k + rem : 0;
+    if (!on) k = 0;
+    const int r = tri(j, k);
+    int kmin = on ? k : P + 1;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
+    // translation row: sources n' = k + i, i < p - k in tz[], the n' = p term in tzl
+    double tz[P > 0 ? P : 1], tzl;
+    {
+        const int wd = P + 1 - k;
+        const double* row = a.tzx + a.tzx_off[k] + (j - k) * (wd > 0 ? wd : 0);
+#pragma unroll
+        for (int i = 0; i < P; ++i) tz[i] = (on && i < wd - 1) ? __ldg(row + i) : 0.0;
+        tzl = (on && wd > 0) ? __ldg(row + wd - 1) : 0.0;
+    }
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        if (a.nchild[g] == 0) continue;
+        const int lt = level_of(a, g) + 1;
+        const int nbat = group_prologue<P, CB>(a, S, g, tid);
+        int cmeta = 0;
+        for (int s = 0; s < nbat + 3; ++s) {
+            if (s + 1 < nbat && ci < CB) compute_meta<CB>(S, s + 1, ci, qd, S.meta[(s + 1) & 7], cmeta);
+            if (s < nbat) {
+                const Meta& M = S.meta[s & 7];
+                cplx* X = S.X + (s & 1) * CB * T;
+                for (int e = ci; e < M.ncol * T; e += NC) {
+                    const int cc = e / T, t = e - cc * T;
+                    const int src = M.src[cc], sb = M.sb[cc];
+                    const int bq = sb - (sb / qd) * qd;
+                    const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + S.tm[t]);
+                    const double2 v = __ldg(reinterpret_cast<const double2*>(a.M) + (int64_t(src) * qd + bq) * T + t);
+                    X[cc * T + t] = cmul(cplx{ph.x, ph.y}, cplx{v.x, v.y});
+                }
+            }
+            if (on && s >= 2 && s - 2 < nbat) {
+                const Meta& M = S.meta[(s - 2) & 7];
+                const int ncol = M.ncol;
+                const cplx* W = S.W + (s & 1) * CB * T;          // (s - 2) & 1 == s & 1
+                cplx* LzA = S.LzA + (s & 1) * CB * T;
+                cplx* LzB = S.LzB + (s & 1) * CB * T1;
+                const double sc = a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + j];
+                double bre[CB], bim[CB];
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc) bre[cc] = bim[cc] = 0;
+#pragma unroll
+                for (int i = 0; i < P; ++i) {
+                    if (i >= P - kmin) break;
+                    if (i < P - k) {
+                        const int np = k + i;
+                        const cplx* y = W + np * (np + 1) / 2 + k;
+#pragma unroll
+                        for (int cc = 0; cc < CB; ++cc)
+                            if (cc < ncol) {
+                                const cplx v = y[cc * T];
+                                bre[cc] = fma(tz[i], v.re, bre[cc]);
+                                bim[cc] = fma(tz[i], v.im, bim[cc]);
+                            }
+                    }
+                }
+                // field local: sources of order <= p - 1; potential local adds order p
+                const cplx* yl = W + P * (P + 1) / 2 + (k <= P ? k : 0);
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < ncol) {
+                        LzB[cc * T1 + r] = cplx{bre[cc] * sc, bim[cc] * sc};
+                        if (j <= P) {
+                            const cplx v = yl[cc * T];
+                            LzA[cc * T + r] = cplx{fma(tzl, v.re, bre[cc]) * sc, fma(tzl, v.im, bim[cc]) * sc};
+                        }
+                    }
+            }
+            block_barrier();
+        }
+        group_epilogue<P, CB>(a, S, g, tid);
+    }
+}
+
+template<int P, int CB>
+__device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
+{
+    constexpr int T = RoleCfg<P, CB>::T;
+    const int bi = tid - RoleCfg<P, CB>::OB;
+    const bool on = bi < T;
+    int n = 0, m = 0;
+    if (on) tri_nm(bi, n, m);
+    const int base = n * (n + 1) / 2;
+    int nmax = on ? n : 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    double Pr[P + 1], Qr[P + 1];
+    int cur = -1;
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        if (a.nchild[g] == 0) continue;
+        const int lt = level_of(a, g) + 1;
+        const int nbat = group_prologue<P, CB>(a, S, g, tid);
+        for (int s = 0; s < nbat + 3; ++s) {
+            if (on && s >= 1 && s - 1 < nbat) {
+                const Meta& M = S.meta[(s - 1) & 7];
+                const int ncol = M.ncol;
+                if (M.cls != cur) {
+                    const double* Pp = a.rot + int64_t(M.cls) * a.rot_len + a.rot_off[n] + m * (n + 1);
+                    const double* Qp = Pp + (n + 1) * (n + 1);
+#pragma unroll
+                    for (int b = 0; b <= P; ++b) {
+                        Pr[b] = b <= n ? __ldg(Pp + b) : 0.0;
+                        Qr[b] = b <= n ? __ldg(Qp + b) : 0.0;
+                    }
+                    cur = M.cls;
+                }
+                const cplx* X = S.X + ((s - 1) & 1) * CB * T + base;
+                cplx* W = S.W + ((s - 1) & 1) * CB * T;
+                double re[CB], im[CB];
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
+#pragma unroll
+                for (int b = 0; b <= P; ++b) {
+                    if (b > nmax) break;
+                    if (b <= n) {
+#pragma unroll
+                        for (int cc = 0; cc < CB; ++cc)
+                            if (cc < ncol) {
+                                const cplx x = X[cc * T + b];
+                                re[cc] = fma(Pr[b], x.re, re[cc]);
+                                im[cc] = fma(Qr[b], x.im, im[cc]);
+                            }
+                    }
+                }
+                const double sc = n ? a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + n - 1] : 1.0;
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < ncol) W[cc * T + bi] = cplx{re[cc] * sc, im[cc] * sc};
+            }
+            block_barrier();
+        }
+        group_epilogue<P, CB>(a, S, g, tid);
+    }
+}
+
+// Inverse rotation of one local (LA: order <= P, ORDER1 = false; LB: order
+// <= P + 1, ORDER1 = true) into the group accumulators.
+template<int P, int CB, bool ORDER1>
+__device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid, int off)
+{
+    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
+    constexpr int TO = ORDER1 ? T1 : T;               // rows of this local
+    constexpr int NMAX = ORDER1 ? P + 1 : P;
+    const int di = tid - off;
+    const bool wanted = ORDER1 ? a.want_field : a.want_pot;
+    const bool on = di < TO && wanted;
+    int n = 0, m = 0;
+    if (di < TO) tri_nm(di, n, m);
+    const int base = n * (n + 1) / 2;
+    int nmax = on ? n : 0;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+    double PB[NMAX + 1], QB[NMAX + 1];
+    int cur = -1;
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        if (a.nchild[g] == 0) continue;
+        const int nbat = group_prologue<P, CB>(a, S, g, tid);
+        for (int s = 0; s < nbat + 3; ++s) {
+            if (on && s >= 3) {
+                const Meta& M = S.meta[(s - 3) & 7];
+                const int ncol = M.ncol;
+                if (M.cls != cur) {
+                    const int wd = (n + 1) * (n + 1);
+                    const double* PBp = a.rot + int64_t(M.cls) * a.rot_len + a.rot_off[n] + 2 * wd + m * (n + 1);
+                    const double* QBp = PBp + wd;
+#pragma unroll
+                    for (int b = 0; b <= NMAX; ++b) {
+                        PB[b] = b <= n ? __ldg(PBp + b) : 0.0;
+                        QB[b] = b <= n ? __ldg(QBp + b) : 0.0;
+                    }
+                    cur = M.cls;
+                }
+                const cplx* Lz = (ORDER1 ? S.LzB + ((s - 3) & 1) * CB * T1 : S.LzA + ((s - 3) & 1) * CB * T) + base;
+                double re[CB], im[CB];
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
+#pragma unroll
+                for (int b = 0; b <= NMAX; ++b) {
+                    if (b > nmax) break;
+                    if (b <= n) {
+#pragma unroll
+                        for (int cc = 0; cc < CB; ++cc)
+                            if (cc < ncol) {
+                                const cplx z = Lz[cc * TO + b];
+                                re[cc] = fma(PB[b], z.re, re[cc]);
+                                im[cc] = fma(QB[b], z.im, im[cc]);
+                            }
+                    }
+                }
+                cplx* acc = ORDER1 ? S.accB : S.accA;
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < ncol) {
+                        const double2 e = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + m);
+                        const cplx v = cmul(cplx{e.x, -e.y}, cplx{re[cc], im[cc]});
+                        cplx& d = acc[M.sb[cc] * TO + di];
+                        d.re += v.re;
+                        d.im += v.im;
+                    }
+            }
+            block_barrier();
+        }
+        group_epilogue<P, CB>(a, S, g, tid);
+    }
+}
+
+template<int P, int CB>
+__global__ void __launch_bounds__(RoleCfg<P, CB>::NT) k_m2l_roles(EvalArgs a, int64_t g0, int64_t g1)
+{
+    using C = RoleCfg<P, CB>;
+    extern __shared__ __align__(16) unsigned char sm[];
+    const RoleSmem L = role_smem(C::T, C::T1, a.qdim, CB);
+    RoleShared S;
+    S.ent_src = reinterpret_cast<int*>(sm + L.ent_src);
+    S.ent_code = reinterpret_cast<int*>(sm + L.ent_code);
+    S.sorted = reinterpret_cast<short*>(sm + L.sorted);
+    S.cls = sm + L.cls;
+    S.cls_cnt = reinterpret_cast<int*>(sm + L.cls_cnt);
+    S.cls_off = reinterpret_cast<int*>(sm + L.cls_off);
+    S.bat_off = reinterpret_cast<int*>(sm + L.bat_off);
+    S.meta = reinterpret_cast<Meta*>(sm + L.meta);
+    S.tm = sm + L.tm;
+    S.X = reinterpret_cast<cplx*>(sm + L.X);
+    S.W = reinterpret_cast<cplx*>(sm + L.W);
+    S.LzA = reinterpret_cast<cplx*>(sm + L.LzA);
+    S.LzB = reinterpret_cast<cplx*>(sm + L.LzB);
+    S.accA = reinterpret_cast<cplx*>(sm + L.accA);
+    S.accB = reinterpret_cast<cplx*>(sm + L.accB);
+    const int tid = threadIdx.x;
+    for (int t = tid; t < C::T1; t += C::NT) {
+        int n, m;
+        tri_nm(t, n, m);
+        S.tm[t] = static_cast<unsigned char>(m);
+    }
+    block_barrier();
+    if (tid < C::OC) role_B<P, CB>(a, S, g0, g1, tid);
+    else if (tid < C::ODA) role_C<P, CB>(a, S, g0, g1, tid);
+    else if (tid < C::ODB) role_D<P, CB, false>(a, S, g0, g1, tid, C::ODA);
+    else role_D<P, CB, true>(a, S, g0, g1, tid, C::ODB);
+}
+
+template<int P, int CB>
+bool try_launch_roles(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
+{
+    using C = RoleCfg<P, CB>;
+    const size_t smem = role_smem(C::T, C::T1, a.qdim, CB).total;
+    int dev = 0, optin = 0;
+    SFMM_CUDA(cudaGetDevice(&dev));
+    SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > size_t(optin)) return false;
+    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_roles<P, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0;
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_roles<P, CB>, C::NT, smem));
+    if (per_sm < 1) return false;
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
+    k_m2l_roles<P, CB><<<static_cast<unsigned>(grid), C::NT, smem, st>>>(a, g0, g1);
+    SFMM_CHECK_LAUNCH();
+    return true;
+}
+
+template<int P>
+void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
+{
+    if constexpr (P >= 2 && P <= 12) {
+        if (try_launch_roles<P, 8>(a, g0, g1, sms, st)) return;
+        if (try_launch_roles<P, 4>(a, g0, g1, sms, st)) return;
+    }
+    launch_rows_fallback<P>(a, g0, g1, sms, st);
+}
+
 }  // namespace
 
 void launch_m2l(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     if (g1 <= g0) return;
     switch (a.p) {
-#define SFMM_M2L_CASE(P) case P: launch_rows<P>(a, g0, g1, sms, st); break;
+#define SFMM_M2L_CASE(P) case P: launch_m2l_p<P>(a, g0, g1, sms, st); break;
         SFMM_M2L_CASE(0) SFMM_M2L_CASE(1) SFMM_M2L_CASE(2) SFMM_M2L_CASE(3) SFMM_M2L_CASE(4) SFMM_M2L_CASE(5)
         SFMM_M2L_CASE(6) SFMM_M2L_CASE(7) SFMM_M2L_CASE(8) SFMM_M2L_CASE(9) SFMM_M2L_CASE(10) SFMM_M2L_CASE(11)
         SFMM_M2L_CASE(12) SFMM_M2L_CASE(13) SFMM_M2L_CASE(14) SFMM_M2L_CASE(15) SFMM_M2L_CASE(16)

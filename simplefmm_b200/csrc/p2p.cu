@@ -1,0 +1,174 @@
+// P2P (fmm.hpp:773-809) for the FP64 path: the near field of every leaf over
+// its neighbour-list point ranges, with the reference's self exclusion
+// (is_self: i == j, fmm.hpp:786, 880).
+//
+// Warp per target leaf.  The leaf's source ranges are gathered into full
+// shared tiles of kChunk sources (x y | z q packed as double2).  Lanes are
+// (target group, source slice): tg targets per pass and 32/tg slices, with tg
+// chosen per leaf so that at most kMaxPass passes cover its targets; every
+// source read from shared memory is applied to the lane's target of every
+// pass (register blocking over passes).  Slices of a target are summed with
+// xor shuffles at the end.
+#include "eval_util.cuh"
+
+namespace sfmm {
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kChunk = 256;
+constexpr int kMaxPass = 4;
+constexpr int kTargetsPerBlock = 32 * kMaxPass;
+
+template<int QD>
+struct P2PSmem {
+    static constexpr int per_warp = kChunk * (16 + 16 + (QD > 1 ? 16 : 0) + 4);
+    static constexpr int total = kWarps * per_warp;
+};
+
+template<int QD, bool POT, bool FLD>
+__global__ void __launch_bounds__(kWarps * 32) k_p2p(EvalArgs a)
+{
+    constexpr int NO = (POT ? QD : 0) + (FLD ? 3 : 0);
+    extern __shared__ __align__(16) unsigned char sm[];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    unsigned char* mine = sm + w * P2PSmem<QD>::per_warp;
+    double2* sxy = reinterpret_cast<double2*>(mine);
+    double2* szq = sxy + kChunk;
+    double2* sq12 = szq + kChunk;                       // only for QD > 1
+    int* sj = reinterpret_cast<int*>(mine + kChunk * (32 + (QD > 1 ? 16 : 0)));
+    const double* q0 = a.qs;
+    const double* q1 = a.qs + (QD > 1 ? a.n : 0);
+    const double* q2 = a.qs + (QD > 2 ? 2 * a.n : 0);
+
+    for (int64_t f = blockIdx.x * int64_t(kWarps) + w; f < a.n_leaves; f += int64_t(gridDim.x) * kWarps) {
+        const int g = a.leaf_node[f];
+        const int t0 = a.pbeg[g], t1 = a.pend[g];
+        const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
+        for (int tb = t0; tb < t1; tb += kTargetsPerBlock) {
+            const int nt = min(kTargetsPerBlock, t1 - tb);
+            int tg = 1;
+            while (tg < 32 && tg * kMaxPass < nt) tg <<= 1;
+            const int slices = 32 / tg;
+            const int passes = (nt + tg - 1) / tg;
+            const int ti = lane / slices, s = lane - ti * slices;
+            double xi[kMaxPass], yi[kMaxPass], zi[kMaxPass];
+            int ii[kMaxPass];
+            double acc[kMaxPass][NO > 0 ? NO : 1];
+#pragma unroll
+            for (int p = 0; p < kMaxPass; ++p) {
+                const int t = p * tg + ti;
+                const bool on = p < passes && t < nt;
+                ii[p] = on ? tb + t : -1;
+                const int i = on ? tb + t : tb;
+                xi[p] = a.px[i];
+                yi[p] = a.py[i];
+                zi[p] = a.pz[i];
+#pragma unroll
+                for (int o = 0; o < NO; ++o) acc[p][o] = 0;
+            }
+            // stream the leaf's near-field sources through full shared tiles
+            int ri = r0, roff = 0;
+            while (ri < r1) {
+                int fill = 0;
+                while (ri < r1 && fill < kChunk) {
+                    const int2 rg = a.nr[ri];
+                    const int len = min(rg.y - rg.x - roff, kChunk - fill);
+                    for (int k = lane; k < len; k += 32) {
+                        const int j = rg.x + roff + k;
+                        sxy[fill + k] = make_double2(a.px[j], a.py[j]);
+                        szq[fill + k] = make_double2(a.pz[j], q0[j]);
+                        if (QD > 1) sq12[fill + k] = make_double2(q1[j], q2[j]);
+                        sj[fill + k] = j;
+                    }
+                    fill += len;
+                    roff += len;
+                    if (roff == rg.y - rg.x) {
+                        ++ri;
+                        roff = 0;
+                    }
+                }
+                __syncwarp();
+                for (int k = s; k < fill; k += slices) {
+                    const double2 xy = sxy[k], zq = szq[k];
+                    double2 qq = make_double2(0, 0);
+                    if (QD > 1) qq = sq12[k];
+                    const int j = sj[k];
+#pragma unroll
+                    for (int p = 0; p < kMaxPass; ++p) {
+                        if (p >= passes) break;
+                        const double dx = xi[p] - xy.x, dy = yi[p] - xy.y, dz = zi[p] - zq.x;
+                        const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
+                        const double ir = j == ii[p] ? 0.0 : rsqrt(r2);
+                        int o = 0;
+                        if (POT) {
+                            acc[p][o++] = fma(zq.y, ir, acc[p][0]);
+                            if (QD > 1) acc[p][o++] = fma(qq.x, ir, acc[p][1]);
+                            if (QD > 2) acc[p][o++] = fma(qq.y, ir, acc[p][2]);
+                        }
+                        if (FLD) {
+                            const double ir3 = ir * ir * ir;
+                            if (QD == 1) {
+                                const double cq = zq.y * ir3;
+                                acc[p][o] = fma(cq, dx, acc[p][o]);
+                                acc[p][o + 1] = fma(cq, dy, acc[p][o + 1]);
+                                acc[p][o + 2] = fma(cq, dz, acc[p][o + 2]);
+                            } else {
+                                const double qa = zq.y, qb = qq.x, qc = qq.y;
+                                acc[p][o] = fma((qb * dz - qc * dy), ir3, acc[p][o]);
+                                acc[p][o + 1] = fma((qc * dx - qa * dz), ir3, acc[p][o + 1]);
+                                acc[p][o + 2] = fma((qa * dy - qb * dx), ir3, acc[p][o + 2]);
+                            }
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            // sum the slices of each target (consecutive lanes)
+#pragma unroll
+            for (int p = 0; p < kMaxPass; ++p)
+#pragma unroll
+                for (int o = 0; o < NO; ++o)
+                    for (int off = slices >> 1; off; off >>= 1) acc[p][o] += __shfl_xor_sync(0xffffffffu, acc[p][o], off);
+            if (s == 0) {
+#pragma unroll
+                for (int p = 0; p < kMaxPass; ++p) {
+                    if (ii[p] < 0) continue;
+                    int o = 0;
+                    if (POT)
+                        for (int b = 0; b < QD; ++b) a.out2[int64_t(b) * a.n + ii[p]] = acc[p][o++];
+                    if (FLD)
+                        for (int c = 0; c < 3; ++c) a.out2[int64_t(a.kf + c) * a.n + ii[p]] = acc[p][o++];
+                }
+            }
+        }
+    }
+}
+
+template<int QD, bool POT, bool FLD>
+void launch(const EvalArgs& a, int sms, cudaStream_t st)
+{
+    const size_t smem = P2PSmem<QD>::total;
+    SFMM_CUDA(cudaFuncSetAttribute(k_p2p<QD, POT, FLD>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    const int64_t grid = std::min<int64_t>((a.n_leaves + kWarps - 1) / kWarps, int64_t(sms) * 8);
+    k_p2p<QD, POT, FLD><<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kWarps * 32, smem, st>>>(a);
+    SFMM_CHECK_LAUNCH();
+}
+
+}  // namespace
+
+void launch_p2p(const EvalArgs& a, int sms, cudaStream_t st)
+{
+    const int mode = (a.want_pot ? 1 : 0) | (a.want_field ? 2 : 0);
+#define SFMM_P2P(Q)                                              \
+    if (a.qdim == Q) {                                           \
+        if (mode == 1) return launch<Q, true, false>(a, sms, st); \
+        if (mode == 2) return launch<Q, false, true>(a, sms, st); \
+        return launch<Q, true, true>(a, sms, st);                \
+    }
+    SFMM_P2P(1)
+    SFMM_P2P(2)
+    SFMM_P2P(3)
+#undef SFMM_P2P
+}
+
+}  // namespace sfmm
