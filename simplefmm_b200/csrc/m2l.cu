@@ -366,7 +366,7 @@ void launch_rows_fallback(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cu
 
 struct Meta {
     int cls, ncol, dsq, pad;
-    int src[8], sb[8], pidx[8];
+    int src[8], bq[8], sb[8], pidx[8];
 };
 
 template<int P, int CB>
@@ -380,7 +380,7 @@ struct RoleCfg {
 };
 
 struct RoleSmem {
-    int ent_src, ent_code, sorted, cls, cls_cnt, cls_off, bat_off, meta, tm, X, W, LzA, LzB, accA, accB, total;
+    int ent_src, ent_code, sorted, cls, cls_cnt, cls_off, bat_off, meta, X, W, LzA, LzB, accA, accB, total;
 };
 
 __host__ __device__ inline RoleSmem role_smem(int T, int T1, int qd, int CB)
@@ -395,8 +395,7 @@ __host__ __device__ inline RoleSmem role_smem(int T, int T1, int qd, int CB)
     s.cls_off = o; o = al16(o + 4 * 72);
     s.bat_off = o; o = al16(o + 4 * 72);
     s.meta = o; o = al16(o + int(sizeof(Meta)) * 8);
-    s.tm = o; o = al16(o + T1);
-    s.X = o; o = al16(o + 16 * 2 * CB * T);
+    s.X = o; o = al16(o + 16 * 2 * CB * T);       // X, W, LzA, LzB are contiguous (zeroed together)
     s.W = o; o = al16(o + 16 * 2 * CB * T);
     s.LzA = o; o = al16(o + 16 * 2 * CB * T);
     s.LzB = o; o = al16(o + 16 * 2 * CB * T1);
@@ -417,7 +416,6 @@ struct RoleShared {
     int* cls_off;
     int* bat_off;
     Meta* meta;
-    unsigned char* tm;
     cplx* X;
     cplx* W;
     cplx* LzA;
@@ -428,7 +426,8 @@ struct RoleShared {
 
 // Column table of batch b (thread k < CB of the calling group fills column k).
 // c is the class of an earlier batch (batches ascend by class) and is
-// advanced to batch b's class.
+// advanced to batch b's class.  Columns past ncol point at node 0 / slot 0;
+// their arithmetic runs on stale (finite) buffer contents and is discarded.
 template<int CB>
 __device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M, int& c)
 {
@@ -437,11 +436,14 @@ __device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M,
     const int ncol = min(CB, S.cls_cnt[c] * qd - col0);
     if (k < ncol) {
         const int col = col0 + k;
-        const int e = S.sorted[S.cls_off[c] + col / qd];
+        const int pair = col / qd;
+        const int e = S.sorted[S.cls_off[c] + pair];
         const int code = S.ent_code[e];
         const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
+        const int bq = col - pair * qd;
         M.src[k] = S.ent_src[e];
-        M.sb[k] = ((code >> 9) & 7) * qd + (col - (col / qd) * qd);
+        M.bq[k] = bq;
+        M.sb[k] = ((code >> 9) & 7) * qd + bq;
         M.pidx[k] = 7 * (dj + 3) + (di + 3);
         if (k == 0) {
             M.cls = c;
@@ -450,6 +452,7 @@ __device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M,
         }
     } else if (k < CB) {
         M.src[k] = 0;
+        M.bq[k] = 0;
         M.sb[k] = 0;
         M.pidx[k] = 24;
     }
@@ -524,13 +527,16 @@ __device__ void group_epilogue(const EvalArgs& a, const RoleShared& S, int64_t g
     block_barrier();
 }
 
+// C: column table, load + phase, z-translation.  Translation rows are
+// ordered by azimuth k (row ci -> (j, k)); operator entries past a row's
+// length are zero, so the loop runs to the warp's longest row without
+// per-lane tests, reading in-range (clamped) source coefficients.
 template<int P, int CB>
 __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
 {
-    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NC = RoleCfg<P, CB>::NC;
+    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
     const int ci = tid - RoleCfg<P, CB>::OC;
     const int qd = a.qdim;
-    // rows ordered by azimuth k, then target order j
     int k = 0, rem = ci;
     while (k <= P + 1 && rem >= P + 2 - k) {
         rem -= P + 2 - k;
@@ -540,17 +546,25 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
     const int j = on ? k + rem : 0;
     if (!on) k = 0;
     const int r = tri(j, k);
+    const int kc = k <= P ? k : P;                    // clamped azimuth for source reads
     int kmin = on ? k : P + 1;
 #pragma unroll
     for (int o = 16; o; o >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
     // translation row: sources n' = k + i, i < p - k in tz[], the n' = p term in tzl
-    double tz[P > 0 ? P : 1], tzl;
+    double tz[P], tzl;
     {
         const int wd = P + 1 - k;
         const double* row = a.tzx + a.tzx_off[k] + (j - k) * (wd > 0 ? wd : 0);
 #pragma unroll
         for (int i = 0; i < P; ++i) tz[i] = (on && i < wd - 1) ? __ldg(row + i) : 0.0;
         tzl = (on && wd > 0) ? __ldg(row + wd - 1) : 0.0;
+    }
+    // load role: coefficient xt = ci of every column (T <= NC)
+    const bool ld = ci < T;
+    int xm = 0;
+    if (ld) {
+        int xn;
+        tri_nm(ci, xn, xm);
     }
     for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
         if (a.nchild[g] == 0) continue;
@@ -559,21 +573,23 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
         int cmeta = 0;
         for (int s = 0; s < nbat + 3; ++s) {
             if (s + 1 < nbat && ci < CB) compute_meta<CB>(S, s + 1, ci, qd, S.meta[(s + 1) & 7], cmeta);
-            if (s < nbat) {
+            if (s < nbat && ld) {
                 const Meta& M = S.meta[s & 7];
-                cplx* X = S.X + (s & 1) * CB * T;
-                for (int e = ci; e < M.ncol * T; e += NC) {
-                    const int cc = e / T, t = e - cc * T;
-                    const int src = M.src[cc], sb = M.sb[cc];
-                    const int bq = sb - (sb / qd) * qd;
-                    const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + S.tm[t]);
-                    const double2 v = __ldg(reinterpret_cast<const double2*>(a.M) + (int64_t(src) * qd + bq) * T + t);
-                    X[cc * T + t] = cmul(cplx{ph.x, ph.y}, cplx{v.x, v.y});
-                }
-            }
-            if (on && s >= 2 && s - 2 < nbat) {
-                const Meta& M = S.meta[(s - 2) & 7];
                 const int ncol = M.ncol;
+                cplx* X = S.X + (s & 1) * CB * T + ci;
+                double2 v[CB], ph[CB];
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < ncol) {
+                        v[cc] = __ldg(reinterpret_cast<const double2*>(a.M) + (int64_t(M.src[cc]) * qd + M.bq[cc]) * T + ci);
+                        ph[cc] = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + xm);
+                    }
+#pragma unroll
+                for (int cc = 0; cc < CB; ++cc)
+                    if (cc < ncol) X[cc * T] = cmul(cplx{ph[cc].x, ph[cc].y}, cplx{v[cc].x, v[cc].y});
+            }
+            if (s >= 2 && s - 2 < nbat) {
+                const Meta& M = S.meta[(s - 2) & 7];
                 const cplx* W = S.W + (s & 1) * CB * T;          // (s - 2) & 1 == s & 1
                 cplx* LzA = S.LzA + (s & 1) * CB * T;
                 cplx* LzB = S.LzB + (s & 1) * CB * T1;
@@ -584,29 +600,27 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 #pragma unroll
                 for (int i = 0; i < P; ++i) {
                     if (i >= P - kmin) break;
-                    if (i < P - k) {
-                        const int np = k + i;
-                        const cplx* y = W + np * (np + 1) / 2 + k;
+                    const int np = min(k + i, P);
+                    const cplx* y = W + np * (np + 1) / 2 + kc;
 #pragma unroll
-                        for (int cc = 0; cc < CB; ++cc)
-                            if (cc < ncol) {
-                                const cplx v = y[cc * T];
-                                bre[cc] = fma(tz[i], v.re, bre[cc]);
-                                bim[cc] = fma(tz[i], v.im, bim[cc]);
-                            }
+                    for (int cc = 0; cc < CB; ++cc) {
+                        const cplx w = y[cc * T];
+                        bre[cc] = fma(tz[i], w.re, bre[cc]);
+                        bim[cc] = fma(tz[i], w.im, bim[cc]);
                     }
                 }
-                // field local: sources of order <= p - 1; potential local adds order p
-                const cplx* yl = W + P * (P + 1) / 2 + (k <= P ? k : 0);
+                if (on) {
+                    // field local: sources of order <= p - 1; potential local adds order p
+                    const cplx* yl = W + P * (P + 1) / 2 + kc;
 #pragma unroll
-                for (int cc = 0; cc < CB; ++cc)
-                    if (cc < ncol) {
+                    for (int cc = 0; cc < CB; ++cc) {
                         LzB[cc * T1 + r] = cplx{bre[cc] * sc, bim[cc] * sc};
                         if (j <= P) {
-                            const cplx v = yl[cc * T];
-                            LzA[cc * T + r] = cplx{fma(tzl, v.re, bre[cc]) * sc, fma(tzl, v.im, bim[cc]) * sc};
+                            const cplx w = yl[cc * T];
+                            LzA[cc * T + r] = cplx{fma(tzl, w.re, bre[cc]) * sc, fma(tzl, w.im, bim[cc]) * sc};
                         }
                     }
+                }
             }
             block_barrier();
         }
@@ -614,6 +628,7 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
     }
 }
 
+// B: forward rotation, order n row m (operator entries past n are zero).
 template<int P, int CB>
 __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
 {
@@ -627,24 +642,27 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 #pragma unroll
     for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
     double Pr[P + 1], Qr[P + 1];
+#pragma unroll
+    for (int b = 0; b <= P; ++b) Pr[b] = Qr[b] = 0.0;
     int cur = -1;
     for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
         if (a.nchild[g] == 0) continue;
         const int lt = level_of(a, g) + 1;
         const int nbat = group_prologue<P, CB>(a, S, g, tid);
         for (int s = 0; s < nbat + 3; ++s) {
-            if (on && s >= 1 && s - 1 < nbat) {
+            if (s >= 1 && s - 1 < nbat) {
                 const Meta& M = S.meta[(s - 1) & 7];
-                const int ncol = M.ncol;
                 if (M.cls != cur) {
-                    const double* Pp = a.rot + int64_t(M.cls) * a.rot_len + a.rot_off[n] + m * (n + 1);
-                    const double* Qp = Pp + (n + 1) * (n + 1);
-#pragma unroll
-                    for (int b = 0; b <= P; ++b) {
-                        Pr[b] = b <= n ? __ldg(Pp + b) : 0.0;
-                        Qr[b] = b <= n ? __ldg(Qp + b) : 0.0;
-                    }
                     cur = M.cls;
+                    if (on) {
+                        const double* Pp = a.rot + int64_t(cur) * a.rot_len + a.rot_off[n] + m * (n + 1);
+                        const double* Qp = Pp + (n + 1) * (n + 1);
+#pragma unroll
+                        for (int b = 0; b <= P; ++b) {
+                            Pr[b] = b <= n ? __ldg(Pp + b) : 0.0;
+                            Qr[b] = b <= n ? __ldg(Qp + b) : 0.0;
+                        }
+                    }
                 }
                 const cplx* X = S.X + ((s - 1) & 1) * CB * T + base;
                 cplx* W = S.W + ((s - 1) & 1) * CB * T;
@@ -654,20 +672,18 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 #pragma unroll
                 for (int b = 0; b <= P; ++b) {
                     if (b > nmax) break;
-                    if (b <= n) {
 #pragma unroll
-                        for (int cc = 0; cc < CB; ++cc)
-                            if (cc < ncol) {
-                                const cplx x = X[cc * T + b];
-                                re[cc] = fma(Pr[b], x.re, re[cc]);
-                                im[cc] = fma(Qr[b], x.im, im[cc]);
-                            }
+                    for (int cc = 0; cc < CB; ++cc) {
+                        const cplx x = X[cc * T + b];
+                        re[cc] = fma(Pr[b], x.re, re[cc]);
+                        im[cc] = fma(Qr[b], x.im, im[cc]);
                     }
                 }
-                const double sc = n ? a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + n - 1] : 1.0;
+                if (on) {
+                    const double sc = n ? a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + n - 1] : 1.0;
 #pragma unroll
-                for (int cc = 0; cc < CB; ++cc)
-                    if (cc < ncol) W[cc * T + bi] = cplx{re[cc] * sc, im[cc] * sc};
+                    for (int cc = 0; cc < CB; ++cc) W[cc * T + bi] = cplx{re[cc] * sc, im[cc] * sc};
+                }
             }
             block_barrier();
         }
@@ -675,8 +691,9 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
     }
 }
 
-// Inverse rotation of one local (LA: order <= P, ORDER1 = false; LB: order
-// <= P + 1, ORDER1 = true) into the group accumulators.
+// D: inverse rotation of one local (LA: order <= P, ORDER1 = false; LB:
+// order <= P + 1, ORDER1 = true) and phase, accumulated into the group's
+// targets in column order (deterministic).
 template<int P, int CB, bool ORDER1>
 __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid, int off)
 {
@@ -693,24 +710,28 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 #pragma unroll
     for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
     double PB[NMAX + 1], QB[NMAX + 1];
+#pragma unroll
+    for (int b = 0; b <= NMAX; ++b) PB[b] = QB[b] = 0.0;
     int cur = -1;
     for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
         if (a.nchild[g] == 0) continue;
         const int nbat = group_prologue<P, CB>(a, S, g, tid);
         for (int s = 0; s < nbat + 3; ++s) {
-            if (on && s >= 3) {
+            if (wanted && s >= 3) {
                 const Meta& M = S.meta[(s - 3) & 7];
                 const int ncol = M.ncol;
                 if (M.cls != cur) {
-                    const int wd = (n + 1) * (n + 1);
-                    const double* PBp = a.rot + int64_t(M.cls) * a.rot_len + a.rot_off[n] + 2 * wd + m * (n + 1);
-                    const double* QBp = PBp + wd;
-#pragma unroll
-                    for (int b = 0; b <= NMAX; ++b) {
-                        PB[b] = b <= n ? __ldg(PBp + b) : 0.0;
-                        QB[b] = b <= n ? __ldg(QBp + b) : 0.0;
-                    }
                     cur = M.cls;
+                    if (on) {
+                        const int wd = (n + 1) * (n + 1);
+                        const double* PBp = a.rot + int64_t(cur) * a.rot_len + a.rot_off[n] + 2 * wd + m * (n + 1);
+                        const double* QBp = PBp + wd;
+#pragma unroll
+                        for (int b = 0; b <= NMAX; ++b) {
+                            PB[b] = b <= n ? __ldg(PBp + b) : 0.0;
+                            QB[b] = b <= n ? __ldg(QBp + b) : 0.0;
+                        }
+                    }
                 }
                 const cplx* Lz = (ORDER1 ? S.LzB + ((s - 3) & 1) * CB * T1 : S.LzA + ((s - 3) & 1) * CB * T) + base;
                 double re[CB], im[CB];
@@ -719,26 +740,25 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 #pragma unroll
                 for (int b = 0; b <= NMAX; ++b) {
                     if (b > nmax) break;
-                    if (b <= n) {
 #pragma unroll
-                        for (int cc = 0; cc < CB; ++cc)
-                            if (cc < ncol) {
-                                const cplx z = Lz[cc * TO + b];
-                                re[cc] = fma(PB[b], z.re, re[cc]);
-                                im[cc] = fma(QB[b], z.im, im[cc]);
-                            }
+                    for (int cc = 0; cc < CB; ++cc) {
+                        const cplx z = Lz[cc * TO + b];
+                        re[cc] = fma(PB[b], z.re, re[cc]);
+                        im[cc] = fma(QB[b], z.im, im[cc]);
                     }
                 }
-                cplx* acc = ORDER1 ? S.accB : S.accA;
+                if (on) {
+                    cplx* acc = (ORDER1 ? S.accB : S.accA) + di;
 #pragma unroll
-                for (int cc = 0; cc < CB; ++cc)
-                    if (cc < ncol) {
-                        const double2 e = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + m);
-                        const cplx v = cmul(cplx{e.x, -e.y}, cplx{re[cc], im[cc]});
-                        cplx& d = acc[M.sb[cc] * TO + di];
-                        d.re += v.re;
-                        d.im += v.im;
-                    }
+                    for (int cc = 0; cc < CB; ++cc)
+                        if (cc < ncol) {
+                            const double2 e = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + m);
+                            const cplx v = cmul(cplx{e.x, -e.y}, cplx{re[cc], im[cc]});
+                            cplx& d = acc[M.sb[cc] * TO];
+                            d.re += v.re;
+                            d.im += v.im;
+                        }
+                }
             }
             block_barrier();
         }
@@ -761,7 +781,6 @@ __global__ void __launch_bounds__(RoleCfg<P, CB>::NT) k_m2l_roles(EvalArgs a, in
     S.cls_off = reinterpret_cast<int*>(sm + L.cls_off);
     S.bat_off = reinterpret_cast<int*>(sm + L.bat_off);
     S.meta = reinterpret_cast<Meta*>(sm + L.meta);
-    S.tm = sm + L.tm;
     S.X = reinterpret_cast<cplx*>(sm + L.X);
     S.W = reinterpret_cast<cplx*>(sm + L.W);
     S.LzA = reinterpret_cast<cplx*>(sm + L.LzA);
@@ -769,11 +788,9 @@ __global__ void __launch_bounds__(RoleCfg<P, CB>::NT) k_m2l_roles(EvalArgs a, in
     S.accA = reinterpret_cast<cplx*>(sm + L.accA);
     S.accB = reinterpret_cast<cplx*>(sm + L.accB);
     const int tid = threadIdx.x;
-    for (int t = tid; t < C::T1; t += C::NT) {
-        int n, m;
-        tri_nm(t, n, m);
-        S.tm[t] = static_cast<unsigned char>(m);
-    }
+    // batch buffers start at zero: columns past a batch's count are computed
+    // on whatever the buffers hold, which must be finite
+    for (int t = tid; t < (L.accA - L.X) / 16; t += C::NT) S.X[t] = cplx{0, 0};
     block_barrier();
     if (tid < C::OC) role_B<P, CB>(a, S, g0, g1, tid);
     else if (tid < C::ODA) role_C<P, CB>(a, S, g0, g1, tid);
