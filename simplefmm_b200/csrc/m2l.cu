@@ -44,7 +44,7 @@ struct M2LSmem {
     int ent_src, ent_code, sorted, cls, cls_cnt, cls_off, bat_off, X, W, LzA, LzB, accA, accB, total;
 };
 
-__host__ __device__ inline int al16(int x) { return (x + 15) & ~15; }
+__host__ __device__ constexpr int al16(int x) { return (x + 15) & ~15; }
 
 __host__ __device__ inline M2LSmem m2l_smem(int T, int T1, int qd)
 {
@@ -353,8 +353,10 @@ void launch_rows_fallback(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cu
 // The same row-ownership arithmetic as k_m2l_rows, with the four operators
 // given to four disjoint thread groups (roles) so each thread keeps only one
 // operator row in registers, and pipelined over batches: in every step
-//   C  computes batch s+1's column table, loads+phases batch s (X),
-//      z-translates batch s-2 (W -> LzA, LzB);
+//   C  phases batch s (its source moments were copied into shared memory
+//      asynchronously during step s-1), starts the copy of batch s+1,
+//      computes batch s+2's column table, z-translates batch s-2
+//      (W -> LzA, LzB);
 //   B  rotates batch s-1 (X -> W);
 //   DA rotates back the potential local of batch s-3 (LzA -> accA);
 //   DB rotates back the field local of batch s-3 (LzB -> accB);
@@ -379,69 +381,86 @@ struct RoleCfg {
     static constexpr int NT = 2 * NB + 2 * NC;
 };
 
-struct RoleSmem {
-    int ent_src, ent_code, sorted, cls, cls_cnt, cls_off, bat_off, meta, X, W, LzA, LzB, accA, accB, total;
+// Shared-memory layout of one block (byte offsets; all but accB are
+// compile-time constants so buffer addresses are immediate offsets).
+template<int P, int CB>
+struct RoleLayout {
+    static constexpr int T = (P + 1) * (P + 2) / 2;
+    static constexpr int T1 = (P + 2) * (P + 3) / 2;
+    static constexpr int ent_src = 0;
+    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
+    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
+    static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
+    static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
+    static constexpr int cls_off = al16(cls_cnt + 4 * 72);
+    static constexpr int bat_off = al16(cls_off + 4 * 72);
+    static constexpr int meta = al16(bat_off + 4 * 72);
+    static constexpr int Xraw = al16(meta + int(sizeof(Meta)) * 8);   // thread-private staging of source moments
+    static constexpr int X = al16(Xraw + 16 * 2 * CB * T);            // X, W, LzA, LzB are contiguous (zeroed together)
+    static constexpr int W = al16(X + 16 * 2 * CB * T);
+    static constexpr int LzA = al16(W + 16 * 2 * CB * T);
+    static constexpr int LzB = al16(LzA + 16 * 2 * CB * T);
+    static constexpr int accA = al16(LzB + 16 * 2 * CB * T1);
+    __host__ __device__ static constexpr int accB(int qd) { return al16(accA + 16 * 8 * qd * T); }
+    __host__ __device__ static constexpr int total(int qd) { return al16(accB(qd) + 16 * 8 * qd * T1); }
 };
-
-__host__ __device__ inline RoleSmem role_smem(int T, int T1, int qd, int CB)
-{
-    RoleSmem s;
-    int o = 0;
-    s.ent_src = o; o = al16(o + 4 * kMaxGroupPairs);
-    s.ent_code = o; o = al16(o + 4 * kMaxGroupPairs);
-    s.sorted = o; o = al16(o + 2 * kMaxGroupPairs);
-    s.cls = o; o = al16(o + kMaxGroupPairs);
-    s.cls_cnt = o; o = al16(o + 4 * 72);
-    s.cls_off = o; o = al16(o + 4 * 72);
-    s.bat_off = o; o = al16(o + 4 * 72);
-    s.meta = o; o = al16(o + int(sizeof(Meta)) * 8);
-    s.X = o; o = al16(o + 16 * 2 * CB * T);       // X, W, LzA, LzB are contiguous (zeroed together)
-    s.W = o; o = al16(o + 16 * 2 * CB * T);
-    s.LzA = o; o = al16(o + 16 * 2 * CB * T);
-    s.LzB = o; o = al16(o + 16 * 2 * CB * T1);
-    s.accA = o; o = al16(o + 16 * 8 * qd * T);
-    s.accB = o; o = al16(o + 16 * 8 * qd * T1);
-    s.total = o;
-    return s;
-}
 
 __device__ __forceinline__ void block_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
+// 16-byte global -> shared copy that completes asynchronously (L2 only);
+// the issuing thread waits with cp_async_wait_all before reading it.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template<int P, int CB>
 struct RoleShared {
-    int* ent_src;
-    int* ent_code;
-    short* sorted;
-    unsigned char* cls;
-    int* cls_cnt;
-    int* cls_off;
-    int* bat_off;
-    Meta* meta;
-    cplx* X;
-    cplx* W;
-    cplx* LzA;
-    cplx* LzB;
-    cplx* accA;
-    cplx* accB;
+    using L = RoleLayout<P, CB>;
+    int accB_off;
+    __device__ static unsigned char* base()
+    {
+        extern __shared__ __align__(16) unsigned char sm_roles[];
+        return sm_roles;
+    }
+    __device__ int* ent_src() const { return reinterpret_cast<int*>(base() + L::ent_src); }
+    __device__ int* ent_code() const { return reinterpret_cast<int*>(base() + L::ent_code); }
+    __device__ short* sorted() const { return reinterpret_cast<short*>(base() + L::sorted); }
+    __device__ unsigned char* cls() const { return base() + L::cls; }
+    __device__ int* cls_cnt() const { return reinterpret_cast<int*>(base() + L::cls_cnt); }
+    __device__ int* cls_off() const { return reinterpret_cast<int*>(base() + L::cls_off); }
+    __device__ int* bat_off() const { return reinterpret_cast<int*>(base() + L::bat_off); }
+    __device__ Meta* meta() const { return reinterpret_cast<Meta*>(base() + L::meta); }
+    __device__ cplx* Xraw() const { return reinterpret_cast<cplx*>(base() + L::Xraw); }
+    __device__ cplx* X() const { return reinterpret_cast<cplx*>(base() + L::X); }
+    __device__ cplx* W() const { return reinterpret_cast<cplx*>(base() + L::W); }
+    __device__ cplx* LzA() const { return reinterpret_cast<cplx*>(base() + L::LzA); }
+    __device__ cplx* LzB() const { return reinterpret_cast<cplx*>(base() + L::LzB); }
+    __device__ cplx* accA() const { return reinterpret_cast<cplx*>(base() + L::accA); }
+    __device__ cplx* accB() const { return reinterpret_cast<cplx*>(base() + accB_off); }
 };
 
 // Column table of batch b (thread k < CB of the calling group fills column k).
 // c is the class of an earlier batch (batches ascend by class) and is
 // advanced to batch b's class.  Columns past ncol point at node 0 / slot 0;
 // their arithmetic runs on stale (finite) buffer contents and is discarded.
-template<int CB>
-__device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M, int& c)
+template<int P, int CB>
+__device__ void compute_meta(const RoleShared<P, CB>& S, int b, int k, int qd, Meta& M, int& c)
 {
-    while (S.bat_off[c + 1] <= b) ++c;
-    const int col0 = (b - S.bat_off[c]) * CB;
-    const int ncol = min(CB, S.cls_cnt[c] * qd - col0);
+    while (S.bat_off()[c + 1] <= b) ++c;
+    const int col0 = (b - S.bat_off()[c]) * CB;
+    const int ncol = min(CB, S.cls_cnt()[c] * qd - col0);
     if (k < ncol) {
         const int col = col0 + k;
         const int pair = col / qd;
-        const int e = S.sorted[S.cls_off[c] + pair];
-        const int code = S.ent_code[e];
+        const int e = S.sorted()[S.cls_off()[c] + pair];
+        const int code = S.ent_code()[e];
         const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
         const int bq = col - pair * qd;
-        M.src[k] = S.ent_src[e];
+        M.src[k] = S.ent_src()[e];
         M.bq[k] = bq;
         M.sb[k] = ((code >> 9) & 7) * qd + bq;
         M.pidx[k] = 7 * (dj + 3) + (di + 3);
@@ -461,7 +480,7 @@ __device__ void compute_meta(const RoleShared& S, int b, int k, int qd, Meta& M,
 // Group set-up shared by all roles: gather, class sort, batch table, batch
 // 0's column table, zeroed accumulators.  Returns the batch count.
 template<int P, int CB>
-__device__ int group_prologue(const EvalArgs& a, const RoleShared& S, int64_t g, int tid)
+__device__ int group_prologue(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g, int tid)
 {
     constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
     const int qd = a.qdim;
@@ -473,57 +492,58 @@ __device__ int group_prologue(const EvalArgs& a, const RoleShared& S, int64_t g,
         const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
         for (int e = q0 + tid; e < q1; e += NT) {
             const int code = a.il_code[e0 + e];
-            S.ent_src[e] = a.il_src[e0 + e];
-            S.ent_code[e] = code | (s << 9);
-            S.cls[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
+            S.ent_src()[e] = a.il_src[e0 + e];
+            S.ent_code()[e] = code | (s << 9);
+            S.cls()[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
         }
     }
-    for (int t = tid; t < 8 * qd * T; t += NT) S.accA[t] = cplx{0, 0};
-    for (int t = tid; t < 8 * qd * T1; t += NT) S.accB[t] = cplx{0, 0};
+    for (int t = tid; t < 8 * qd * T; t += NT) S.accA()[t] = cplx{0, 0};
+    for (int t = tid; t < 8 * qd * T1; t += NT) S.accB()[t] = cplx{0, 0};
     block_barrier();
     for (int cl = tid; cl < kNumClasses; cl += NT) {
         int cnt = 0;
-        for (int e = 0; e < E; ++e) cnt += S.cls[e] == cl;
-        S.cls_cnt[cl] = cnt;
+        for (int e = 0; e < E; ++e) cnt += S.cls()[e] == cl;
+        S.cls_cnt()[cl] = cnt;
     }
     block_barrier();
     if (tid == 0) {
         int s = 0, k = 0;
         for (int c = 0; c < kNumClasses; ++c) {
-            S.cls_off[c] = s;
-            S.bat_off[c] = k;
-            s += S.cls_cnt[c];
-            k += (S.cls_cnt[c] * qd + CB - 1) / CB;
+            S.cls_off()[c] = s;
+            S.bat_off()[c] = k;
+            s += S.cls_cnt()[c];
+            k += (S.cls_cnt()[c] * qd + CB - 1) / CB;
         }
-        S.cls_off[kNumClasses] = s;
-        S.bat_off[kNumClasses] = k;
+        S.cls_off()[kNumClasses] = s;
+        S.bat_off()[kNumClasses] = k;
     }
     block_barrier();
     for (int cl = tid; cl < kNumClasses; cl += NT) {
-        int pos = S.cls_off[cl];
+        int pos = S.cls_off()[cl];
         for (int e = 0; e < E; ++e)
-            if (S.cls[e] == cl) S.sorted[pos++] = static_cast<short>(e);
+            if (S.cls()[e] == cl) S.sorted()[pos++] = static_cast<short>(e);
     }
     block_barrier();
-    if (tid < CB && S.bat_off[kNumClasses] > 0) {
+    if (tid < CB) {
         int c = 0;
-        compute_meta<CB>(S, 0, tid, qd, S.meta[0], c);
+        if (S.bat_off()[kNumClasses] > 0) compute_meta<P, CB>(S, 0, tid, qd, S.meta()[0], c);
+        if (S.bat_off()[kNumClasses] > 1) compute_meta<P, CB>(S, 1, tid, qd, S.meta()[1], c);
     }
     block_barrier();
-    return S.bat_off[kNumClasses];
+    return S.bat_off()[kNumClasses];
 }
 
 template<int P, int CB>
-__device__ void group_epilogue(const EvalArgs& a, const RoleShared& S, int64_t g, int tid)
+__device__ void group_epilogue(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g, int tid)
 {
     constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
     const int qd = a.qdim;
     const int nc = a.nchild[g];
     const int cb = a.child_beg[g];
     if (a.want_pot)
-        for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = S.accA[e];
+        for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = S.accA()[e];
     if (a.want_field)
-        for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = S.accB[e];
+        for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = S.accB()[e];
     block_barrier();
 }
 
@@ -532,7 +552,7 @@ __device__ void group_epilogue(const EvalArgs& a, const RoleShared& S, int64_t g
 // length are zero, so the loop runs to the warp's longest row without
 // per-lane tests, reading in-range (clamped) source coefficients.
 template<int P, int CB>
-__device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
+__device__ void role_C(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid)
 {
     constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
     const int ci = tid - RoleCfg<P, CB>::OC;
@@ -566,33 +586,43 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
         int xn;
         tri_nm(ci, xn, xm);
     }
+    // batch b's source coefficients -> Xraw[b & 1], issued a step ahead of use
+    auto issue = [&](int b) {
+        const Meta& M = S.meta()[b & 7];
+        const int ncol = M.ncol;
+        cplx* xr = S.Xraw() + (b & 1) * CB * T + ci;
+#pragma unroll
+        for (int cc = 0; cc < CB; ++cc)
+            if (cc < ncol) cp_async16(xr + cc * T, a.M + (int64_t(M.src[cc]) * qd + M.bq[cc]) * T + ci);
+        cp_async_commit();
+    };
     for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
         if (a.nchild[g] == 0) continue;
         const int lt = level_of(a, g) + 1;
         const int nbat = group_prologue<P, CB>(a, S, g, tid);
         int cmeta = 0;
+        if (ld && nbat > 0) issue(0);
         for (int s = 0; s < nbat + 3; ++s) {
-            if (s + 1 < nbat && ci < CB) compute_meta<CB>(S, s + 1, ci, qd, S.meta[(s + 1) & 7], cmeta);
             if (s < nbat && ld) {
-                const Meta& M = S.meta[s & 7];
+                cp_async_wait_all();
+                const Meta& M = S.meta()[s & 7];
                 const int ncol = M.ncol;
-                cplx* X = S.X + (s & 1) * CB * T + ci;
-                double2 v[CB], ph[CB];
+                const cplx* xr = S.Xraw() + (s & 1) * CB * T + ci;
+                cplx* X = S.X() + (s & 1) * CB * T + ci;
 #pragma unroll
                 for (int cc = 0; cc < CB; ++cc)
                     if (cc < ncol) {
-                        v[cc] = __ldg(reinterpret_cast<const double2*>(a.M) + (int64_t(M.src[cc]) * qd + M.bq[cc]) * T + ci);
-                        ph[cc] = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + xm);
+                        const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + xm);
+                        X[cc * T] = cmul(cplx{ph.x, ph.y}, xr[cc * T]);
                     }
-#pragma unroll
-                for (int cc = 0; cc < CB; ++cc)
-                    if (cc < ncol) X[cc * T] = cmul(cplx{ph[cc].x, ph[cc].y}, cplx{v[cc].x, v[cc].y});
+                if (s + 1 < nbat) issue(s + 1);
             }
+            if (s + 2 < nbat && ci < CB) compute_meta<P, CB>(S, s + 2, ci, qd, S.meta()[(s + 2) & 7], cmeta);
             if (s >= 2 && s - 2 < nbat) {
-                const Meta& M = S.meta[(s - 2) & 7];
-                const cplx* W = S.W + (s & 1) * CB * T;          // (s - 2) & 1 == s & 1
-                cplx* LzA = S.LzA + (s & 1) * CB * T;
-                cplx* LzB = S.LzB + (s & 1) * CB * T1;
+                const Meta& M = S.meta()[(s - 2) & 7];
+                const cplx* W = S.W() + (s & 1) * CB * T;          // (s - 2) & 1 == s & 1
+                cplx* LzA = S.LzA() + (s & 1) * CB * T;
+                cplx* LzB = S.LzB() + (s & 1) * CB * T1;
                 const double sc = a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + j];
                 double bre[CB], bim[CB];
 #pragma unroll
@@ -630,7 +660,7 @@ __device__ void role_C(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 
 // B: forward rotation, order n row m (operator entries past n are zero).
 template<int P, int CB>
-__device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid)
+__device__ void role_B(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid)
 {
     constexpr int T = RoleCfg<P, CB>::T;
     const int bi = tid - RoleCfg<P, CB>::OB;
@@ -651,7 +681,7 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
         const int nbat = group_prologue<P, CB>(a, S, g, tid);
         for (int s = 0; s < nbat + 3; ++s) {
             if (s >= 1 && s - 1 < nbat) {
-                const Meta& M = S.meta[(s - 1) & 7];
+                const Meta& M = S.meta()[(s - 1) & 7];
                 if (M.cls != cur) {
                     cur = M.cls;
                     if (on) {
@@ -664,8 +694,8 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
                         }
                     }
                 }
-                const cplx* X = S.X + ((s - 1) & 1) * CB * T + base;
-                cplx* W = S.W + ((s - 1) & 1) * CB * T;
+                const cplx* X = S.X() + ((s - 1) & 1) * CB * T + base;
+                cplx* W = S.W() + ((s - 1) & 1) * CB * T;
                 double re[CB], im[CB];
 #pragma unroll
                 for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
@@ -695,7 +725,7 @@ __device__ void role_B(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
 // order <= P + 1, ORDER1 = true) and phase, accumulated into the group's
 // targets in column order (deterministic).
 template<int P, int CB, bool ORDER1>
-__device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64_t g1, int tid, int off)
+__device__ void role_D(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid, int off)
 {
     constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
     constexpr int TO = ORDER1 ? T1 : T;               // rows of this local
@@ -718,7 +748,7 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
         const int nbat = group_prologue<P, CB>(a, S, g, tid);
         for (int s = 0; s < nbat + 3; ++s) {
             if (wanted && s >= 3) {
-                const Meta& M = S.meta[(s - 3) & 7];
+                const Meta& M = S.meta()[(s - 3) & 7];
                 const int ncol = M.ncol;
                 if (M.cls != cur) {
                     cur = M.cls;
@@ -733,7 +763,7 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
                         }
                     }
                 }
-                const cplx* Lz = (ORDER1 ? S.LzB + ((s - 3) & 1) * CB * T1 : S.LzA + ((s - 3) & 1) * CB * T) + base;
+                const cplx* Lz = (ORDER1 ? S.LzB() + ((s - 3) & 1) * CB * T1 : S.LzA() + ((s - 3) & 1) * CB * T) + base;
                 double re[CB], im[CB];
 #pragma unroll
                 for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
@@ -748,7 +778,7 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
                     }
                 }
                 if (on) {
-                    cplx* acc = (ORDER1 ? S.accB : S.accA) + di;
+                    cplx* acc = (ORDER1 ? S.accB() : S.accA()) + di;
 #pragma unroll
                     for (int cc = 0; cc < CB; ++cc)
                         if (cc < ncol) {
@@ -766,31 +796,17 @@ __device__ void role_D(const EvalArgs& a, const RoleShared& S, int64_t g0, int64
     }
 }
 
-template<int P, int CB>
-__global__ void __launch_bounds__(RoleCfg<P, CB>::NT) k_m2l_roles(EvalArgs a, int64_t g0, int64_t g1)
+template<int P, int CB, int MINB>
+__global__ void __launch_bounds__(RoleCfg<P, CB>::NT, MINB) k_m2l_roles(EvalArgs a, int64_t g0, int64_t g1)
 {
     using C = RoleCfg<P, CB>;
-    extern __shared__ __align__(16) unsigned char sm[];
-    const RoleSmem L = role_smem(C::T, C::T1, a.qdim, CB);
-    RoleShared S;
-    S.ent_src = reinterpret_cast<int*>(sm + L.ent_src);
-    S.ent_code = reinterpret_cast<int*>(sm + L.ent_code);
-    S.sorted = reinterpret_cast<short*>(sm + L.sorted);
-    S.cls = sm + L.cls;
-    S.cls_cnt = reinterpret_cast<int*>(sm + L.cls_cnt);
-    S.cls_off = reinterpret_cast<int*>(sm + L.cls_off);
-    S.bat_off = reinterpret_cast<int*>(sm + L.bat_off);
-    S.meta = reinterpret_cast<Meta*>(sm + L.meta);
-    S.X = reinterpret_cast<cplx*>(sm + L.X);
-    S.W = reinterpret_cast<cplx*>(sm + L.W);
-    S.LzA = reinterpret_cast<cplx*>(sm + L.LzA);
-    S.LzB = reinterpret_cast<cplx*>(sm + L.LzB);
-    S.accA = reinterpret_cast<cplx*>(sm + L.accA);
-    S.accB = reinterpret_cast<cplx*>(sm + L.accB);
+    using L = RoleLayout<P, CB>;
+    RoleShared<P, CB> S;
+    S.accB_off = L::accB(a.qdim);
     const int tid = threadIdx.x;
     // batch buffers start at zero: columns past a batch's count are computed
     // on whatever the buffers hold, which must be finite
-    for (int t = tid; t < (L.accA - L.X) / 16; t += C::NT) S.X[t] = cplx{0, 0};
+    for (int t = tid; t < (L::accA - L::X) / 16; t += C::NT) S.X()[t] = cplx{0, 0};
     block_barrier();
     if (tid < C::OC) role_B<P, CB>(a, S, g0, g1, tid);
     else if (tid < C::ODA) role_C<P, CB>(a, S, g0, g1, tid);
@@ -798,21 +814,21 @@ __global__ void __launch_bounds__(RoleCfg<P, CB>::NT) k_m2l_roles(EvalArgs a, in
     else role_D<P, CB, true>(a, S, g0, g1, tid, C::ODB);
 }
 
-template<int P, int CB>
+template<int P, int CB, int MINB>
 bool try_launch_roles(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     using C = RoleCfg<P, CB>;
-    const size_t smem = role_smem(C::T, C::T1, a.qdim, CB).total;
+    const size_t smem = RoleLayout<P, CB>::total(a.qdim);
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_roles<P, CB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_roles<P, CB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
     int per_sm = 0;
-    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_roles<P, CB>, C::NT, smem));
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_roles<P, CB, MINB>, C::NT, smem));
     if (per_sm < 1) return false;
     const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
-    k_m2l_roles<P, CB><<<static_cast<unsigned>(grid), C::NT, smem, st>>>(a, g0, g1);
+    k_m2l_roles<P, CB, MINB><<<static_cast<unsigned>(grid), C::NT, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
     return true;
 }
@@ -821,8 +837,14 @@ template<int P>
 void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     if constexpr (P >= 2 && P <= 12) {
-        if (try_launch_roles<P, 8>(a, g0, g1, sms, st)) return;
-        if (try_launch_roles<P, 4>(a, g0, g1, sms, st)) return;
+        // two blocks per SM of 4-column batches measured fastest up to p = 10
+        // (4M-point Plummer, p = 10: 122 ms against 144 ms for one block of
+        // 8-column batches); higher orders keep one block of 8 columns
+        if constexpr (P <= 10) {
+            if (try_launch_roles<P, 4, 2>(a, g0, g1, sms, st)) return;
+        }
+        if (try_launch_roles<P, 8, 1>(a, g0, g1, sms, st)) return;
+        if (try_launch_roles<P, 4, 1>(a, g0, g1, sms, st)) return;
     }
     launch_rows_fallback<P>(a, g0, g1, sms, st);
 }
