@@ -275,7 +275,8 @@ def main():
     value = n * world * args.steps / (total_ms * 1e-3)
 
     # accuracy of the last step against the FP64 direct sum on seeded targets
-    tg = np.random.default_rng(SEED).choice(n, 1000, replace=False)
+    n_check = min(n, 10_000)
+    tg = np.random.default_rng(SEED).choice(n, n_check, replace=False)
     dpot, dfld = sf.direct(pos_h, q_h, tg, ctx=ctx)
     pot_h, fld_h = pot_d.cpu().numpy(), fld_d.cpu().numpy()
     err_pot = float(np.linalg.norm(pot_h[tg] - dpot) / np.linalg.norm(dpot))
@@ -328,7 +329,7 @@ def main():
                        "leaf": LEAF, "distribution": args.dist, "precision": "fp64",
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
                        "depth": tree.depth, **stats},
-            "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": 1000},
+            "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": n_check},
             "phases_ms": {k: round(statistics.mean(ph[k] for ph in phases), 3) for k in phases[0]},
             "roofline": {"bound": "fp64", "kernel": "k_m2l", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
