@@ -138,6 +138,21 @@ int fmm_plan_timings(const fmm_plan* plan, double* ms6);
 int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
                int64_t nt, double* pot, double* field, int where);
 
+/* Direct sums that allocate nothing (no counterpart in the reference).
+   For callers that cannot allocate device memory while they run: a service
+   that holds a fixed device-memory budget for its lifetime, or a caller that
+   cannot wait on an allocation.  Same sums and output layout as fmm_direct;
+   every pointer is device memory of the current device; the work is queued
+   on `stream` (a cudaStream_t) and the call returns without waiting.
+   Scratch is one fixed 8 MiB device array per device, held from the first
+   call until the process exits; the first call on a device looks up its
+   address (set-up), so make that first call before any stream capture.
+   Limit: nt <= 174762 targets per call (FMM_ERR_OVER_BUDGET above it).
+   Every call shares the array: calls that overlap on the GPU (other streams,
+   other host threads) race and corrupt each other's results. */
+int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
+                       int64_t nt, double* pot, double* field, void* stream);
+
 /* Number of kernels this library has launched in this process. */
 int fmm_launch_count(int64_t* count);
 

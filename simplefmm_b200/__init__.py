@@ -71,6 +71,7 @@ def load_library():
         "fmm_evaluate": ([vp, vp, vp, vp, i32], i32),
         "fmm_plan_timings": ([vp, C.POINTER(dbl)], i32),
         "fmm_direct": ([vp, vp, i64, vp, i32, vp, i64, vp, vp, i32], i32),
+        "fmm_direct_noalloc": ([vp, i64, vp, i32, vp, i64, vp, vp, vp], i32),
         "fmm_launch_count": ([C.POINTER(i64)], i32),
     }
     for name, (args, res) in sig.items():

@@ -46,6 +46,15 @@ int fail(int status, const std::string& msg)
     return status;
 }
 
+}  // namespace
+
+namespace sfmm {
+// For entry points defined outside this file.
+int record_failure(int status, const char* msg) { return fail(status, msg); }
+}  // namespace sfmm
+
+namespace {
+
 #define API_TRY try {
 #define API_CATCH                                                              \
     }                                                                          \

@@ -3,6 +3,8 @@
 // in shared memory.  Used to state the FMM error against the exact sum.
 #include "fmm_internal.cuh"
 
+#include <mutex>
+
 namespace sfmm {
 
 std::atomic<long long> g_launches{0};
@@ -98,3 +100,87 @@ void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int q
 }
 
 }  // namespace sfmm
+
+// ------------------------------------------------------------------ direct sum without allocation
+// fmm_direct_noalloc: the same two kernels with their partial sums in a
+// fixed, file-scope device array instead of memory allocated per call.  It is
+// for callers that cannot allocate device memory while they run: callers that
+// hold a fixed device-memory budget for their own lifetime (a solver service
+// that admits work against a budget), and callers that cannot wait on an
+// allocation (growing a memory pool can stall a call for a long time).
+namespace sfmm {
+namespace {
+
+// Partial sums: 6 doubles per (source chunk, target).  8 MiB on every device
+// that loads this library, held until the process exits.
+constexpr int64_t kNoAllocScratchDoubles = int64_t(1) << 20;
+constexpr int64_t kNoAllocMaxTargets = kNoAllocScratchDoubles / 6;    // 174,762
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+
+struct NoAllocDevice {
+    double* scratch = nullptr;     // device address of g_noalloc_scratch
+    int sms = 0;
+};
+
+// Set-up, once per device, with that device current: the device address of
+// the scratch array (its host-side name is only a stand-in) and the SM count.
+NoAllocDevice noalloc_device(int dev)
+{
+    static std::mutex mu;
+    static NoAllocDevice table[64];
+    std::lock_guard<std::mutex> lk(mu);
+    NoAllocDevice& d = table[dev];
+    if (!d.scratch) {
+        double* ptr = nullptr;
+        SFMM_CUDA(cudaGetSymbolAddress(reinterpret_cast<void**>(&ptr), g_noalloc_scratch));
+        int sms = 0;
+        SFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        d.sms = sms;
+        d.scratch = ptr;
+    }
+    return d;
+}
+
+}  // namespace
+}  // namespace sfmm
+
+extern "C" int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
+                                  int64_t nt, double* pot, double* field, void* stream)
+{
+    using namespace sfmm;
+    try {
+        if (!xyz || !Q || !targets) return record_failure(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (qdim < 1 || qdim > 3) return record_failure(FMM_ERR_UNSUPPORTED, "qdim must be 1, 2 or 3");
+        if (field && qdim == 2) return record_failure(FMM_ERR_UNSUPPORTED, "the field needs qdim 1 or 3");
+        if (n <= 0 || nt < 0) return record_failure(FMM_ERR_INVALID_ARGUMENT, "bad sizes");
+        if (nt > kNoAllocMaxTargets)
+            return record_failure(FMM_ERR_OVER_BUDGET,
+                                  "fmm_direct_noalloc takes at most 174762 targets per call (8 MiB of fixed scratch)");
+        if (nt == 0) return FMM_OK;
+        int dev = 0;
+        SFMM_CUDA(cudaGetDevice(&dev));
+        if (dev < 0 || dev >= 64) return record_failure(FMM_ERR_UNSUPPORTED, "device index above 63");
+        const NoAllocDevice d = noalloc_device(dev);
+        cudaStream_t st = static_cast<cudaStream_t>(stream);
+        // chunking as direct_sum, capped by the scratch size
+        const int64_t gx = (nt + kThreads - 1) / kThreads;
+        int64_t nchunk = std::max<int64_t>(1, (int64_t(d.sms) * 8 + gx - 1) / gx);
+        nchunk = std::min<int64_t>(nchunk, std::max<int64_t>(1, n / (4 * kThreads)));
+        nchunk = std::min<int64_t>(nchunk, kNoAllocScratchDoubles / (6 * nt));
+        nchunk = std::min<int64_t>(nchunk, 65535);
+        const int64_t chunk = (n + nchunk - 1) / nchunk;
+        // every (chunk, target) slot of the scratch is written before it is
+        // read, so nothing left by an earlier call needs clearing
+        k_direct<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(nchunk)), kThreads, 0, st>>>(
+            xyz, n, Q, qdim, targets, nt, chunk, d.scratch);
+        SFMM_CHECK_LAUNCH();
+        k_direct_sum<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, st>>>(d.scratch, nt, static_cast<int>(nchunk),
+                                                                            qdim, pot, field);
+        SFMM_CHECK_LAUNCH();
+        return FMM_OK;
+    } catch (const sfmm::Error& e) {
+        return record_failure(e.status, e.what());
+    } catch (const std::exception& e) {
+        return record_failure(FMM_ERR_CUDA, e.what());
+    }
+}

@@ -30,6 +30,9 @@ struct Error : std::runtime_error {
 
 extern std::atomic<long long> g_launches;
 
+// Records the calling thread's last-error message (fmm_last_error) and returns status.
+int record_failure(int status, const char* msg);
+
 #define SFMM_CHECK_LAUNCH()                   \
     do {                                      \
         ::sfmm::g_launches.fetch_add(1);      \
