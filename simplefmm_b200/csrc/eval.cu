@@ -332,6 +332,7 @@ void plan_init(Plan& pl)
             for (int k = 0; k + 1 < pl.ipow_w; ++k) r[k + 1] = r[k] / rho;
         }
     upload(pl.ipow, ipw, st);
+    build_m2l_fragments(pl, st);
     pl.M.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LA.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
@@ -400,6 +401,10 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.l2l1_g = pl.l2l1_g.ptr;
     a.ipow = pl.ipow.ptr;
     a.ipow_w = pl.ipow_w;
+    a.rfrag = pl.rfrag.ptr;
+    a.rfrag_nf = pl.rfrag_nf;
+    a.tzfrag = pl.tzfrag.ptr;
+    a.tzl = pl.tzl.ptr;
     a.M = reinterpret_cast<cplx*>(pl.M.ptr);
     a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
     a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);

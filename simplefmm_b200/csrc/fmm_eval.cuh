@@ -48,6 +48,13 @@ struct EvalArgs {
     const double* l2l1_g;
     const double* ipow;                   // rho^{-(k+1)} per (level, |d|^2), k = 0..2p+2
     int ipow_w;
+    // M2L operators in tensor-core fragment order (m2l.cu): rotation /
+    // inverse rotation per class, z-translation, and the order-p translation
+    // column that the potential local adds to the field local's sources
+    const double* rfrag;
+    int rfrag_nf;                         // fragments per class and matrix
+    const double* tzfrag;
+    const double* tzl;
     cplx* M;
     cplx* LA;
     cplx* LB;
@@ -61,6 +68,8 @@ struct Plan {
     int p = 0, T = 0, T1 = 0, qdim = 1, precision = FMM_PRECISION_FP64;
     int rot_len = 0, tzx_len = 0, ipow_w = 0;
     DevBuf<double> rot, tzx, eil, echild, eparent, eparent1, m2m_g, l2l_g, l2l1_g, ipow;
+    DevBuf<double> rfrag, tzfrag, tzl;
+    int rfrag_nf = 0;
     DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
@@ -69,6 +78,9 @@ struct Plan {
 };
 
 void plan_init(Plan& pl);
+// Fills pl.rfrag / pl.tzfrag / pl.tzl from the uploaded rotation and
+// translation tables (m2l.cu).
+void build_m2l_fragments(Plan& pl, cudaStream_t st);
 void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
 void plan_read_timings(Plan& pl, double* ms6);
 

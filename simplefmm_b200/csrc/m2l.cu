@@ -24,6 +24,8 @@
 // The kernel is instantiated per order p so the register rows are indexed
 // statically.
 #include "eval_util.cuh"
+
+#include <type_traits>
 #include "fmm_tables.h"
 
 namespace sfmm {
@@ -833,9 +835,496 @@ bool try_launch_roles(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaSt
     return true;
 }
 
+// ------------------------------------------------------------------ FP64 tensor-core kernel
+// The same rotate / translate / rotate-back arithmetic as matrix products on
+// the FP64 tensor cores (mma.sync m8n8k4 f64: A 8x4 row-major, B 4x8
+// column-major, D 8x8; 256 FMAs per warp instruction with every operand in
+// registers).  A tile is up to 8 columns (pair x charge component) of one
+// rotation class, the MMA's N.  For a tile:
+//   X     = e^{i m phi} M_src                      [coef t][col], re / im apart
+//   W_n   = rho^{-n} (P_n Re X_n, Q_n Im X_n)       per order n: A = P_n / Q_n rows
+//   LzB^k = rho^{-(j+1)} Tz_k W^k  (sources <= p-1)  per azimuth k: A = Tz_k rows,
+//           the same A for the re and im halves
+//   LzA^k = LzB^k + rho^{-(j+1)} tz[j][p] W_p^k      (rows j <= p)
+//   L_j   = e^{-i m phi} (PB_j Re Lz_j, QB_j Im Lz_j)   for LzA and LzB
+// then the tile's columns are added into their target in column order
+// (deterministic).  Operators come from tables in fragment order (one
+// coalesced 256-byte load per fragment, L1/L2 resident).  Zero-padded
+// operator rows and columns make out-of-range operand rows contribute
+// nothing; those rows are kept finite.  Four block barriers per tile; two
+// blocks per SM overlap each other's barriers; the next tile's source
+// moments are copied with cp.async two phases ahead.
+
+__host__ __device__ constexpr int mma_rt(int n) { return (n + 8) / 8; }   // 8-row tiles of order n
+__host__ __device__ constexpr int mma_kc(int n) { return (n + 4) / 4; }   // 4-wide K chunks of order n
+__host__ __device__ constexpr int mma_foff(int n)                         // fragments of orders < n
+{
+    int s = 0;
+    for (int i = 0; i < n; ++i) s += mma_rt(i) * mma_kc(i);
+    return s;
+}
+// z-translation for azimuth k: rows j = k..P+1, field-local sources n' = k..P-1
+__host__ __device__ constexpr int tz_rt(int P, int k) { return (P + 2 - k + 7) / 8; }
+__host__ __device__ constexpr int tz_kc(int P, int k) { return k < P ? (P - k + 3) / 4 : 0; }
+__host__ __device__ constexpr int tz_foff(int P, int k)
+{
+    int s = 0;
+    for (int i = 0; i < k; ++i) s += tz_rt(P, i) * tz_kc(P, i);
+    return s;
+}
+// first row of azimuth k in the azimuth-major layout of W (n' = k..P)
+__host__ __device__ constexpr int az_off(int P, int k) { return k * (P + 1) - k * (k - 1) / 2; }
+
+__device__ __forceinline__ void mma884(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+struct MmaMeta {
+    int cls, ncol, dsq, pad;
+    int src[8], bq[8], sb[8], pidx[8];
+};
+
+// Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
+template<int B, int E, typename F>
+__device__ __forceinline__ void static_for(F&& f)
+{
+    if constexpr (B < E) {
+        f(std::integral_constant<int, B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+// padded leading dimension of a [col][row] operand buffer: >= rows + 4 (K
+// chunks read up to 3 rows past an order) and = 4 mod 16 doubles, which
+// makes the B-fragment loads (4 rows x 8 columns) bank-conflict free
+__host__ __device__ constexpr int mma_ld(int rows) { return ((rows + 4 + 11) / 16) * 16 + 4; }
+// rotation jobs (n, rt), n = P..0: index of the first job of order n
+__host__ __device__ constexpr int rot_job0(int P, int n)
+{
+    int s = 0;
+    for (int i = P; i > n; --i) s += mma_rt(i);
+    return s;
+}
+// translation jobs (k, rt), k = 0..P+1: index of the first job of azimuth k
+__host__ __device__ constexpr int tz_job0(int P, int k)
+{
+    int s = 0;
+    for (int i = 0; i < k; ++i) s += tz_rt(P, i);
+    return s;
+}
+
+template<int P>
+struct MmaLayout {
+    static constexpr int T = (P + 1) * (P + 2) / 2;
+    static constexpr int T1 = (P + 2) * (P + 3) / 2;
+    static constexpr int LD = mma_ld(T), LD1 = mma_ld(T1);        // column strides (doubles)
+    static constexpr int ent_src = 0;
+    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
+    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
+    static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
+    static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
+    static constexpr int cls_off = al16(cls_cnt + 4 * 72);
+    static constexpr int bat_off = al16(cls_off + 4 * 72);
+    static constexpr int meta = al16(bat_off + 4 * 72);
+    static constexpr int tm = al16(meta + int(sizeof(MmaMeta)) * 3);
+    static constexpr int Xraw = al16(tm + T1);                    // 2 x [col][T] complex (cp.async)
+    static constexpr int X = al16(Xraw + 2 * 8 * T * 16);          // re, im: [col][LD] doubles each
+    static constexpr int W = al16(X + 2 * 8 * LD * 8);             // azimuth-major rows
+    static constexpr int LzA = al16(W + 2 * 8 * LD * 8);
+    static constexpr int LzB = al16(LzA + 2 * 8 * LD * 8);         // [col][LD1]
+    static constexpr int acc = al16(LzB + 2 * 8 * LD1 * 8);        // [8 qd][T] then [8 qd][T1] complex
+    __host__ __device__ static constexpr int total(int qd) { return al16(acc + 16 * 8 * qd * (T + T1)); }
+};
+
+template<int P>
+__global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int64_t g1)
+{
+    using L = MmaLayout<P>;
+    constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 256;
+    extern __shared__ __align__(16) unsigned char sm[];
+    int* ent_src = reinterpret_cast<int*>(sm + L::ent_src);
+    int* ent_code = reinterpret_cast<int*>(sm + L::ent_code);
+    short* sorted = reinterpret_cast<short*>(sm + L::sorted);
+    unsigned char* cls = sm + L::cls;
+    int* cls_cnt = reinterpret_cast<int*>(sm + L::cls_cnt);
+    int* cls_off = reinterpret_cast<int*>(sm + L::cls_off);
+    int* bat_off = reinterpret_cast<int*>(sm + L::bat_off);
+    MmaMeta* meta = reinterpret_cast<MmaMeta*>(sm + L::meta);
+    unsigned char* tm = sm + L::tm;
+    cplx* Xraw = reinterpret_cast<cplx*>(sm + L::Xraw);
+    double* Xre = reinterpret_cast<double*>(sm + L::X);
+    double* Xim = Xre + 8 * LD;
+    double* Wre = reinterpret_cast<double*>(sm + L::W);
+    double* Wim = Wre + 8 * LD;
+    double* Are = reinterpret_cast<double*>(sm + L::LzA);
+    double* Aim = Are + 8 * LD;
+    double* Bre = reinterpret_cast<double*>(sm + L::LzB);
+    double* Bim = Bre + 8 * LD1;
+    const int qd = a.qdim;
+    cplx* accA = reinterpret_cast<cplx*>(sm + L::acc);
+    cplx* accB = accA + 8 * qd * T;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int lr = lane >> 2, lc = lane & 3;                       // fragment row / column group
+    // B-fragment element (K row lc, column lr) and D-fragment columns 2 lc + {0, 1}
+    const int bofs = lr * LD + lc, bofs1 = lr * LD1 + lc;
+    const int d0 = (2 * lc) * LD, d1 = (2 * lc + 1) * LD, e0 = (2 * lc) * LD1, e1 = (2 * lc + 1) * LD1;
+    // operand buffers start at zero: padding rows and unused columns must be finite
+    for (int e = tid; e < (L::acc - L::X) / 8; e += NT) Xre[e] = 0.0;
+    for (int t = tid; t < T1; t += NT) {
+        int n, m;
+        tri_nm(t, n, m);
+        tm[t] = static_cast<unsigned char>(m);
+    }
+    __syncthreads();
+    const double* rf = a.rfrag;
+    const int NF = a.rfrag_nf;
+
+    // column table of tile b (threads k < 8); c: class cursor
+    auto make_meta = [&](int b, int k, MmaMeta& M, int& c) {
+        while (bat_off[c + 1] <= b) ++c;
+        const int col0 = (b - bat_off[c]) * 8;
+        const int ncol = min(8, cls_cnt[c] * qd - col0);
+        if (k < ncol) {
+            const int col = col0 + k;
+            const int pair = col / qd;
+            const int e = sorted[cls_off[c] + pair];
+            const int code = ent_code[e];
+            const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
+            const int bq = col - pair * qd;
+            M.src[k] = ent_src[e];
+            M.bq[k] = bq;
+            M.sb[k] = ((code >> 9) & 7) * qd + bq;
+            M.pidx[k] = 7 * (dj + 3) + (di + 3);
+            if (k == 0) {
+                M.cls = c;
+                M.ncol = ncol;
+                M.dsq = di * di + dj * dj + dk * dk;
+            }
+        } else {
+            M.src[k] = 0;
+            M.bq[k] = 0;
+            M.sb[k] = 0;
+            M.pidx[k] = 24;
+        }
+    };
+    // raw source moments of tile b -> Xraw[b & 1] (asynchronous)
+    auto issue = [&](int b) {
+        const MmaMeta& M = meta[b % 3];
+        const int ncol = M.ncol;
+        cplx* xr = Xraw + (b & 1) * 8 * T;
+        for (int e = tid; e < 8 * T; e += NT) {
+            const int c = e / T, t = e - c * T;
+            if (c < ncol) cp_async16(xr + e, a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
+        }
+        cp_async_commit();
+    };
+    // X = e^{i m phi} M for tile b, column-major
+    auto phase_in = [&](int b) {
+        const MmaMeta& M = meta[b % 3];
+        const int ncol = M.ncol;
+        const cplx* xr = Xraw + (b & 1) * 8 * T;
+        for (int e = tid; e < 8 * T; e += NT) {
+            const int c = e / T, t = e - c * T;
+            if (c < ncol) {
+                const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
+                const cplx v = cmul(cplx{ph.x, ph.y}, xr[e]);
+                Xre[c * LD + t] = v.re;
+                Xim[c * LD + t] = v.im;
+            }
+        }
+    };
+
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        const int nc = a.nchild[g];
+        if (nc == 0) continue;
+        const int cb = a.child_beg[g];
+        const int lt = level_of(a, g) + 1;
+        // ---- group set-up: gather, stable class sort, tiles
+        {
+            const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
+            for (int s = 0; s < nc; ++s) {
+                const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
+                for (int e = q0 + tid; e < q1; e += NT) {
+                    const int code = a.il_code[e0 + e];
+                    ent_src[e] = a.il_src[e0 + e];
+                    ent_code[e] = code | (s << 9);
+                    cls[e] = static_cast<unsigned char>(
+                        rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
+                }
+            }
+            for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = cplx{0, 0};
+            __syncthreads();
+            for (int cl = tid; cl < kNumClasses; cl += NT) {
+                int cnt = 0;
+                for (int e = 0; e < E; ++e) cnt += cls[e] == cl;
+                cls_cnt[cl] = cnt;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int s = 0, k = 0;
+                for (int c = 0; c < kNumClasses; ++c) {
+                    cls_off[c] = s;
+                    bat_off[c] = k;
+                    s += cls_cnt[c];
+                    k += (cls_cnt[c] * qd + 7) / 8;
+                }
+                cls_off[kNumClasses] = s;
+                bat_off[kNumClasses] = k;
+            }
+            __syncthreads();
+            for (int cl = tid; cl < kNumClasses; cl += NT) {
+                int pos = cls_off[cl];
+                for (int e = 0; e < E; ++e)
+                    if (cls[e] == cl) sorted[pos++] = static_cast<short>(e);
+            }
+            __syncthreads();
+        }
+        const int nbat = bat_off[kNumClasses];
+        int cur = 0;                                      // class cursor of threads < 8
+        if (tid < 8 && nbat > 0) make_meta(0, tid, meta[0], cur);
+        __syncthreads();
+        if (nbat > 0) issue(0);
+        if (tid < 8 && nbat > 1) make_meta(1, tid, meta[1], cur);
+        cp_async_wait_all();
+        __syncthreads();
+        if (nbat > 0) phase_in(0);
+        if (nbat > 1) issue(1);
+        __syncthreads();
+
+        for (int b = 0; b < nbat; ++b) {
+            const MmaMeta& M = meta[b % 3];
+            const double* ipw = a.ipow + (int64_t(lt) * 28 + M.dsq) * a.ipow_w;
+            const double* rfc = rf + int64_t(M.cls) * NF * 4 * 32 + lane;
+            // ---- rotation: jobs (n, rt), largest orders first, round robin over warps
+            static_for<0, P + 1>([&](auto nn) {
+                constexpr int n = P - decltype(nn)::value;
+                constexpr int KC = mma_kc(n), base = n * (n + 1) / 2;
+                static_for<0, mma_rt(n)>([&](auto rr) {
+                    constexpr int rt = decltype(rr)::value;
+                    if ((rot_job0(P, n) + rt) % 8 != warp) return;
+                    const double* fr = rfc + (mma_foff(n) + rt * KC) * 4 * 32;
+                    double aP[KC], aQ[KC];
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) {
+                        aP[kc] = __ldg(fr + (kc * 4 + 0) * 32);
+                        aQ[kc] = __ldg(fr + (kc * 4 + 1) * 32);
+                    }
+                    double r0 = 0, r1 = 0, i0 = 0, i1 = 0;
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) {
+                        mma884(r0, r1, aP[kc], Xre[bofs + base + 4 * kc]);
+                        mma884(i0, i1, aQ[kc], Xim[bofs + base + 4 * kc]);
+                    }
+                    const int m = 8 * rt + lr;
+                    if (m <= n) {
+                        const double sc = n ? ipw[n - 1] : 1.0;
+                        const int u = az_off(P, m) + (n - m);
+                        Wre[d0 + u] = r0 * sc;
+                        Wre[d1 + u] = r1 * sc;
+                        Wim[d0 + u] = i0 * sc;
+                        Wim[d1 + u] = i1 * sc;
+                    }
+                });
+            });
+            __syncthreads();
+            // ---- z-translation: jobs (k, rt); the same operator for re and im
+            static_for<0, P + 2>([&](auto kk) {
+                constexpr int k = decltype(kk)::value;
+                constexpr int KC = tz_kc(P, k), u0 = az_off(P, k);
+                static_for<0, tz_rt(P, k)>([&](auto rr) {
+                    constexpr int rt = decltype(rr)::value;
+                    if ((tz_job0(P, k) + rt) % 8 != warp) return;
+                    const double* fz = a.tzfrag + (tz_foff(P, k) + rt * KC) * 32 + lane;
+                    double az[KC > 0 ? KC : 1];
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) az[kc] = __ldg(fz + kc * 32);
+                    double r0 = 0, r1 = 0, i0 = 0, i1 = 0;
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) {
+                        mma884(r0, r1, az[kc], Wre[bofs + u0 + 4 * kc]);
+                        mma884(i0, i1, az[kc], Wim[bofs + u0 + 4 * kc]);
+                    }
+                    const int j = k + 8 * rt + lr;
+                    if (j <= P + 1) {
+                        const double sc = ipw[j];
+                        const int t1 = j * (j + 1) / 2 + k;
+                        Bre[e0 + t1] = r0 * sc;
+                        Bre[e1 + t1] = r1 * sc;
+                        Bim[e0 + t1] = i0 * sc;
+                        Bim[e1 + t1] = i1 * sc;
+                        if constexpr (k <= P) {
+                            if (j <= P) {
+                                const double tl = a.tzl[k * (P + 2) + j];
+                                constexpr int up = u0 + (P - k);          // n' = p
+                                Are[d0 + t1] = fma(tl, Wre[d0 + up], r0) * sc;
+                                Are[d1 + t1] = fma(tl, Wre[d1 + up], r1) * sc;
+                                Aim[d0 + t1] = fma(tl, Wim[d0 + up], i0) * sc;
+                                Aim[d1 + t1] = fma(tl, Wim[d1 + up], i1) * sc;
+                            }
+                        }
+                    }
+                });
+            });
+            // column table of tile b + 2 (its ring slot is free)
+            if (tid < 8 && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
+            __syncthreads();
+            // ---- inverse rotation + phase, in place: one warp per order j (all its rows)
+            {
+                const int pc0 = M.pidx[2 * lc] * (P + 2), pc1 = M.pidx[2 * lc + 1] * (P + 2);
+                static_for<0, P + 2>([&](auto jj) {
+                    constexpr int j = P + 1 - decltype(jj)::value;
+                    if (decltype(jj)::value % 8 != warp) return;
+                    constexpr int KC = mma_kc(j), RT = mma_rt(j), base = j * (j + 1) / 2;
+                    constexpr bool hasA = j <= P;
+                    const double* fr = rfc + mma_foff(j) * 4 * 32;
+                    double ar[RT][2] = {}, ai[RT][2] = {}, br[RT][2] = {}, bi[RT][2] = {};
+#pragma unroll
+                    for (int rt = 0; rt < RT; ++rt) {
+                        double aPB[KC], aQB[KC];
+#pragma unroll
+                        for (int kc = 0; kc < KC; ++kc) {
+                            aPB[kc] = __ldg(fr + ((rt * KC + kc) * 4 + 2) * 32);
+                            aQB[kc] = __ldg(fr + ((rt * KC + kc) * 4 + 3) * 32);
+                        }
+#pragma unroll
+                        for (int kc = 0; kc < KC; ++kc) {
+                            mma884(br[rt][0], br[rt][1], aPB[kc], Bre[bofs1 + base + 4 * kc]);
+                            mma884(bi[rt][0], bi[rt][1], aQB[kc], Bim[bofs1 + base + 4 * kc]);
+                            if constexpr (hasA) {
+                                mma884(ar[rt][0], ar[rt][1], aPB[kc], Are[bofs + base + 4 * kc]);
+                                mma884(ai[rt][0], ai[rt][1], aQB[kc], Aim[bofs + base + 4 * kc]);
+                            }
+                        }
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int rt = 0; rt < RT; ++rt) {
+                        const int m = 8 * rt + lr;
+                        if (m > j) continue;
+                        const int t = base + m;
+                        const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0 + m);
+                        const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1 + m);
+                        Bre[e0 + t] = f0.x * br[rt][0] + f0.y * bi[rt][0];
+                        Bim[e0 + t] = f0.x * bi[rt][0] - f0.y * br[rt][0];
+                        Bre[e1 + t] = f1.x * br[rt][1] + f1.y * bi[rt][1];
+                        Bim[e1 + t] = f1.x * bi[rt][1] - f1.y * br[rt][1];
+                        if constexpr (hasA) {
+                            Are[d0 + t] = f0.x * ar[rt][0] + f0.y * ai[rt][0];
+                            Aim[d0 + t] = f0.x * ai[rt][0] - f0.y * ar[rt][0];
+                            Are[d1 + t] = f1.x * ar[rt][1] + f1.y * ai[rt][1];
+                            Aim[d1 + t] = f1.x * ai[rt][1] - f1.y * ar[rt][1];
+                        }
+                    }
+                });
+            }
+            cp_async_wait_all();                          // tile b + 1's moments
+            __syncthreads();
+            // ---- accumulate tile b into the targets (column order); phase tile b + 1 in
+            {
+                const int ncol = M.ncol;
+                int sb[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) sb[c] = M.sb[c];
+                for (int t = tid; t < T + T1; t += NT) {
+                    const bool isA = t < T;
+                    const int r = isA ? t : t - T;
+                    const double* sre = isA ? Are + r : Bre + r;
+                    const double* sim = isA ? Aim + r : Bim + r;
+                    const int ld = isA ? LD : LD1;
+                    cplx* acc = isA ? accA + r : accB + r;
+                    const int stride = isA ? T : T1;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        if (c < ncol) {
+                            cplx& d = acc[sb[c] * stride];
+                            d.re += sre[c * ld];
+                            d.im += sim[c * ld];
+                        }
+                }
+                if (b + 1 < nbat) phase_in(b + 1);
+                if (b + 2 < nbat) issue(b + 2);
+            }
+            __syncthreads();
+        }
+        if (a.want_pot)
+            for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = accA[e];
+        if (a.want_field)
+            for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = accB[e];
+        __syncthreads();
+    }
+}
+
+template<int P>
+bool try_launch_mma(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
+{
+    const size_t smem = MmaLayout<P>::total(a.qdim);
+    int dev = 0, optin = 0;
+    SFMM_CUDA(cudaGetDevice(&dev));
+    SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > size_t(optin)) return false;
+    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0;
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P>, 256, smem));
+    if (per_sm < 1) return false;
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
+    k_m2l_mma<P><<<static_cast<unsigned>(grid), 256, smem, st>>>(a, g0, g1);
+    SFMM_CHECK_LAUNCH();
+    return true;
+}
+
+// Fragment-order tables (device): rotation matrices of every class for
+// orders <= P + 1 and the z-translation operator.
+__global__ void k_frag_rot(const double* __restrict__ rot, const int* __restrict__ rot_off, int rot_len, int P, int NF,
+                           double* __restrict__ out)
+{
+    const int64_t total = int64_t(kNumClasses) * NF * 4 * 32;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+        const int lane = static_cast<int>(idx & 31), mat = static_cast<int>((idx >> 5) & 3);
+        const int64_t rest = idx >> 7;
+        const int f = static_cast<int>(rest % NF), c = static_cast<int>(rest / NF);
+        int n = 0;
+        while (n < P + 1 && mma_foff(n + 1) <= f) ++n;
+        const int KC = mma_kc(n);
+        const int rt = (f - mma_foff(n)) / KC, kc = (f - mma_foff(n)) - rt * KC;
+        const int row = 8 * rt + (lane >> 2), col = 4 * kc + (lane & 3);
+        double v = 0.0;
+        if (row <= n && col <= n)
+            v = rot[int64_t(c) * rot_len + rot_off[n] + mat * (n + 1) * (n + 1) + row * (n + 1) + col];
+        out[idx] = v;
+    }
+}
+
+__global__ void k_frag_tz(const double* __restrict__ tzx, const int* __restrict__ tzx_off, int P, int NFZ,
+                          double* __restrict__ out, double* __restrict__ tzl)
+{
+    const int total = NFZ * 32;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < total; idx += gridDim.x * blockDim.x) {
+        const int lane = idx & 31, f = idx >> 5;
+        int k = 0;
+        while (k < P + 1 && tz_foff(P, k + 1) <= f) ++k;
+        const int KC = tz_kc(P, k);
+        const int rt = (f - tz_foff(P, k)) / KC, kc = (f - tz_foff(P, k)) - rt * KC;
+        const int j = k + 8 * rt + (lane >> 2), np = k + 4 * kc + (lane & 3);
+        double v = 0.0;
+        if (j <= P + 1 && np <= P - 1) v = tzx[tzx_off[k] + (j - k) * (P + 1 - k) + (np - k)];
+        out[idx] = v;
+    }
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < (P + 1) * (P + 2); idx += gridDim.x * blockDim.x) {
+        const int k = idx / (P + 2), j = idx - k * (P + 2);
+        tzl[idx] = (j >= k && j <= P) ? tzx[tzx_off[k] + (j - k) * (P + 1 - k) + (P - k)] : 0.0;
+    }
+}
+
 template<int P>
 void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
+    if constexpr (P >= 2) {
+        if (try_launch_mma<P>(a, g0, g1, sms, st)) return;
+    }
     if constexpr (P >= 2 && P <= 12) {
         // two blocks per SM of 4-column batches measured fastest up to p = 10
         // (4M-point Plummer, p = 10: 122 ms against 144 ms for one block of
@@ -850,6 +1339,20 @@ void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream
 }
 
 }  // namespace
+
+void build_m2l_fragments(Plan& pl, cudaStream_t st)
+{
+    const int P = pl.p;
+    pl.rfrag_nf = mma_foff(P + 2);
+    pl.rfrag.alloc(size_t(kNumClasses) * pl.rfrag_nf * 4 * 32, st);
+    const int nfz = std::max(tz_foff(P, P + 2), 1);
+    pl.tzfrag.alloc(size_t(nfz) * 32, st);
+    pl.tzl.alloc(size_t(P + 1) * (P + 2), st);
+    k_frag_rot<<<256, 256, 0, st>>>(pl.rot.ptr, pl.rot_off.ptr, pl.rot_len, P, pl.rfrag_nf, pl.rfrag.ptr);
+    SFMM_CHECK_LAUNCH();
+    k_frag_tz<<<16, 256, 0, st>>>(pl.tzx.ptr, pl.tzx_off.ptr, P, tz_foff(P, P + 2), pl.tzfrag.ptr, pl.tzl.ptr);
+    SFMM_CHECK_LAUNCH();
+}
 
 void launch_m2l(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
