@@ -127,6 +127,14 @@ def fp64_peak_tflops(torch) -> float:
     return best
 
 
+DATA_DESC = {
+    "plummer": "synthetic (seeded Plummer sphere, a=1, r<=10; charges U[-1,1])",
+    "uniform": "synthetic (seeded uniform unit cube; charges U[-1,1])",
+    "shell": "synthetic (seeded thin spherical shell r=1, thickness 0.01; charges U[-1,1])",
+    "gauss2": "synthetic (seeded two Gaussian clusters sigma 0.05, centres 0.5 apart, clipped; charges U[-1,1])",
+}
+
+
 def traffic_per_pair():
     """DRAM bytes per M2L pair from the committed ncu summary, if present."""
     f = ROOT / "profiles" / "m2l_fp64_plummer.md"
@@ -198,6 +206,7 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=100_000)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -239,7 +248,7 @@ def main():
         pot_d.zero_()
         fld_d.zero_()
         tree = sf.Tree(pos_d, 20, LEAF, ctx=ctx)
-        plan = sf.Plan(tree, p, 1)
+        plan = sf.Plan(tree, p, 1, precision=args.precision)
         plan.evaluate(q_d, pot_d, fld_d)
         live.extend([plan, tree])
         return tree, plan
@@ -297,7 +306,7 @@ def main():
         pot_p, fld_p = pin(np.zeros(n)), pin(np.zeros((n, 3)))
         ctx2 = sf.Context(local)
         tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
-        sf.Plan(tr, p, 1).evaluate(q_p, pot_p, fld_p)
+        sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
         et = []
         for _ in range(args.steps):
             pot_p[:] = 0
@@ -307,7 +316,7 @@ def main():
             t0 = time.perf_counter()
             tr.close()
             tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
-            sf.Plan(tr, p, 1).evaluate(q_p, pot_p, fld_p)
+            sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
             et.append(time.perf_counter() - t0)
         tr.close()
         e2e = {"value": n * world / statistics.mean(et), "unit": "points/s",
@@ -323,10 +332,11 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded Plummer sphere, a=1, r<=10; charges U[-1,1])",
-            "config": {"workload": f"{args.dist}_n{n}_p{p}_leaf{LEAF}_fp64_potential+field", "n": n, "p": p,
-                       "leaf": LEAF, "distribution": args.dist, "precision": "fp64",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
+            "data": DATA_DESC.get(args.dist, f"synthetic (seeded {args.dist})"),
+            "config": {"workload": f"{args.dist}_n{n}_p{p}_leaf{LEAF}_{args.precision}_potential+field", "n": n,
+                       "p": p, "leaf": LEAF, "distribution": args.dist, "precision": args.precision,
                        "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
                        "depth": tree.depth, **stats},
             "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": n_check},

@@ -263,7 +263,8 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
     *out = nullptr;
     if (p < 0 || p > sfmm::kMaxOrder) return fail(FMM_ERR_UNSUPPORTED, "expansion order must be in [0, 16]");
     if (qdim < 1 || qdim > 3) return fail(FMM_ERR_UNSUPPORTED, "charge components N must be 1, 2 or 3");
-    if (precision != FMM_PRECISION_FP64) return fail(FMM_ERR_UNSUPPORTED, "only the FP64 precision is available");
+    if (precision != FMM_PRECISION_FP64 && precision != FMM_PRECISION_MIXED)
+        return fail(FMM_ERR_INVALID_ARGUMENT, "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
     bind(*tree->t.ctx);
     auto* pl = new fmm_plan;
     pl->owner = tree;

@@ -378,6 +378,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.qdim = pl.qdim;
     a.want_pot = pot != nullptr;
     a.want_field = field != nullptr;
+    a.mixed = pl.precision == FMM_PRECISION_MIXED;
     a.kf = a.want_pot ? pl.qdim : 0;
     a.K = a.kf + (a.want_field ? 3 : 0);
     a.rot = pl.rot.ptr;
@@ -405,6 +406,11 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.rfrag_nf = pl.rfrag_nf;
     a.tzfrag = pl.tzfrag.ptr;
     a.tzl = pl.tzl.ptr;
+    a.rf32 = pl.rf32.ptr;
+    a.rf32_nf = pl.rf32_nf;
+    a.tz32 = pl.tz32.ptr;
+    a.tz32_nf = pl.tz32_nf;
+    a.tzl32 = pl.tzl32.ptr;
     a.M = reinterpret_cast<cplx*>(pl.M.ptr);
     a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
     a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);

@@ -28,6 +28,7 @@ struct EvalArgs {
     const int2* nr;
     int p, T, T1, qdim;
     int want_pot, want_field;
+    int mixed;                            // FMM_PRECISION_MIXED: FP32 near field, tensor-core M2L
     int K;                                // output components: qdim (if pot) + 3 (if field)
     int kf;                               // first field output component
     const double* rot;                    // rotation classes up to order p + 1
@@ -55,6 +56,13 @@ struct EvalArgs {
     int rfrag_nf;                         // fragments per class and matrix
     const double* tzfrag;
     const double* tzl;
+    // mixed precision: FP32 operators in TF32 fragment order (per class, the
+    // z-translation pre-scaled by the class's distance)
+    const float* rf32;
+    int rf32_nf;
+    const float* tz32;
+    int tz32_nf;
+    const float* tzl32;
     cplx* M;
     cplx* LA;
     cplx* LB;
@@ -70,6 +78,8 @@ struct Plan {
     DevBuf<double> rot, tzx, eil, echild, eparent, eparent1, m2m_g, l2l_g, l2l1_g, ipow;
     DevBuf<double> rfrag, tzfrag, tzl;
     int rfrag_nf = 0;
+    DevBuf<float> rf32, tz32, tzl32;
+    int rf32_nf = 0, tz32_nf = 0;
     DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;

@@ -1319,10 +1319,544 @@ __global__ void k_frag_tz(const double* __restrict__ tzx, const int* __restrict_
     }
 }
 
+// ------------------------------------------------------------------ mixed precision (3xTF32)
+// The tensor-core kernel above in FP32 with TF32 tensor cores
+// (mma.sync m16n8k8 tf32: A 16x8 row-major, B 8x8 column-major, D 16x8 f32),
+// each product taken as three TF32 products of the split operands,
+// a b ~ a_hi b_hi + a_hi b_lo + a_lo b_hi (x_hi = tf32(x), x_lo = tf32(x - x_hi)),
+// accumulated in FP32.  To keep FP32 in range the expansions are scaled by the
+// box size s of the level: X~_n = s^-n X_n in, L_j = s^-(j+1) L~_j out, and
+// the z-translation is pre-scaled per class by rho^-(j+n'+1) with rho the
+// centre distance in box sizes (2 .. sqrt 27), so every operand is O(1).
+// Moments and the per-target sums stay in FP64.
+
+__host__ __device__ constexpr int tf_rt(int n) { return (n + 16) / 16; }   // 16-row tiles of order n
+__host__ __device__ constexpr int tf_kc(int n) { return (n + 8) / 8; }     // 8-wide K chunks of order n
+__host__ __device__ constexpr int tf_foff(int n)
+{
+    int s = 0;
+    for (int i = 0; i < n; ++i) s += tf_rt(i) * tf_kc(i);
+    return s;
+}
+__host__ __device__ constexpr int tf_zrt(int P, int k) { return (P + 2 - k + 15) / 16; }
+__host__ __device__ constexpr int tf_zkc(int P, int k) { return k < P ? (P - k + 7) / 8 : 0; }
+__host__ __device__ constexpr int tf_zoff(int P, int k)
+{
+    int s = 0;
+    for (int i = 0; i < k; ++i) s += tf_zrt(P, i) * tf_zkc(P, i);
+    return s;
+}
+__host__ __device__ constexpr int tf_rjob0(int P, int n)
+{
+    int s = 0;
+    for (int i = P; i > n; --i) s += tf_rt(i);
+    return s;
+}
+__host__ __device__ constexpr int tf_zjob0(int P, int k)
+{
+    int s = 0;
+    for (int i = 0; i < k; ++i) s += tf_zrt(P, i);
+    return s;
+}
+// column stride of an FP32 operand buffer: >= rows + 8, = 4 mod 32 (conflict-free fragments)
+__host__ __device__ constexpr int tf_ld(int rows) { return ((rows + 8 + 27) / 32) * 32 + 4; }
+// |d|^2 of a rotation class (class = 7 t2i + dk + 3, fmm.hpp:171)
+__host__ __device__ inline int class_dsq(int c)
+{
+    const int t2[10] = {0, 1, 2, 4, 5, 8, 9, 10, 13, 18};
+    const int dk = c % 7 - 3;
+    return t2[c / 7] + dk * dk;
+}
+
+__device__ __forceinline__ unsigned to_tf32(float x)
+{
+    unsigned r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+struct Tf32x2 {
+    unsigned h, l;
+};
+
+__device__ __forceinline__ Tf32x2 split_tf32(float x)
+{
+    const unsigned h = to_tf32(x);
+    return Tf32x2{h, to_tf32(x - __uint_as_float(h))};
+}
+
+struct FragA {
+    unsigned h[4], l[4];
+};
+
+__device__ __forceinline__ FragA split_a(const float4 v)
+{
+    FragA f;
+    const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const Tf32x2 s = split_tf32(e[i]);
+        f.h[i] = s.h;
+        f.l[i] = s.l;
+    }
+    return f;
+}
+
+__device__ __forceinline__ void mma1688(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// d += a b in 3xTF32 (small terms first)
+__device__ __forceinline__ void mma3x(float (&d)[4], const FragA& a, float b0, float b1)
+{
+    const Tf32x2 s0 = split_tf32(b0), s1 = split_tf32(b1);
+    mma1688(d, a.l, s0.h, s1.h);
+    mma1688(d, a.h, s0.l, s1.l);
+    mma1688(d, a.h, s0.h, s1.h);
+}
+
+template<int P>
+struct MixLayout {
+    static constexpr int T = (P + 1) * (P + 2) / 2;
+    static constexpr int T1 = (P + 2) * (P + 3) / 2;
+    static constexpr int LD = tf_ld(T), LD1 = tf_ld(T1);          // column strides (floats)
+    static constexpr int ent_src = 0;
+    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
+    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
+    static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
+    static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
+    static constexpr int cls_off = al16(cls_cnt + 4 * 72);
+    static constexpr int bat_off = al16(cls_off + 4 * 72);
+    static constexpr int meta = al16(bat_off + 4 * 72);
+    static constexpr int tm = al16(meta + int(sizeof(MmaMeta)) * 3);
+    static constexpr int tn = al16(tm + T1);                       // order n of coefficient t
+    static constexpr int spow = al16(tn + T1);                     // s^-k, k = 0..P+2 (doubles)
+    static constexpr int Xraw = al16(spow + 8 * (P + 3));          // 2 x [col][T] complex (cp.async)
+    static constexpr int X = al16(Xraw + 2 * 8 * T * 16);          // re, im: [col][LD] floats each
+    static constexpr int W = al16(X + 2 * 8 * LD * 4);
+    static constexpr int LzA = al16(W + 2 * 8 * LD * 4);
+    static constexpr int LzB = al16(LzA + 2 * 8 * LD * 4);         // [col][LD1]
+    static constexpr int acc = al16(LzB + 2 * 8 * LD1 * 4);        // FP64 complex [8 qd][T] then [8 qd][T1]
+    __host__ __device__ static constexpr int total(int qd) { return al16(acc + 16 * 8 * qd * (T + T1)); }
+};
+
+template<int P>
+__global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int64_t g1)
+{
+    using L = MixLayout<P>;
+    constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 256;
+    extern __shared__ __align__(16) unsigned char sm[];
+    int* ent_src = reinterpret_cast<int*>(sm + L::ent_src);
+    int* ent_code = reinterpret_cast<int*>(sm + L::ent_code);
+    short* sorted = reinterpret_cast<short*>(sm + L::sorted);
+    unsigned char* cls = sm + L::cls;
+    int* cls_cnt = reinterpret_cast<int*>(sm + L::cls_cnt);
+    int* cls_off = reinterpret_cast<int*>(sm + L::cls_off);
+    int* bat_off = reinterpret_cast<int*>(sm + L::bat_off);
+    MmaMeta* meta = reinterpret_cast<MmaMeta*>(sm + L::meta);
+    unsigned char* tm = sm + L::tm;
+    unsigned char* tn = sm + L::tn;
+    double* spow = reinterpret_cast<double*>(sm + L::spow);
+    cplx* Xraw = reinterpret_cast<cplx*>(sm + L::Xraw);
+    float* Xre = reinterpret_cast<float*>(sm + L::X);
+    float* Xim = Xre + 8 * LD;
+    float* Wre = reinterpret_cast<float*>(sm + L::W);
+    float* Wim = Wre + 8 * LD;
+    float* Are = reinterpret_cast<float*>(sm + L::LzA);
+    float* Aim = Are + 8 * LD;
+    float* Bre = reinterpret_cast<float*>(sm + L::LzB);
+    float* Bim = Bre + 8 * LD1;
+    const int qd = a.qdim;
+    cplx* accA = reinterpret_cast<cplx*>(sm + L::acc);
+    cplx* accB = accA + 8 * qd * T;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g8 = lane >> 2, t4 = lane & 3;                      // fragment group / thread in group
+    const int bofs = g8 * LD + t4, bofs1 = g8 * LD1 + t4;          // B element (K row t4, column g8)
+    const int d0 = (2 * t4) * LD, d1 = (2 * t4 + 1) * LD, e0 = (2 * t4) * LD1, e1 = (2 * t4 + 1) * LD1;
+    for (int e = tid; e < (L::acc - L::X) / 4; e += NT) Xre[e] = 0.f;
+    for (int t = tid; t < T1; t += NT) {
+        int n, m;
+        tri_nm(t, n, m);
+        tm[t] = static_cast<unsigned char>(m);
+        tn[t] = static_cast<unsigned char>(n);
+    }
+    __syncthreads();
+    const float4* rf = reinterpret_cast<const float4*>(a.rf32);
+    const float4* tzf = reinterpret_cast<const float4*>(a.tz32);
+    const int NF = a.rf32_nf, NFZ = a.tz32_nf;
+
+    auto make_meta = [&](int b, int k, MmaMeta& M, int& c) {
+        while (bat_off[c + 1] <= b) ++c;
+        const int col0 = (b - bat_off[c]) * 8;
+        const int ncol = min(8, cls_cnt[c] * qd - col0);
+        if (k < ncol) {
+            const int col = col0 + k;
+            const int pair = col / qd;
+            const int e = sorted[cls_off[c] + pair];
+            const int code = ent_code[e];
+            const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
+            const int bq = col - pair * qd;
+            M.src[k] = ent_src[e];
+            M.bq[k] = bq;
+            M.sb[k] = ((code >> 9) & 7) * qd + bq;
+            M.pidx[k] = 7 * (dj + 3) + (di + 3);
+            if (k == 0) {
+                M.cls = c;
+                M.ncol = ncol;
+                M.dsq = di * di + dj * dj + dk * dk;
+            }
+        } else {
+            M.src[k] = 0;
+            M.bq[k] = 0;
+            M.sb[k] = 0;
+            M.pidx[k] = 24;
+        }
+    };
+    auto issue = [&](int b) {
+        const MmaMeta& M = meta[b % 3];
+        const int ncol = M.ncol;
+        cplx* xr = Xraw + (b & 1) * 8 * T;
+        for (int e = tid; e < 8 * T; e += NT) {
+            const int c = e / T, t = e - c * T;
+            if (c < ncol) cp_async16(xr + e, a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
+        }
+        cp_async_commit();
+    };
+    // X~ = s^-n e^{i m phi} M, rounded to FP32, column-major
+    auto phase_in = [&](int b) {
+        const MmaMeta& M = meta[b % 3];
+        const int ncol = M.ncol;
+        const cplx* xr = Xraw + (b & 1) * 8 * T;
+        for (int e = tid; e < 8 * T; e += NT) {
+            const int c = e / T, t = e - c * T;
+            if (c < ncol) {
+                const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
+                const cplx v = cmul(cplx{ph.x, ph.y}, xr[e]);
+                const double sc = spow[tn[t]];
+                Xre[c * LD + t] = static_cast<float>(v.re * sc);
+                Xim[c * LD + t] = static_cast<float>(v.im * sc);
+            }
+        }
+    };
+
+    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+        const int nc = a.nchild[g];
+        if (nc == 0) continue;
+        const int cb = a.child_beg[g];
+        const int lt = level_of(a, g) + 1;
+        {
+            const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
+            for (int s = 0; s < nc; ++s) {
+                const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
+                for (int e = q0 + tid; e < q1; e += NT) {
+                    const int code = a.il_code[e0 + e];
+                    ent_src[e] = a.il_src[e0 + e];
+                    ent_code[e] = code | (s << 9);
+                    cls[e] = static_cast<unsigned char>(
+                        rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
+                }
+            }
+            for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = cplx{0, 0};
+            if (tid == 0) {
+                // s^-k for the box size s of the targets' (= sources') level
+                const double sinv = double(1 << lt) / a.box->width;
+                double v = 1.0;
+                for (int k = 0; k <= P + 2; ++k) {
+                    spow[k] = v;
+                    v *= sinv;
+                }
+            }
+            __syncthreads();
+            for (int cl = tid; cl < kNumClasses; cl += NT) {
+                int cnt = 0;
+                for (int e = 0; e < E; ++e) cnt += cls[e] == cl;
+                cls_cnt[cl] = cnt;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int s = 0, k = 0;
+                for (int c = 0; c < kNumClasses; ++c) {
+                    cls_off[c] = s;
+                    bat_off[c] = k;
+                    s += cls_cnt[c];
+                    k += (cls_cnt[c] * qd + 7) / 8;
+                }
+                cls_off[kNumClasses] = s;
+                bat_off[kNumClasses] = k;
+            }
+            __syncthreads();
+            for (int cl = tid; cl < kNumClasses; cl += NT) {
+                int pos = cls_off[cl];
+                for (int e = 0; e < E; ++e)
+                    if (cls[e] == cl) sorted[pos++] = static_cast<short>(e);
+            }
+            __syncthreads();
+        }
+        const int nbat = bat_off[kNumClasses];
+        int cur = 0;
+        if (tid < 8 && nbat > 0) make_meta(0, tid, meta[0], cur);
+        __syncthreads();
+        if (nbat > 0) issue(0);
+        if (tid < 8 && nbat > 1) make_meta(1, tid, meta[1], cur);
+        cp_async_wait_all();
+        __syncthreads();
+        if (nbat > 0) phase_in(0);
+        if (nbat > 1) issue(1);
+        __syncthreads();
+
+        for (int b = 0; b < nbat; ++b) {
+            const MmaMeta& M = meta[b % 3];
+            const float4* rfc = rf + int64_t(M.cls) * NF * 4 * 32 + lane;
+            const float4* tzc = tzf + int64_t(M.cls) * NFZ * 32 + lane;
+            const float* tlc = a.tzl32 + M.cls * (P + 1) * (P + 2);
+            // ---- rotation
+            static_for<0, P + 1>([&](auto nn) {
+                constexpr int n = P - decltype(nn)::value;
+                constexpr int KC = tf_kc(n), base = n * (n + 1) / 2;
+                static_for<0, tf_rt(n)>([&](auto rr) {
+                    constexpr int rt = decltype(rr)::value;
+                    if ((tf_rjob0(P, n) + rt) % 8 != warp) return;
+                    const float4* fr = rfc + (tf_foff(n) + rt * KC) * 4 * 32;
+                    float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) {
+                        const FragA aP = split_a(__ldg(fr + (kc * 4 + 0) * 32));
+                        const FragA aQ = split_a(__ldg(fr + (kc * 4 + 1) * 32));
+                        const int ro = bofs + base + 8 * kc;
+                        mma3x(r, aP, Xre[ro], Xre[ro + 4]);
+                        mma3x(im, aQ, Xim[ro], Xim[ro + 4]);
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int m = 16 * rt + g8 + 8 * h;
+                        if (m <= n) {
+                            const int u = az_off(P, m) + (n - m);
+                            Wre[d0 + u] = r[2 * h];
+                            Wre[d1 + u] = r[2 * h + 1];
+                            Wim[d0 + u] = im[2 * h];
+                            Wim[d1 + u] = im[2 * h + 1];
+                        }
+                    }
+                });
+            });
+            __syncthreads();
+            // ---- z-translation (class-scaled operator, the same for re and im)
+            static_for<0, P + 2>([&](auto kk) {
+                constexpr int k = decltype(kk)::value;
+                constexpr int KC = tf_zkc(P, k), u0 = az_off(P, k);
+                static_for<0, tf_zrt(P, k)>([&](auto rr) {
+                    constexpr int rt = decltype(rr)::value;
+                    if ((tf_zjob0(P, k) + rt) % 8 != warp) return;
+                    const float4* fz = tzc + (tf_zoff(P, k) + rt * KC) * 32;
+                    float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+#pragma unroll
+                    for (int kc = 0; kc < KC; ++kc) {
+                        const FragA az = split_a(__ldg(fz + kc * 32));
+                        const int ro = bofs + u0 + 8 * kc;
+                        mma3x(r, az, Wre[ro], Wre[ro + 4]);
+                        mma3x(im, az, Wim[ro], Wim[ro + 4]);
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int j = k + 16 * rt + g8 + 8 * h;
+                        if (j <= P + 1) {
+                            const int t1 = j * (j + 1) / 2 + k;
+                            Bre[e0 + t1] = r[2 * h];
+                            Bre[e1 + t1] = r[2 * h + 1];
+                            Bim[e0 + t1] = im[2 * h];
+                            Bim[e1 + t1] = im[2 * h + 1];
+                            if constexpr (k <= P) {
+                                if (j <= P) {
+                                    const float tl = tlc[k * (P + 2) + j];
+                                    constexpr int up = u0 + (P - k);
+                                    Are[d0 + t1] = fmaf(tl, Wre[d0 + up], r[2 * h]);
+                                    Are[d1 + t1] = fmaf(tl, Wre[d1 + up], r[2 * h + 1]);
+                                    Aim[d0 + t1] = fmaf(tl, Wim[d0 + up], im[2 * h]);
+                                    Aim[d1 + t1] = fmaf(tl, Wim[d1 + up], im[2 * h + 1]);
+                                }
+                            }
+                        }
+                    }
+                });
+            });
+            if (tid < 8 && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
+            __syncthreads();
+            // ---- inverse rotation + phase, in place, one warp per order j
+            {
+                const int pc0 = M.pidx[2 * t4] * (P + 2), pc1 = M.pidx[2 * t4 + 1] * (P + 2);
+                static_for<0, P + 2>([&](auto jj) {
+                    constexpr int j = P + 1 - decltype(jj)::value;
+                    if (decltype(jj)::value % 8 != warp) return;
+                    constexpr int KC = tf_kc(j), RT = tf_rt(j), base = j * (j + 1) / 2;
+                    constexpr bool hasA = j <= P;
+                    const float4* fr = rfc + tf_foff(j) * 4 * 32;
+                    float ar[RT][4] = {}, ai[RT][4] = {}, br[RT][4] = {}, bi[RT][4] = {};
+#pragma unroll
+                    for (int rt = 0; rt < RT; ++rt)
+#pragma unroll
+                        for (int kc = 0; kc < KC; ++kc) {
+                            const FragA aPB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 2) * 32));
+                            const FragA aQB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 3) * 32));
+                            const int ro1 = bofs1 + base + 8 * kc;
+                            mma3x(br[rt], aPB, Bre[ro1], Bre[ro1 + 4]);
+                            mma3x(bi[rt], aQB, Bim[ro1], Bim[ro1 + 4]);
+                            if constexpr (hasA) {
+                                const int ro = bofs + base + 8 * kc;
+                                mma3x(ar[rt], aPB, Are[ro], Are[ro + 4]);
+                                mma3x(ai[rt], aQB, Aim[ro], Aim[ro + 4]);
+                            }
+                        }
+                    __syncwarp();
+#pragma unroll
+                    for (int rt = 0; rt < RT; ++rt)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int m = 16 * rt + g8 + 8 * h;
+                            if (m > j) continue;
+                            const int t = base + m;
+                            const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0 + m);
+                            const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1 + m);
+                            const float c0 = static_cast<float>(f0.x), s0 = static_cast<float>(f0.y);
+                            const float c1 = static_cast<float>(f1.x), s1 = static_cast<float>(f1.y);
+                            const float b0r = br[rt][2 * h], b0i = bi[rt][2 * h], b1r = br[rt][2 * h + 1], b1i = bi[rt][2 * h + 1];
+                            Bre[e0 + t] = c0 * b0r + s0 * b0i;
+                            Bim[e0 + t] = c0 * b0i - s0 * b0r;
+                            Bre[e1 + t] = c1 * b1r + s1 * b1i;
+                            Bim[e1 + t] = c1 * b1i - s1 * b1r;
+                            if constexpr (hasA) {
+                                const float a0r = ar[rt][2 * h], a0i = ai[rt][2 * h], a1r = ar[rt][2 * h + 1], a1i = ai[rt][2 * h + 1];
+                                Are[d0 + t] = c0 * a0r + s0 * a0i;
+                                Aim[d0 + t] = c0 * a0i - s0 * a0r;
+                                Are[d1 + t] = c1 * a1r + s1 * a1i;
+                                Aim[d1 + t] = c1 * a1i - s1 * a1r;
+                            }
+                        }
+                });
+            }
+            cp_async_wait_all();
+            __syncthreads();
+            // ---- accumulate (FP64, s^-(j+1) scale) in column order; phase tile b + 1 in
+            {
+                const int ncol = M.ncol;
+                int sb[8];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) sb[c] = M.sb[c];
+                for (int t = tid; t < T + T1; t += NT) {
+                    const bool isA = t < T;
+                    const int r = isA ? t : t - T;
+                    const double sc = spow[tn[r] + 1];
+                    const float* sre = isA ? Are + r : Bre + r;
+                    const float* sim = isA ? Aim + r : Bim + r;
+                    const int ld = isA ? LD : LD1;
+                    cplx* acc = isA ? accA + r : accB + r;
+                    const int stride = isA ? T : T1;
+#pragma unroll
+                    for (int c = 0; c < 8; ++c)
+                        if (c < ncol) {
+                            cplx& d = acc[sb[c] * stride];
+                            d.re += sc * static_cast<double>(sre[c * ld]);
+                            d.im += sc * static_cast<double>(sim[c * ld]);
+                        }
+                }
+                if (b + 1 < nbat) phase_in(b + 1);
+                if (b + 2 < nbat) issue(b + 2);
+            }
+            __syncthreads();
+        }
+        if (a.want_pot)
+            for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = accA[e];
+        if (a.want_field)
+            for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = accB[e];
+        __syncthreads();
+    }
+}
+
+template<int P>
+bool try_launch_tf32(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
+{
+    const size_t smem = MixLayout<P>::total(a.qdim);
+    int dev = 0, optin = 0;
+    SFMM_CUDA(cudaGetDevice(&dev));
+    SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    if (smem > size_t(optin)) return false;
+    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    int per_sm = 0;
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_tf32<P>, 256, smem));
+    if (per_sm < 1) return false;
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
+    k_m2l_tf32<P><<<static_cast<unsigned>(grid), 256, smem, st>>>(a, g0, g1);
+    SFMM_CHECK_LAUNCH();
+    return true;
+}
+
+// FP32 TF32-fragment tables: rotation matrices per class (orders <= P+1) and
+// the class-scaled z-translation and order-p column.
+__global__ void k_frag_rot32(const double* __restrict__ rot, const int* __restrict__ rot_off, int rot_len, int P, int NF,
+                             float4* __restrict__ out)
+{
+    const int64_t total = int64_t(kNumClasses) * NF * 4 * 32;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+        const int lane = static_cast<int>(idx & 31), mat = static_cast<int>((idx >> 5) & 3);
+        const int64_t rest = idx >> 7;
+        const int f = static_cast<int>(rest % NF), c = static_cast<int>(rest / NF);
+        int n = 0;
+        while (n < P + 1 && tf_foff(n + 1) <= f) ++n;
+        const int KC = tf_kc(n);
+        const int rt = (f - tf_foff(n)) / KC, kc = (f - tf_foff(n)) - rt * KC;
+        const int g = lane >> 2, t = lane & 3;
+        float v[4];
+        for (int q = 0; q < 4; ++q) {
+            const int row = 16 * rt + g + 8 * (q & 1), col = 8 * kc + t + 4 * (q >> 1);
+            v[q] = (row <= n && col <= n)
+                       ? static_cast<float>(rot[int64_t(c) * rot_len + rot_off[n] + mat * (n + 1) * (n + 1) + row * (n + 1) + col])
+                       : 0.f;
+        }
+        out[idx] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+}
+
+__global__ void k_frag_tz32(const double* __restrict__ tzx, const int* __restrict__ tzx_off, int P, int NFZ,
+                            float4* __restrict__ out, float* __restrict__ tzl)
+{
+    const int64_t total = int64_t(kNumClasses) * NFZ * 32;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+        const int lane = static_cast<int>(idx & 31);
+        const int f = static_cast<int>((idx >> 5) % NFZ), c = static_cast<int>((idx >> 5) / NFZ);
+        const double rho = sqrt(double(class_dsq(c)));
+        int k = 0;
+        while (k < P + 1 && tf_zoff(P, k + 1) <= f) ++k;
+        const int KC = tf_zkc(P, k);
+        const int rt = (f - tf_zoff(P, k)) / KC, kc = (f - tf_zoff(P, k)) - rt * KC;
+        const int g = lane >> 2, t = lane & 3;
+        float v[4];
+        for (int q = 0; q < 4; ++q) {
+            const int j = k + 16 * rt + g + 8 * (q & 1), np = k + 8 * kc + t + 4 * (q >> 1);
+            v[q] = (j <= P + 1 && np <= P - 1)
+                       ? static_cast<float>(tzx[tzx_off[k] + (j - k) * (P + 1 - k) + (np - k)] * pow(rho, -(j + np + 1)))
+                       : 0.f;
+        }
+        out[idx] = make_float4(v[0], v[1], v[2], v[3]);
+    }
+    const int ntl = kNumClasses * (P + 1) * (P + 2);
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ntl; idx += gridDim.x * blockDim.x) {
+        const int c = idx / ((P + 1) * (P + 2)), r = idx - c * (P + 1) * (P + 2);
+        const int k = r / (P + 2), j = r - k * (P + 2);
+        const double rho = sqrt(double(class_dsq(c)));
+        tzl[idx] = (j >= k && j <= P)
+                       ? static_cast<float>(tzx[tzx_off[k] + (j - k) * (P + 1 - k) + (P - k)] * pow(rho, -(j + P + 1)))
+                       : 0.f;
+    }
+}
+
 template<int P>
 void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     if constexpr (P >= 2) {
+        if (a.mixed && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
         if (try_launch_mma<P>(a, g0, g1, sms, st)) return;
     }
     if constexpr (P >= 2 && P <= 12) {
@@ -1352,6 +1886,19 @@ void build_m2l_fragments(Plan& pl, cudaStream_t st)
     SFMM_CHECK_LAUNCH();
     k_frag_tz<<<16, 256, 0, st>>>(pl.tzx.ptr, pl.tzx_off.ptr, P, tz_foff(P, P + 2), pl.tzfrag.ptr, pl.tzl.ptr);
     SFMM_CHECK_LAUNCH();
+    if (pl.precision == FMM_PRECISION_MIXED) {
+        pl.rf32_nf = tf_foff(P + 2);
+        pl.tz32_nf = std::max(tf_zoff(P, P + 2), 1);
+        pl.rf32.alloc(size_t(kNumClasses) * pl.rf32_nf * 4 * 32 * 4, st);
+        pl.tz32.alloc(size_t(kNumClasses) * pl.tz32_nf * 32 * 4, st);
+        pl.tzl32.alloc(size_t(kNumClasses) * (P + 1) * (P + 2), st);
+        k_frag_rot32<<<256, 256, 0, st>>>(pl.rot.ptr, pl.rot_off.ptr, pl.rot_len, P, pl.rf32_nf,
+                                          reinterpret_cast<float4*>(pl.rf32.ptr));
+        SFMM_CHECK_LAUNCH();
+        k_frag_tz32<<<64, 256, 0, st>>>(pl.tzx.ptr, pl.tzx_off.ptr, P, tf_zoff(P, P + 2),
+                                        reinterpret_cast<float4*>(pl.tz32.ptr), pl.tzl32.ptr);
+        SFMM_CHECK_LAUNCH();
+    }
 }
 
 void launch_m2l(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
