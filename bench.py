@@ -194,6 +194,95 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def serve_bench(args):
+    """Serving stream: seeded requests with Poisson arrivals, N log-uniform in
+    [1e3, 1e6], uniform / Plummer / thin shell with equal probability, p in
+    {6, 10}, charges U[-1,1].  The server (continuous batching under a memory
+    budget, autotuned leaf size, the given precision) against the plain FP64
+    path solving one request at a time in arrival order.  Latency = completion
+    minus arrival."""
+    import threading
+
+    import simplefmm_b200 as sf
+    from simplefmm_b200 import workloads as W
+
+    rng = np.random.default_rng(SEED + 4)
+    k = args.requests
+    ns = np.exp(rng.uniform(np.log(1e3), np.log(1e6), k)).astype(np.int64)
+    dists = rng.choice(["uniform", "plummer", "shell"], k)
+    ps = rng.choice([6, 10], k)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, k))
+    reqs = [(W.points(str(d), int(n), SEED + 1000 + i), W.charges(int(n), SEED + 1000 + i), int(p))
+            for i, (n, d, p) in enumerate(zip(ns, dists, ps))]
+    total_points = int(ns.sum())
+
+    def stream_server(precision):
+        srv = sf.Server(0, slots=args.slots, memory_budget=args.budget_gib << 30)
+        ids = [None] * k
+        t0 = time.perf_counter()
+
+        def feeder():
+            for i, (pos, q, p) in enumerate(reqs):
+                dt = arrivals[i] - (time.perf_counter() - t0)
+                if dt > 0:
+                    time.sleep(dt)
+                ids[i] = srv.submit(pos, q, p, precision=precision)
+
+        th = threading.Thread(target=feeder)
+        th.start()
+        lat = []
+        for i in range(k):
+            while ids[i] is None:
+                time.sleep(0.0005)
+            _, _, l_ms = srv.wait(ids[i])
+            lat.append(l_ms)
+        th.join()
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return np.array(lat), span, st
+
+    def stream_plain():
+        ctx = sf.Context(0)
+        t0 = time.perf_counter()
+        lat = []
+        for i, (pos, q, p) in enumerate(reqs):
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt > 0:
+                time.sleep(dt)
+            t = sf.Tree(pos, 20, LEAF, ctx=ctx)
+            pot, fld = np.zeros(len(q)), np.zeros((len(q), 3))
+            sf.Plan(t, p, 1).evaluate(q, pot, fld)
+            t.close()
+            lat.append((time.perf_counter() - t0 - arrivals[i]) * 1e3)
+        return np.array(lat), time.perf_counter() - t0
+
+    # warm-up: one small solve on each path (tables, modules, pools)
+    for pos, q, p in reqs[:2]:
+        srv = sf.Server(0, slots=1, memory_budget=args.budget_gib << 30)
+        srv.wait(srv.submit(pos, q, p, precision=args.precision))
+        srv.close()
+    lat_s, span_s, st = stream_server(args.precision)
+    lat_p, span_p = stream_plain()
+    pct = lambda a, q: float(np.percentile(a, q))  # noqa: E731
+    line = {
+        "metric": "solves/s on a served mixed-size stream (p50/p99 latency beside)", "value": k / span_s,
+        "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
+        "data": "synthetic (seeded; Poisson arrivals; N log-uniform [1e3, 1e6]; uniform / Plummer / shell; p in {6, 10})",
+        "config": {"workload": f"serving_stream_{k}_requests_rate{args.rate:g}", "requests": k, "rate_per_s": args.rate,
+                   "points_total": total_points, "slots": args.slots, "budget_gib": args.budget_gib,
+                   "precision": args.precision, "leaf": "autotuned {32, 64, 128}"},
+        "latency_ms": {"p50": pct(lat_s, 50), "p99": pct(lat_s, 99), "mean": float(lat_s.mean())},
+        "points_per_s": total_points / span_s,
+        "server": st,
+        "plain_one_at_a_time": {"solves_per_s": k / span_p, "points_per_s": total_points / span_p,
+                                "p50_ms": pct(lat_p, 50), "p99_ms": pct(lat_p, 99), "precision": "fp64",
+                                "leaf": LEAF},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -207,9 +296,17 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--serve", action="store_true", help="serving-stream benchmark instead of the solve benchmark")
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--rate", type=float, default=100.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--budget-gib", type=int, default=32)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.serve:
+        serve_bench(args)
         return
 
     import torch

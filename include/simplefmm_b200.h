@@ -153,6 +153,30 @@ int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, 
 int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
                        int64_t nt, double* pot, double* field, void* stream);
 
+/* ---- Serving loop (no counterpart in the reference: its API solves one
+   problem per call).  Solves of different N, p and precision are submitted
+   as they arrive and run concurrently on one device: `slots` workers, each
+   with its own stream, admit queued requests in arrival order as a slot and
+   `memory_budget` bytes of (estimated) device memory become free, so the
+   kernels of admitted requests overlap.  A request keeps its host pointers
+   (xyz, Q, pot, field) until fmm_server_wait returns; pot / field are
+   accumulated as by fmm_evaluate.  max_particles_per_node = 0 lets the
+   server's autotuner pick the leaf size per (p, precision, log2 N). */
+typedef struct fmm_server fmm_server;
+int fmm_server_create(int device, int slots, size_t memory_budget, fmm_server** out);
+/* Finishes every queued request, then frees the server. */
+int fmm_server_destroy(fmm_server* server);
+int fmm_server_submit(fmm_server* server, const double* xyz, int64_t n, const double* Q, int qdim, int p,
+                      int precision, int max_particles_per_node, double* pot, double* field, int64_t* id);
+int fmm_server_poll(fmm_server* server, int64_t id, int* done);
+/* Blocks until request `id` is done; returns its status and its latency
+   (submission to completion, ms).  The id is released. */
+int fmm_server_wait(fmm_server* server, int64_t id, double* latency_ms);
+/* [0] completed requests, [1] p50 latency ms, [2] p99 latency ms, [3] mean
+   latency ms, [4] most requests running at once, [5] most budgeted bytes in
+   use at once, [6] budget bytes, [7] requests queued now. */
+int fmm_server_stats(fmm_server* server, double* stats8);
+
 /* Number of kernels this library has launched in this process. */
 int fmm_launch_count(int64_t* count);
 

@@ -19,7 +19,7 @@ from pathlib import Path
 import numpy as np
 
 __all__ = ["FMMError", "Context", "Tree", "Plan", "Box", "OctreePartitioner", "OctreeLevel", "FMM3D",
-           "direct", "launch_count", "load_library", "LIB_PATH"]
+           "direct", "launch_count", "load_library", "LIB_PATH", "Server"]
 
 LIB_PATH = Path(__file__).resolve().parent / "libsimplefmm_b200.so"
 
@@ -73,6 +73,12 @@ def load_library():
         "fmm_direct": ([vp, vp, i64, vp, i32, vp, i64, vp, vp, i32], i32),
         "fmm_direct_noalloc": ([vp, i64, vp, i32, vp, i64, vp, vp, vp], i32),
         "fmm_launch_count": ([C.POINTER(i64)], i32),
+        "fmm_server_create": ([i32, i32, C.c_size_t, C.POINTER(vp)], i32),
+        "fmm_server_destroy": ([vp], i32),
+        "fmm_server_submit": ([vp, vp, i64, vp, i32, i32, i32, i32, vp, vp, C.POINTER(i64)], i32),
+        "fmm_server_poll": ([vp, i64, C.POINTER(i32)], i32),
+        "fmm_server_wait": ([vp, i64, C.POINTER(dbl)], i32),
+        "fmm_server_stats": ([vp, C.POINTER(dbl)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -296,6 +302,63 @@ def direct(positions, Q, targets, pot=True, field=True, ctx: Context | None = No
     if po is not None and qdim == 1:
         po = po[:, 0]
     return po, fo
+
+
+class Server:
+    """Serving loop (fmm_server_*): submit solves as they arrive; they run
+    concurrently on one device under a device-memory budget.  Arrays passed to
+    submit() are kept alive until wait()."""
+
+    def __init__(self, device: int = 0, slots: int = 4, memory_budget: int = 16 << 30):
+        h = C.c_void_p()
+        _check(load_library().fmm_server_create(device, slots, memory_budget, C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, positions, Q, p: int, precision: str = "fp64", leaf: int = 0, pot=True, field=True):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        n = pos.shape[0]
+        qdim = 1 if Q.ndim == 1 else Q.shape[1]
+        po = np.zeros((n,) if qdim == 1 else (n, qdim)) if pot else None
+        fo = np.zeros((n, 3)) if field else None
+        rid = C.c_int64()
+        _check(load_library().fmm_server_submit(
+            self._h, C.c_void_p(pos.ctypes.data), n, C.c_void_p(Q.ctypes.data), qdim, p, PRECISION[precision], leaf,
+            C.c_void_p(po.ctypes.data) if pot else None, C.c_void_p(fo.ctypes.data) if field else None, C.byref(rid)))
+        self._keep[rid.value] = (pos, Q, po, fo)
+        return rid.value
+
+    def done(self, rid: int) -> bool:
+        d = C.c_int()
+        _check(load_library().fmm_server_poll(self._h, rid, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, rid: int):
+        """(pot, field, latency_ms) of request rid."""
+        lat = C.c_double()
+        try:
+            _check(load_library().fmm_server_wait(self._h, rid, C.byref(lat)))
+        finally:
+            keep = self._keep.pop(rid, None)
+        return keep[2], keep[3], lat.value
+
+    def stats(self) -> dict:
+        s = (C.c_double * 8)()
+        _check(load_library().fmm_server_stats(self._h, s))
+        return dict(completed=int(s[0]), p50_ms=s[1], p99_ms=s[2], mean_ms=s[3], peak_running=int(s[4]),
+                    peak_bytes=int(s[5]), budget_bytes=int(s[6]), queued=int(s[7]))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().fmm_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def launch_count() -> int:

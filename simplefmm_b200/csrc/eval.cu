@@ -252,7 +252,8 @@ int warps_for(size_t head, size_t per_warp, int maxw = 4)
 template<typename KernelT>
 void allow_smem(KernelT k, size_t smem)
 {
-    SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    SFMM_REQUIRE(smem <= g_smem_optin, FMM_ERR_UNSUPPORTED, "kernel working set exceeds shared memory");
+    allow_max_smem(k);
 }
 
 }  // namespace

@@ -44,6 +44,20 @@ int record_failure(int status, const char* msg);
         if (!(cond)) throw ::sfmm::Error((status), (msg)); \
     } while (0)
 
+// Lets kernel k use up to the device's opt-in shared memory per block.  The
+// attribute belongs to the function, not the launch, so it is always set to
+// the same maximum: host threads launching k concurrently with different
+// shared-memory sizes (a server running several solves) cannot undo each
+// other's setting between the attribute call and the launch.
+template<typename KernelT>
+inline void allow_max_smem(KernelT k)
+{
+    int dev = 0, optin = 0;
+    SFMM_CUDA(cudaGetDevice(&dev));
+    SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+}
+
 // ------------------------------------------------------------------ device memory
 // Stream-ordered device allocation from a memory pool owned by this library
 // (one per device, created on first use, kept until exit, release threshold

@@ -341,7 +341,7 @@ void launch_rows_fallback(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cu
 {
     constexpr int T = RowCfg<P>::T, T1 = RowCfg<P>::T1, NT = RowCfg<P>::NT;
     const size_t smem = m2l_smem(T, T1, a.qdim).total;
-    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_rows<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_max_smem(k_m2l_rows<P>);
     int per_sm = 1;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_rows<P>, NT, smem));
     SFMM_REQUIRE(per_sm > 0, FMM_ERR_UNSUPPORTED, "M2L working set exceeds the device");
@@ -825,7 +825,7 @@ bool try_launch_roles(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaSt
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_roles<P, CB, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_max_smem(k_m2l_roles<P, CB, MINB>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_roles<P, CB, MINB>, C::NT, smem));
     if (per_sm < 1) return false;
@@ -1266,7 +1266,7 @@ bool try_launch_mma(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStre
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_mma<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_max_smem(k_m2l_mma<P>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P>, 256, smem));
     if (per_sm < 1) return false;
@@ -1783,7 +1783,7 @@ bool try_launch_tf32(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStr
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    SFMM_CUDA(cudaFuncSetAttribute(k_m2l_tf32<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+    allow_max_smem(k_m2l_tf32<P>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_tf32<P>, 256, smem));
     if (per_sm < 1) return false;

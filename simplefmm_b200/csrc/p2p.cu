@@ -320,8 +320,7 @@ template<int QD, bool POT, bool FLD, int MP, int MINB>
 void launch_mixed(const EvalArgs& a, int sms, cudaStream_t st)
 {
     const size_t smem = P2PSmemF<QD>::total;
-    SFMM_CUDA(cudaFuncSetAttribute(k_p2p_mixed<QD, POT, FLD, MP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(smem)));
+    allow_max_smem(k_p2p_mixed<QD, POT, FLD, MP, MINB>);
     const int64_t grid = std::min<int64_t>((a.n_leaves + kWarps - 1) / kWarps, int64_t(sms) * 16);
     k_p2p_mixed<QD, POT, FLD, MP, MINB><<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kWarps * 32, smem, st>>>(a);
     SFMM_CHECK_LAUNCH();
@@ -331,8 +330,7 @@ template<int QD, bool POT, bool FLD, int MP, int MINB>
 void launch_fp64(const EvalArgs& a, int sms, cudaStream_t st)
 {
     const size_t smem = P2PSmem<QD>::total;
-    SFMM_CUDA(cudaFuncSetAttribute(k_p2p<QD, POT, FLD, MP, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   static_cast<int>(smem)));
+    allow_max_smem(k_p2p<QD, POT, FLD, MP, MINB>);
     const int64_t grid = std::min<int64_t>((a.n_leaves + kWarps - 1) / kWarps, int64_t(sms) * 16);
     k_p2p<QD, POT, FLD, MP, MINB><<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kWarps * 32, smem, st>>>(a);
     SFMM_CHECK_LAUNCH();

@@ -1,0 +1,93 @@
+"""Serving loop (fmm_server_*): results are the same alone and in the mix,
+admission respects the device-memory budget, oversize requests are rejected,
+latency statistics are reported."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import simplefmm_b200 as sf
+from conftest import rel_l2
+from simplefmm_b200 import workloads as W
+
+TOL = 1e-12
+
+
+def test_server_argument_checks_need_no_device():
+    L = sf.load_library()
+    h = C.c_void_p()
+    assert L.fmm_server_create(0, 0, 1 << 30, C.byref(h)) == 1          # slots must be >= 1
+    assert L.fmm_server_create(0, 2, 0, C.byref(h)) == 1                # budget must be > 0
+    rid = C.c_int64()
+    assert L.fmm_server_submit(None, None, 10, None, 1, 4, 0, 0, None, None, C.byref(rid)) == 1
+    assert L.fmm_server_destroy(None) == 0
+
+
+def _requests(seed, count, nmax):
+    rng = np.random.default_rng(seed)
+    reqs = []
+    for i in range(count):
+        n = int(np.exp(rng.uniform(np.log(1000), np.log(nmax))))
+        dist = ["uniform", "plummer", "shell"][i % 3]
+        p = [6, 10][(i // 3) % 2]
+        reqs.append((W.points(dist, n, seed + i), W.charges(n, seed + i), p))
+    return reqs
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_same_alone_and_in_the_mix(precision):
+    reqs = _requests(100, 12, 60_000)
+    ctx = sf.Context(0)
+    alone = []
+    for pos, q, p in reqs:
+        t = sf.Tree(pos, 20, 64, ctx=ctx)
+        pot, fld = np.zeros(len(q)), np.zeros((len(q), 3))
+        sf.Plan(t, p, 1, precision=precision).evaluate(q, pot, fld)
+        alone.append((pot, fld))
+    srv = sf.Server(0, slots=4, memory_budget=8 << 30)
+    ids = [srv.submit(pos, q, p, precision=precision, leaf=64) for pos, q, p in reqs]
+    for rid, (pot_a, fld_a) in zip(ids, alone):
+        pot, fld, lat = srv.wait(rid)
+        assert lat > 0
+        np.testing.assert_allclose(pot, pot_a, rtol=0, atol=TOL * np.abs(pot_a).max())
+        np.testing.assert_allclose(fld, fld_a, rtol=0, atol=TOL * np.abs(fld_a).max())
+    st = srv.stats()
+    assert st["completed"] == len(reqs)
+    assert st["peak_running"] >= 2                # work of several requests overlapped
+    assert 0 < st["p50_ms"] <= st["p99_ms"]
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_admission_respects_the_memory_budget():
+    reqs = _requests(200, 10, 200_000)
+    budget = 3 << 29                             # 1.5 GiB: a few of these requests at a time
+    srv = sf.Server(0, slots=8, memory_budget=budget)
+    ids = [srv.submit(pos, q, p, leaf=64) for pos, q, p in reqs]
+    for rid, (pos, q, p) in zip(ids, reqs):
+        pot, fld, _ = srv.wait(rid)
+        assert np.isfinite(pot).all() and np.isfinite(fld).all()
+    st = srv.stats()
+    assert st["peak_bytes"] <= budget
+    assert st["completed"] == len(reqs)
+    srv.close()
+
+
+@pytest.mark.gpu
+def test_oversize_request_is_rejected_and_autotuned_requests_are_correct():
+    srv = sf.Server(0, slots=2, memory_budget=256 << 20)
+    big = W.points("uniform", 2_000_000, 5)
+    with pytest.raises(sf.FMMError) as e:
+        srv.submit(big, W.charges(2_000_000, 5), 10)
+    assert e.value.status == 6                    # FMM_ERR_OVER_BUDGET
+    pos = W.points("plummer", 20_000, 6)
+    q = W.charges(20_000, 6)
+    ids = [srv.submit(pos, q, 8) for _ in range(4)]          # leaf size from the autotuner
+    tg = np.arange(0, 20_000, 97)
+    dpot, dfld = sf.direct(pos, q, tg)
+    for rid in ids:
+        pot, fld, _ = srv.wait(rid)
+        assert rel_l2(pot[tg], dpot) < 1e-4
+        assert rel_l2(fld[tg], dfld) < 1e-3
+    srv.close()
