@@ -1433,7 +1433,8 @@ struct MixLayout {
     static constexpr int meta = al16(bat_off + 4 * 72);
     static constexpr int tm = al16(meta + int(sizeof(MmaMeta)) * 3);
     static constexpr int tn = al16(tm + T1);                       // order n of coefficient t
-    static constexpr int spow = al16(tn + T1);                     // s^-k, k = 0..P+2 (doubles)
+    static constexpr int offs = al16(tn + T1);                     // fragment offsets: foff[P+3], zoff[P+3]
+    static constexpr int spow = al16(offs + 8 * (P + 3));          // s^-k, k = 0..P+2 (doubles)
     static constexpr int Xraw = al16(spow + 8 * (P + 3));          // 2 x [col][T] complex (cp.async)
     static constexpr int X = al16(Xraw + 2 * 8 * T * 16);          // re, im: [col][LD] floats each
     static constexpr int W = al16(X + 2 * 8 * LD * 4);
@@ -1459,6 +1460,8 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
     MmaMeta* meta = reinterpret_cast<MmaMeta*>(sm + L::meta);
     unsigned char* tm = sm + L::tm;
     unsigned char* tn = sm + L::tn;
+    int* foff = reinterpret_cast<int*>(sm + L::offs);
+    int* zoff = foff + (P + 3);
     double* spow = reinterpret_cast<double*>(sm + L::spow);
     cplx* Xraw = reinterpret_cast<cplx*>(sm + L::Xraw);
     float* Xre = reinterpret_cast<float*>(sm + L::X);
@@ -1483,6 +1486,10 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
         tri_nm(t, n, m);
         tm[t] = static_cast<unsigned char>(m);
         tn[t] = static_cast<unsigned char>(n);
+    }
+    for (int k = tid; k < P + 3; k += NT) {
+        foff[k] = tf_foff(k);
+        zoff[k] = tf_zoff(P, k);
     }
     __syncthreads();
     const float4* rf = reinterpret_cast<const float4*>(a.rf32);
@@ -1613,66 +1620,71 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
             const float4* rfc = rf + int64_t(M.cls) * NF * 4 * 32 + lane;
             const float4* tzc = tzf + int64_t(M.cls) * NFZ * 32 + lane;
             const float* tlc = a.tzl32 + M.cls * (P + 1) * (P + 2);
-            // ---- rotation
-            static_for<0, P + 1>([&](auto nn) {
-                constexpr int n = P - decltype(nn)::value;
-                constexpr int KC = tf_kc(n), base = n * (n + 1) / 2;
-                static_for<0, tf_rt(n)>([&](auto rr) {
-                    constexpr int rt = decltype(rr)::value;
-                    if ((tf_rjob0(P, n) + rt) % 8 != warp) return;
-                    const float4* fr = rfc + (tf_foff(n) + rt * KC) * 4 * 32;
-                    float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+            // ---- rotation: jobs (n, rt), largest orders first, round robin over
+            // warps; one copy of the job body (runtime n) keeps the code small
+            {
+                int job = 0;
+#pragma unroll 1
+                for (int n = P; n >= 0; --n) {
+                    const int KC = tf_kc(n), RT = tf_rt(n), base = n * (n + 1) / 2;
+#pragma unroll 1
+                    for (int rt = 0; rt < RT; ++rt, ++job) {
+                        if ((job & 7) != warp) continue;
+                        const float4* fr = rfc + (foff[n] + rt * KC) * 4 * 32;
+                        float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+#pragma unroll 1
+                        for (int kc = 0; kc < KC; ++kc) {
+                            const FragA aP = split_a(__ldg(fr + (kc * 4 + 0) * 32));
+                            const FragA aQ = split_a(__ldg(fr + (kc * 4 + 1) * 32));
+                            const int ro = bofs + base + 8 * kc;
+                            mma3x(r, aP, Xre[ro], Xre[ro + 4]);
+                            mma3x(im, aQ, Xim[ro], Xim[ro + 4]);
+                        }
 #pragma unroll
-                    for (int kc = 0; kc < KC; ++kc) {
-                        const FragA aP = split_a(__ldg(fr + (kc * 4 + 0) * 32));
-                        const FragA aQ = split_a(__ldg(fr + (kc * 4 + 1) * 32));
-                        const int ro = bofs + base + 8 * kc;
-                        mma3x(r, aP, Xre[ro], Xre[ro + 4]);
-                        mma3x(im, aQ, Xim[ro], Xim[ro + 4]);
-                    }
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int m = 16 * rt + g8 + 8 * h;
-                        if (m <= n) {
-                            const int u = az_off(P, m) + (n - m);
-                            Wre[d0 + u] = r[2 * h];
-                            Wre[d1 + u] = r[2 * h + 1];
-                            Wim[d0 + u] = im[2 * h];
-                            Wim[d1 + u] = im[2 * h + 1];
+                        for (int h = 0; h < 2; ++h) {
+                            const int m = 16 * rt + g8 + 8 * h;
+                            if (m <= n) {
+                                const int u = az_off(P, m) + (n - m);
+                                Wre[d0 + u] = r[2 * h];
+                                Wre[d1 + u] = r[2 * h + 1];
+                                Wim[d0 + u] = im[2 * h];
+                                Wim[d1 + u] = im[2 * h + 1];
+                            }
                         }
                     }
-                });
-            });
+                }
+            }
             __syncthreads();
             // ---- z-translation (class-scaled operator, the same for re and im)
-            static_for<0, P + 2>([&](auto kk) {
-                constexpr int k = decltype(kk)::value;
-                constexpr int KC = tf_zkc(P, k), u0 = az_off(P, k);
-                static_for<0, tf_zrt(P, k)>([&](auto rr) {
-                    constexpr int rt = decltype(rr)::value;
-                    if ((tf_zjob0(P, k) + rt) % 8 != warp) return;
-                    const float4* fz = tzc + (tf_zoff(P, k) + rt * KC) * 32;
-                    float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+            {
+                int job = 0;
+#pragma unroll 1
+                for (int k = 0; k <= P + 1; ++k) {
+                    const int KC = tf_zkc(P, k), RT = tf_zrt(P, k), u0 = az_off(P, k);
+#pragma unroll 1
+                    for (int rt = 0; rt < RT; ++rt, ++job) {
+                        if ((job & 7) != warp) continue;
+                        const float4* fz = tzc + (zoff[k] + rt * KC) * 32;
+                        float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
+#pragma unroll 1
+                        for (int kc = 0; kc < KC; ++kc) {
+                            const FragA az = split_a(__ldg(fz + kc * 32));
+                            const int ro = bofs + u0 + 8 * kc;
+                            mma3x(r, az, Wre[ro], Wre[ro + 4]);
+                            mma3x(im, az, Wim[ro], Wim[ro + 4]);
+                        }
 #pragma unroll
-                    for (int kc = 0; kc < KC; ++kc) {
-                        const FragA az = split_a(__ldg(fz + kc * 32));
-                        const int ro = bofs + u0 + 8 * kc;
-                        mma3x(r, az, Wre[ro], Wre[ro + 4]);
-                        mma3x(im, az, Wim[ro], Wim[ro + 4]);
-                    }
-#pragma unroll
-                    for (int h = 0; h < 2; ++h) {
-                        const int j = k + 16 * rt + g8 + 8 * h;
-                        if (j <= P + 1) {
-                            const int t1 = j * (j + 1) / 2 + k;
-                            Bre[e0 + t1] = r[2 * h];
-                            Bre[e1 + t1] = r[2 * h + 1];
-                            Bim[e0 + t1] = im[2 * h];
-                            Bim[e1 + t1] = im[2 * h + 1];
-                            if constexpr (k <= P) {
+                        for (int h = 0; h < 2; ++h) {
+                            const int j = k + 16 * rt + g8 + 8 * h;
+                            if (j <= P + 1) {
+                                const int t1 = j * (j + 1) / 2 + k;
+                                Bre[e0 + t1] = r[2 * h];
+                                Bre[e1 + t1] = r[2 * h + 1];
+                                Bim[e0 + t1] = im[2 * h];
+                                Bim[e1 + t1] = im[2 * h + 1];
                                 if (j <= P) {
                                     const float tl = tlc[k * (P + 2) + j];
-                                    constexpr int up = u0 + (P - k);
+                                    const int up = u0 + (P - k);          // n' = p
                                     Are[d0 + t1] = fmaf(tl, Wre[d0 + up], r[2 * h]);
                                     Are[d1 + t1] = fmaf(tl, Wre[d1 + up], r[2 * h + 1]);
                                     Aim[d0 + t1] = fmaf(tl, Wim[d0 + up], im[2 * h]);
@@ -1681,42 +1693,44 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
                             }
                         }
                     }
-                });
-            });
+                }
+            }
             if (tid < 8 && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
             __syncthreads();
             // ---- inverse rotation + phase, in place, one warp per order j
             {
                 const int pc0 = M.pidx[2 * t4] * (P + 2), pc1 = M.pidx[2 * t4 + 1] * (P + 2);
-                static_for<0, P + 2>([&](auto jj) {
-                    constexpr int j = P + 1 - decltype(jj)::value;
-                    if (decltype(jj)::value % 8 != warp) return;
-                    constexpr int KC = tf_kc(j), RT = tf_rt(j), base = j * (j + 1) / 2;
-                    constexpr bool hasA = j <= P;
-                    const float4* fr = rfc + tf_foff(j) * 4 * 32;
-                    float ar[RT][4] = {}, ai[RT][4] = {}, br[RT][4] = {}, bi[RT][4] = {};
+                constexpr int RTM = tf_rt(P + 1);
+#pragma unroll 1
+                for (int j = P + 1 - warp; j >= 0; j -= 8) {
+                    const int KC = tf_kc(j), RT = tf_rt(j), base = j * (j + 1) / 2;
+                    const bool hasA = j <= P;
+                    const float4* fr = rfc + foff[j] * 4 * 32;
+                    float ar[RTM][4] = {}, ai[RTM][4] = {}, br[RTM][4] = {}, bi[RTM][4] = {};
 #pragma unroll
-                    for (int rt = 0; rt < RT; ++rt)
-#pragma unroll
+                    for (int rt = 0; rt < RTM; ++rt) {
+                        if (rt >= RT) break;
+#pragma unroll 1
                         for (int kc = 0; kc < KC; ++kc) {
                             const FragA aPB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 2) * 32));
                             const FragA aQB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 3) * 32));
                             const int ro1 = bofs1 + base + 8 * kc;
                             mma3x(br[rt], aPB, Bre[ro1], Bre[ro1 + 4]);
                             mma3x(bi[rt], aQB, Bim[ro1], Bim[ro1 + 4]);
-                            if constexpr (hasA) {
+                            if (hasA) {
                                 const int ro = bofs + base + 8 * kc;
                                 mma3x(ar[rt], aPB, Are[ro], Are[ro + 4]);
                                 mma3x(ai[rt], aQB, Aim[ro], Aim[ro + 4]);
                             }
                         }
+                    }
                     __syncwarp();
 #pragma unroll
-                    for (int rt = 0; rt < RT; ++rt)
+                    for (int rt = 0; rt < RTM; ++rt)
 #pragma unroll
                         for (int h = 0; h < 2; ++h) {
                             const int m = 16 * rt + g8 + 8 * h;
-                            if (m > j) continue;
+                            if (rt >= RT || m > j) continue;
                             const int t = base + m;
                             const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0 + m);
                             const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1 + m);
@@ -1727,7 +1741,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
                             Bim[e0 + t] = c0 * b0i - s0 * b0r;
                             Bre[e1 + t] = c1 * b1r + s1 * b1i;
                             Bim[e1 + t] = c1 * b1i - s1 * b1r;
-                            if constexpr (hasA) {
+                            if (hasA) {
                                 const float a0r = ar[rt][2 * h], a0i = ai[rt][2 * h], a1r = ar[rt][2 * h + 1], a1i = ai[rt][2 * h + 1];
                                 Are[d0 + t] = c0 * a0r + s0 * a0i;
                                 Aim[d0 + t] = c0 * a0i - s0 * a0r;
@@ -1735,7 +1749,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
                                 Aim[d1 + t] = c1 * a1i - s1 * a1r;
                             }
                         }
-                });
+                }
             }
             cp_async_wait_all();
             __syncthreads();
