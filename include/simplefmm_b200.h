@@ -97,6 +97,14 @@ int fmm_host_unregister(void* ptr);
    The tree copies the positions it needs; the caller's array may be freed. */
 int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level,
                    int max_particles_per_node, int vertical_axis, double phideg, fmm_tree** out);
+/* Box(corner, width, vertical_axis, phideg) + refine: box.hpp:73-82 -- the
+   caller's root cube (corner in the rotated frame of the keys, as the
+   reference stores it) instead of the one fitted to the points.  Points
+   outside the cube are clamped into its boundary cells, as the reference's
+   keys are (box.hpp:58-63). */
+int fmm_tree_build_box(fmm_context* ctx, const double* xyz, int64_t n, int where, const double* corner3,
+                       double width, int max_level, int max_particles_per_node, int vertical_axis, double phideg,
+                       fmm_tree** out);
 int fmm_tree_destroy(fmm_tree* tree);
 /* Deepest level (OctreePartitioner::level(), partition.hpp:463-466). */
 int fmm_tree_depth(const fmm_tree* tree, int* depth);
@@ -115,6 +123,15 @@ int fmm_tree_stats(const fmm_tree* tree, int64_t* stats5);
    allocates device expansions.  qdim is the number of charge components N. */
 int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** out);
 int fmm_plan_destroy(fmm_plan* plan);
+/* Excluded interactions: FMM3D(partitioner, comm, self_generator) and
+   rinv(Q, U, is_self), fmm.hpp:204, 398-408, 773-807.  row_ptr (n + 1
+   int64) and cols (row_ptr[n] int32, original indices) list for each target
+   i the sources j whose interaction is removed from every later evaluation
+   (j == i is always excluded).  near_too = 0 removes only the listed sources
+   outside i's near field -- the reference's slist with the default is_self
+   (rinv(Q, U)); near_too = 1 removes all of them -- rinv(Q, U, is_self) with
+   an is_self true exactly on the listed pairs.  row_ptr = NULL clears. */
+int fmm_plan_set_exclusions(fmm_plan* plan, const int64_t* row_ptr, const int32_t* cols, int where, int near_too);
 
 /* fmm.rinv(Q, U) (gradient = 0) or fmm.rinv<true>(Q, U) (gradient = 1,
    qdim must be 3): fmm.hpp:864-881.  U (n x qdim, or n x 3) is accumulated. */

@@ -22,6 +22,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "simplefmm_b200.h"
@@ -65,9 +66,18 @@ public:
 
     Box(const std::vector<Coord_t>& positions, int vertical_axis = dim - 1, T phideg = 0)
         : positions_(&positions), vertical_axis_(vertical_axis), phideg_(phideg) {}
+    // box.hpp:73-82: the cube given explicitly (corner in the rotated frame)
+    Box(const Coord_t& corner, T width, int vertical_axis = dim - 1, T phideg = 0)
+        : positions_(nullptr), vertical_axis_(vertical_axis), phideg_(phideg), explicit_(true), width0_(width)
+    {
+        for (int a = 0; a < dim; ++a) corner0_[a] = corner[a];
+    }
 
     int vertical_axis() const noexcept { return vertical_axis_; }
     T phideg() const noexcept { return phideg_; }
+    bool is_explicit() const noexcept { return explicit_; }
+    const double* explicit_corner() const noexcept { return corner0_; }
+    double explicit_width() const noexcept { return width0_; }
     // box.hpp:109-117; available once a partitioner has refined the tree
     T width() const { need(); double w, c[3]; check(fmm_tree_box(tree_, &w, c)); return w; }
     Coord_t corner() const
@@ -86,6 +96,8 @@ private:
     const std::vector<Coord_t>* positions_;
     int vertical_axis_;
     T phideg_;
+    bool explicit_ = false;
+    double corner0_[3] = {0, 0, 0}, width0_ = 0;
     mutable const fmm_tree* tree_ = nullptr;
 };
 
@@ -100,9 +112,15 @@ public:
     void refine(int max_level = 20, int max_particles_per_node = 64)
     {
         fmm_tree* t = nullptr;
-        check(fmm_tree_build(default_context(), reinterpret_cast<const double*>(positions_.data()),
-                             static_cast<int64_t>(positions_.size()), FMM_HOST, max_level, max_particles_per_node,
-                             box_.vertical_axis(), static_cast<double>(box_.phideg()), &t));
+        const double* xyz = reinterpret_cast<const double*>(positions_.data());
+        const int64_t n = static_cast<int64_t>(positions_.size());
+        if (box_.is_explicit())
+            check(fmm_tree_build_box(default_context(), xyz, n, FMM_HOST, box_.explicit_corner(), box_.explicit_width(),
+                                     max_level, max_particles_per_node, box_.vertical_axis(),
+                                     static_cast<double>(box_.phideg()), &t));
+        else
+            check(fmm_tree_build(default_context(), xyz, n, FMM_HOST, max_level, max_particles_per_node,
+                                 box_.vertical_axis(), static_cast<double>(box_.phideg()), &t));
         tree_.reset(t);
         box_.attach(t);
     }
@@ -155,12 +173,49 @@ public:
         plan_.reset(pl);
     }
 
+    // fmm.hpp:204, 398-408: self_generator(i) names the sources whose
+    // interaction with target i is removed.  rinv(Q, U) removes those outside
+    // i's near field (the reference's slist); rinv(Q, U, is_self) removes all
+    // of them, and is_self must be true on every generated pair (other
+    // is_self predicates are not supported: they are checked and rejected).
+    template<typename Comm, typename Generator,
+             typename = decltype(std::declval<Generator>()(0).size())>
+    FMM3D(const Partitioner_t& partitioner, Comm comm, const Generator& self_generator,
+          int precision = FMM_PRECISION_FP64)
+        : FMM3D(partitioner, comm, precision)
+    {
+        ex_ptr_.assign(1, 0);
+        for (int64_t i = 0; i < n_; ++i) {
+            for (int j : self_generator(static_cast<int>(i))) ex_col_.push_back(j);
+            ex_ptr_.push_back(static_cast<int64_t>(ex_col_.size()));
+        }
+        set_exclusions(0);
+    }
+
     // fmm.hpp:864-881: U += sum_j Q_j / |x_i - x_j|  or (gradient) sum_j Q_j x R / |R|^3
     template<bool gradient = false>
     void rinv(const Container<T, N>* Q, Container<T, N>* U) const
     {
         static_assert(support_gradient || !gradient, "rinv<true> needs support_gradient (fmm.hpp:867)");
         static_assert(!gradient || N == 3, "rinv<true> needs N == 3 (fmm.hpp:550)");
+        if (!ex_ptr_.empty()) set_exclusions(0);
+        check(fmm_rinv(plan_.get(), reinterpret_cast<const double*>(Q), reinterpret_cast<double*>(U), gradient ? 1 : 0,
+                       FMM_HOST));
+    }
+
+    // fmm.hpp:864-873 with a custom is_self (see the self_generator constructor)
+    template<bool gradient = false, typename IsSelf>
+    void rinv(const Container<T, N>* Q, Container<T, N>* U, const IsSelf& is_self) const
+    {
+        static_assert(support_gradient || !gradient, "rinv<true> needs support_gradient (fmm.hpp:867)");
+        for (int64_t i = 0; i < n_; ++i) {
+            if (!is_self(static_cast<int>(i), static_cast<int>(i)))
+                throw Error(FMM_ERR_UNSUPPORTED, "is_self(i, i) must be true");
+            for (int64_t e = ex_ptr_.empty() ? 0 : ex_ptr_[i]; e < (ex_ptr_.empty() ? 0 : ex_ptr_[i + 1]); ++e)
+                if (!is_self(static_cast<int>(i), ex_col_[e]))
+                    throw Error(FMM_ERR_UNSUPPORTED, "is_self must be true on every self_generator pair");
+        }
+        if (!ex_ptr_.empty()) set_exclusions(1);
         check(fmm_rinv(plan_.get(), reinterpret_cast<const double*>(Q), reinterpret_cast<double*>(U), gradient ? 1 : 0,
                        FMM_HOST));
     }
@@ -175,9 +230,18 @@ public:
     fmm_plan* handle() const noexcept { return plan_.get(); }
 
 private:
+    void set_exclusions(int near_too) const
+    {
+        if (mode_ == near_too) return;
+        check(fmm_plan_set_exclusions(plan_.get(), ex_ptr_.data(), ex_col_.data(), FMM_HOST, near_too));
+        mode_ = near_too;
+    }
     struct Del { void operator()(fmm_plan* q) const { fmm_plan_destroy(q); } };
     int64_t n_;
     std::unique_ptr<fmm_plan, Del> plan_;
+    std::vector<int64_t> ex_ptr_;
+    std::vector<int32_t> ex_col_;
+    mutable int mode_ = -1;
 };
 
 }  // namespace simplefmm_b200

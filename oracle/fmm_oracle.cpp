@@ -275,13 +275,25 @@ void build_nlist(Tree& T, int lvl)
     }
 }
 
-// partition.hpp:406-446
-Tree* build_tree(const double* pos, int64_t n, int max_level, int max_ppn, int vertical_axis, double phideg)
+// partition.hpp:406-446; box = {corner x, y, z, width} gives the cube of
+// Box(corner, width, vertical_axis, phideg) (box.hpp:73-82), else it is fitted.
+Tree* build_tree(const double* pos, int64_t n, int max_level, int max_ppn, int vertical_axis, double phideg,
+                 const double* box = nullptr)
 {
     auto* T = new Tree;
     T->n = n;
     T->pos.assign(pos, pos + 3 * n);
-    T->cube = make_cube(pos, n, vertical_axis, phideg);
+    if (box) {
+        Cube& b = T->cube;
+        b.X = (vertical_axis + 1) % 3;
+        b.Y = (vertical_axis + 2) % 3;
+        b.Z = vertical_axis;
+        b.phi = phideg * (M_PI / 180);
+        for (int a = 0; a < 3; ++a) b.corner[a] = box[a];
+        b.width = box[3];
+    } else {
+        T->cube = make_cube(pos, n, vertical_axis, phideg);
+    }
     T->root = std::make_unique<Node>();
     T->root->level = 0;
     T->root->key = 0;
@@ -743,6 +755,12 @@ int64_t oracle_key(const double* pos, int64_t n, int vertical_axis, double phide
 void* oracle_tree_build(const double* pos, int64_t n, int max_level, int max_ppn, int vertical_axis, double phideg)
 {
     return build_tree(pos, n, max_level, max_ppn, vertical_axis, phideg);
+}
+
+void* oracle_tree_build_box(const double* pos, int64_t n, int max_level, int max_ppn, int vertical_axis,
+                            double phideg, const double* box4)
+{
+    return build_tree(pos, n, max_level, max_ppn, vertical_axis, phideg, box4);
 }
 
 void oracle_tree_free(void* t) { delete static_cast<Tree*>(t); }

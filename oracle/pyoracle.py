@@ -35,6 +35,8 @@ def lib():
         L.oracle_key.restype = i64
         L.oracle_tree_build.argtypes = [dp, i64, C.c_int, C.c_int, C.c_int, C.c_double]
         L.oracle_tree_build.restype = vp
+        L.oracle_tree_build_box.argtypes = [dp, i64, C.c_int, C.c_int, C.c_int, C.c_double, dp]
+        L.oracle_tree_build_box.restype = vp
         L.oracle_tree_free.argtypes = [vp]
         L.oracle_tree_depth.argtypes = [vp]
         L.oracle_tree_export.argtypes = [vp, C.c_int, C.c_int, vp]
@@ -67,11 +69,17 @@ def keys(pos, level, vertical_axis=2, phideg=0.0) -> np.ndarray:
 class Tree:
     """Restated octree; ``dump()`` mirrors the reference driver's tree sections."""
 
-    def __init__(self, pos, max_level=20, max_ppn=64, vertical_axis=2, phideg=0.0):
+    def __init__(self, pos, max_level=20, max_ppn=64, vertical_axis=2, phideg=0.0, box=None):
         self.pos = np.ascontiguousarray(pos, dtype=np.float64)
         self.n = self.pos.shape[0]
         self.vertical_axis, self.phideg = vertical_axis, phideg
-        self._h = lib().oracle_tree_build(_dp(self.pos), self.n, max_level, max_ppn, vertical_axis, phideg)
+        self._box = None if box is None else np.array([box[1], box[0][0], box[0][1], box[0][2]], dtype=np.float64)
+        if box is None:
+            self._h = lib().oracle_tree_build(_dp(self.pos), self.n, max_level, max_ppn, vertical_axis, phideg)
+        else:
+            b4 = np.array([box[0][0], box[0][1], box[0][2], box[1]], dtype=np.float64)
+            self._h = lib().oracle_tree_build_box(_dp(self.pos), self.n, max_level, max_ppn, vertical_axis, phideg,
+                                                  _dp(b4))
         self.depth = lib().oracle_tree_depth(self._h)
 
     def __del__(self):
@@ -88,7 +96,8 @@ class Tree:
         return out
 
     def dump(self) -> dict:
-        d = {"BOX": cube(self.pos, self.vertical_axis, self.phideg), "DEPTH": np.array([self.depth, 1], np.int32)}
+        box = self._box if self._box is not None else cube(self.pos, self.vertical_axis, self.phideg)
+        d = {"BOX": box, "DEPTH": np.array([self.depth, 1], np.int32)}
         for l in range(self.depth + 1):
             d[f"CNODE{l}"] = self._export(l, 0, np.int64)
             d[f"ILEAF{l}"] = self._export(l, 1, np.int32)
@@ -156,3 +165,33 @@ def error_scales(pos, Q, targets=None):
         targets = np.arange(np.asarray(pos).shape[0])
     s = direct(pos, Q, targets, mode="scale")
     return s[:, 0], s[:, 1]
+
+
+def subtract_exclusions(tree: "Tree", pos, Q, row_ptr, cols, near_too, pot=None, field=None):
+    """fmm.hpp:398-408, 773-807: remove the listed pairs (j != i) from results
+    computed with the default is_self -- all of them (near_too), or only those
+    outside i's near field (the reference's slist).  In place."""
+    d = tree.dump()
+    parts = d["PARTS"].reshape(-1, 2)
+    pos = np.asarray(pos, dtype=np.float64)
+    Q = np.asarray(Q, dtype=np.float64)
+    n = pos.shape[0]
+    for i in range(n):
+        li, fi = parts[i]
+        ptr, val = d[f"NLP{li}"], d[f"NLV{li}"].reshape(-1, 2)
+        near_set = {tuple(x) for x in val[ptr[fi]:ptr[fi + 1]]}
+        for e in range(row_ptr[i], row_ptr[i + 1]):
+            j = int(cols[e])
+            if j == i:
+                continue
+            if not near_too and tuple(parts[j]) in near_set:
+                continue
+            R = pos[i] - pos[j]
+            r = np.sqrt(R @ R)
+            if pot is not None:
+                pot[i] -= Q[j] / r
+            if field is not None:
+                if Q.ndim == 1:
+                    field[i] -= Q[j] * R / r**3
+                else:
+                    field[i] -= np.cross(Q[j], R) / r**3

@@ -15,7 +15,13 @@
 // flags: 1 tree dump, 2 scalar potential (qdim 1), 4 scalar field via two
 //        rinv<true> runs with Q=(q,0,0),(0,0,q) (qdim 1), 8 vector potential
 //        (qdim 3), 16 rinv<true> with vector charges (qdim 3), 32 skip the
-//        evaluation, only time the tree.
+//        evaluation, only time the tree, 64 explicit cube (Box(corner, width,
+//        vertical_axis, phideg), box.hpp:73-82): double corner[3], width follow
+//        the charges, 128 / 256 exclusions: int32 s1, s2 follow (after the
+//        cube if any); FMM3D gets self_generator(i) = {i, (i+s1)%n, (i+s2)%n}
+//        (fmm.hpp:204, 398-408) and rinv runs with the matching is_self (128)
+//        or with the default is_self i == j, so only the non-neighbour
+//        exclusions (slist) are removed (256).
 // Output: "SFMMOUT1" then sections: char tag[8], int64 nbytes, payload.
 #include <mpi.h>
 
@@ -73,6 +79,21 @@ struct Job {
     int qdim, flags;
     std::vector<V3> pos;
     std::vector<double> q;
+    double corner[3] = {0, 0, 0}, width = 0;
+    int s1 = 0, s2 = 0;
+
+    std::vector<int> self(int i) const
+    {
+        if (!(flags & (128 | 256))) return {i};
+        const int n = static_cast<int>(this->n);
+        return {i, (i + s1) % n, (i + s2) % n};
+    }
+    bool is_self(int i, int j) const
+    {
+        if (!(flags & 128)) return i == j;
+        const int n = static_cast<int>(this->n);
+        return j == i || j == (i + s1) % n || j == (i + s2) % n;
+    }
 };
 
 // per-p evaluation entry points (one translation unit per p, see Makefile)
@@ -86,12 +107,12 @@ void run_p(const Job& job, const Part& part, Out& out, int rank)
     const size_t n = static_cast<size_t>(job.n);
     if (job.flags & 2) {
         double t0 = timed_barrier();
-        FMM3D<double, 1, p, Vector> fmm(part, MPI_COMM_WORLD);
+        FMM3D<double, 1, p, Vector> fmm(part, MPI_COMM_WORLD, [&](int i) { return job.self(i); });
         double t1 = timed_barrier();
         std::vector<V1> Q(n), U(n);
         for (size_t i = 0; i < n; ++i) { Q[i][0] = job.q[i]; U[i][0] = 0; }
         double t2 = timed_barrier();
-        fmm.rinv(Q.data(), U.data());
+        fmm.rinv(Q.data(), U.data(), [&](int i, int j) { return job.is_self(i, j); });
         MPI_Allreduce(MPI_IN_PLACE, U.data(), int(n), MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
         double t3 = timed_barrier();
         if (rank == 0) {
@@ -102,7 +123,7 @@ void run_p(const Job& job, const Part& part, Out& out, int rank)
     }
     if ((job.flags & 4) || (job.flags & 16)) {
         double t0 = timed_barrier();
-        FMM3D<double, 3, p, Vector, true> fmm(part, MPI_COMM_WORLD);
+        FMM3D<double, 3, p, Vector, true> fmm(part, MPI_COMM_WORLD, [&](int i) { return job.self(i); });
         double t1 = timed_barrier();
         if (rank == 0) out.scalar("T_CTOR3G", t1 - t0);
         std::vector<V3> Q(n), U(n);
@@ -115,7 +136,7 @@ void run_p(const Job& job, const Part& part, Out& out, int rank)
                     U[i] = V3{{0, 0, 0}};
                 }
                 double t2 = timed_barrier();
-                fmm.template rinv<true>(Q.data(), U.data());
+                fmm.template rinv<true>(Q.data(), U.data(), [&](int i, int j) { return job.is_self(i, j); });
                 MPI_Allreduce(MPI_IN_PLACE, U.data(), int(3 * n), MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
                 double t3 = timed_barrier();
                 tt += t3 - t2;
@@ -139,7 +160,7 @@ void run_p(const Job& job, const Part& part, Out& out, int rank)
                 U[i] = V3{{0, 0, 0}};
             }
             double t2 = timed_barrier();
-            fmm.template rinv<true>(Q.data(), U.data());
+            fmm.template rinv<true>(Q.data(), U.data(), [&](int i, int j) { return job.is_self(i, j); });
             MPI_Allreduce(MPI_IN_PLACE, U.data(), int(3 * n), MPI_DOUBLE, MPI_SUM, MPI_COMM_WORLD);
             double t3 = timed_barrier();
             if (rank == 0) {
@@ -279,6 +300,16 @@ int main(int argc, char** argv)
     ok = ok && std::fread(raw.data(), 8, raw.size(), in) == raw.size();
     job.q.resize(static_cast<size_t>(job.n) * job.qdim);
     ok = ok && std::fread(job.q.data(), 8, job.q.size(), in) == job.q.size();
+    if (ok && (job.flags & 64)) {
+        double cw[4];
+        ok = std::fread(cw, 8, 4, in) == 4;
+        job.corner[0] = cw[0]; job.corner[1] = cw[1]; job.corner[2] = cw[2]; job.width = cw[3];
+    }
+    if (ok && (job.flags & (128 | 256))) {
+        int32_t ss[2];
+        ok = std::fread(ss, 4, 2, in) == 2;
+        job.s1 = ss[0]; job.s2 = ss[1];
+    }
     std::fclose(in);
     if (!ok) { std::fprintf(stderr, "bad input file\n"); return 2; }
     job.pos.resize(static_cast<size_t>(job.n));
@@ -291,7 +322,9 @@ int main(int argc, char** argv)
         std::fwrite("SFMMOUT1", 1, 8, out.f);
     }
     const double t0 = timed_barrier();
-    BoxT box(job.pos, job.vertical_axis, job.phideg);
+    BoxT box = (job.flags & 64) ? BoxT(V3{{job.corner[0], job.corner[1], job.corner[2]}}, job.width, job.vertical_axis,
+                                       job.phideg)
+                                  : BoxT(job.pos, job.vertical_axis, job.phideg);
     Part part(job.pos, box);
     part.refine(job.max_level, job.max_ppn);
     const double t1 = timed_barrier();

@@ -26,6 +26,9 @@ FLAG_FIELD = 4
 FLAG_VECPOT = 8
 FLAG_BIOT = 16
 FLAG_TREE_ONLY = 32
+FLAG_BOX = 64            # explicit cube: corner (3) and width follow the charges
+FLAG_EXCLUDE = 128       # self_generator {i, i+s1, i+s2} with the matching is_self
+FLAG_EXCLUDE_FAR = 256   # the same generator, default is_self (only non-neighbours removed)
 
 
 def ref_binary(native: bool = False) -> Path:
@@ -36,7 +39,8 @@ def have_reference(native: bool = False) -> bool:
     return ref_binary(native).exists()
 
 
-def write_input(path, pos, q, p, max_level, max_ppn, vertical_axis=2, phideg=0.0, flags=FLAG_POT):
+def write_input(path, pos, q, p, max_level, max_ppn, vertical_axis=2, phideg=0.0, flags=FLAG_POT,
+                box=None, strides=None):
     pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
     q = np.ascontiguousarray(q, dtype=np.float64)
     qdim = 1 if q.ndim == 1 else q.shape[1]
@@ -45,6 +49,10 @@ def write_input(path, pos, q, p, max_level, max_ppn, vertical_axis=2, phideg=0.0
         f.write(struct.pack("<q4id2i", pos.shape[0], p, max_level, max_ppn, vertical_axis, phideg, qdim, flags))
         f.write(pos.tobytes())
         f.write(q.reshape(-1).tobytes())
+        if flags & FLAG_BOX:
+            f.write(struct.pack("<4d", box[0][0], box[0][1], box[0][2], box[1]))
+        if flags & (FLAG_EXCLUDE | FLAG_EXCLUDE_FAR):
+            f.write(struct.pack("<2i", strides[0], strides[1]))
 
 
 _INT64_TAGS = ("CNODE", "CLV", "PL")
@@ -76,14 +84,14 @@ def read_output(path) -> dict:
 
 
 def run_reference(pos, q, p, max_level=20, max_ppn=64, vertical_axis=2, phideg=0.0,
-                  flags=FLAG_POT, ranks=1, native=False, timeout=3600) -> dict:
+                  flags=FLAG_POT, ranks=1, native=False, timeout=3600, box=None, strides=None) -> dict:
     """Run the compiled reference on (pos, q) and return its parsed output."""
     binary = ref_binary(native)
     if not binary.exists():
         raise FileNotFoundError(f"{binary} is not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.bin"), os.path.join(td, "out.bin")
-        write_input(fin, pos, q, p, max_level, max_ppn, vertical_axis, phideg, flags)
+        write_input(fin, pos, q, p, max_level, max_ppn, vertical_axis, phideg, flags, box, strides)
         env = dict(os.environ, SIMPLEFMM_SHIM_NP=str(ranks))
         r = subprocess.run([str(binary), fin, fout], env=env, capture_output=True, timeout=timeout)
         if r.returncode != 0:

@@ -60,6 +60,8 @@ def load_library():
         "fmm_host_unregister": ([vp], i32),
         "fmm_tree_build": ([vp, vp, i64, i32, i32, i32, i32, dbl, C.POINTER(vp)], i32),
         "fmm_tree_destroy": ([vp], i32),
+        "fmm_tree_build_box": ([vp, vp, i64, i32, C.POINTER(dbl), dbl, i32, i32, i32, dbl, C.POINTER(vp)], i32),
+        "fmm_plan_set_exclusions": ([vp, vp, vp, i32, i32], i32),
         "fmm_tree_depth": ([vp, C.POINTER(i32)], i32),
         "fmm_tree_box": ([vp, C.POINTER(dbl), C.POINTER(dbl)], i32),
         "fmm_tree_export_size": ([vp, i32, i32, C.POINTER(i64)], i32),
@@ -150,15 +152,23 @@ class Tree:
     """Box + adaptive octree + lists, built and kept on the device."""
 
     def __init__(self, positions, max_level: int = 20, max_particles_per_node: int = 64, vertical_axis: int = 2,
-                 phideg: float = 0.0, ctx: Context | None = None):
+                 phideg: float = 0.0, ctx: Context | None = None, box=None):
+        """box = (corner[3], width) gives the root cube explicitly (Box(corner, width, ...));
+        otherwise it is fitted to the points."""
         self.ctx = ctx or default_context()
         if isinstance(positions, np.ndarray):
             positions = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1, 3)
         n = int(positions.shape[0])
         addr, where = _ptr(positions)
         h = C.c_void_p()
-        _check(load_library().fmm_tree_build(self.ctx._h, C.c_void_p(addr), n, where, max_level,
-                                             max_particles_per_node, vertical_axis, float(phideg), C.byref(h)))
+        L = load_library()
+        if box is None:
+            _check(L.fmm_tree_build(self.ctx._h, C.c_void_p(addr), n, where, max_level,
+                                    max_particles_per_node, vertical_axis, float(phideg), C.byref(h)))
+        else:
+            corner = (C.c_double * 3)(*[float(x) for x in box[0]])
+            _check(L.fmm_tree_build_box(self.ctx._h, C.c_void_p(addr), n, where, corner, float(box[1]), max_level,
+                                        max_particles_per_node, vertical_axis, float(phideg), C.byref(h)))
         self._h = h
         self.n = n
         self.max_level, self.max_ppn = max_level, max_particles_per_node
@@ -267,6 +277,18 @@ class Plan:
             Q = np.ascontiguousarray(Q, dtype=np.float64)
             qa = Q.ctypes.data
         _check(load_library().fmm_rinv(self._h, C.c_void_p(qa), C.c_void_p(ua), int(bool(gradient)), wq))
+
+    def set_exclusions(self, row_ptr, cols, near_too: bool = True):
+        """Excluded sources per target (CSR over original indices); None clears.
+        near_too=False: the reference's slist under the default is_self."""
+        L = load_library()
+        if row_ptr is None:
+            _check(L.fmm_plan_set_exclusions(self._h, None, None, HOST, 0))
+            return
+        rp = np.ascontiguousarray(row_ptr, dtype=np.int64)
+        cl = np.ascontiguousarray(cols, dtype=np.int32)
+        _check(L.fmm_plan_set_exclusions(self._h, C.c_void_p(rp.ctypes.data), C.c_void_p(cl.ctypes.data), HOST,
+                                         int(bool(near_too))))
 
     def timings(self) -> dict:
         t = (C.c_double * 6)()

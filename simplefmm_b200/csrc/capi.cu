@@ -174,8 +174,8 @@ int fmm_host_unregister(void* ptr)
     API_CATCH
 }
 
-int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level, int max_ppn,
-                   int vertical_axis, double phideg, fmm_tree** out)
+static int tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level, int max_ppn,
+                      int vertical_axis, double phideg, const double* corner3, double width, fmm_tree** out)
 {
     API_TRY
     if (!ctx || !out || !xyz) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -196,12 +196,62 @@ int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, in
             SFMM_CUDA(cudaMemcpyAsync(staged.ptr, xyz, size_t(3) * n * sizeof(double), cudaMemcpyHostToDevice, ctx->c.stream));
             dxyz = staged.ptr;
         }
-        sfmm::build_tree(tr->t, dxyz, max_level, max_ppn, vertical_axis, phideg);
+        sfmm::build_tree(tr->t, dxyz, max_level, max_ppn, vertical_axis, phideg, corner3, width);
     } catch (...) {
         release_tree(tr);
         throw;
     }
     *out = tr;
+    API_CATCH
+}
+
+int fmm_tree_build(fmm_context* ctx, const double* xyz, int64_t n, int where, int max_level, int max_ppn,
+                   int vertical_axis, double phideg, fmm_tree** out)
+{
+    return tree_build(ctx, xyz, n, where, max_level, max_ppn, vertical_axis, phideg, nullptr, 0.0, out);
+}
+
+int fmm_tree_build_box(fmm_context* ctx, const double* xyz, int64_t n, int where, const double* corner3,
+                       double width, int max_level, int max_ppn, int vertical_axis, double phideg, fmm_tree** out)
+{
+    if (!corner3) return fail(FMM_ERR_INVALID_ARGUMENT, "corner is NULL");
+    return tree_build(ctx, xyz, n, where, max_level, max_ppn, vertical_axis, phideg, corner3, width, out);
+}
+
+int fmm_plan_set_exclusions(fmm_plan* plan, const int64_t* row_ptr, const int32_t* cols, int where, int near_too)
+{
+    API_TRY
+    if (!plan) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL plan");
+    if (where != FMM_HOST && where != FMM_DEVICE) return fail(FMM_ERR_INVALID_ARGUMENT, "where must be FMM_HOST or FMM_DEVICE");
+    sfmm::Plan& pl = plan->pl;
+    bind(*pl.tree->ctx);
+    if (!row_ptr) {
+        sfmm::plan_clear_exclusions(pl);
+        return FMM_OK;
+    }
+    const int64_t n = pl.tree->n;
+    if (where == FMM_DEVICE) {
+        if (!cols) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL cols");
+        sfmm::plan_set_exclusions(pl, row_ptr, cols, near_too);
+        SFMM_CUDA(cudaStreamSynchronize(pl.tree->ctx->stream));
+        return FMM_OK;
+    }
+    if (row_ptr[0] != 0) return fail(FMM_ERR_INVALID_ARGUMENT, "row_ptr[0] must be 0");
+    for (int64_t i = 0; i < n; ++i)
+        if (row_ptr[i + 1] < row_ptr[i]) return fail(FMM_ERR_INVALID_ARGUMENT, "row_ptr must be non-decreasing");
+    const int64_t nnz = row_ptr[n];
+    if (nnz > 0 && !cols) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL cols");
+    for (int64_t e = 0; e < nnz; ++e)
+        if (cols[e] < 0 || cols[e] >= n) return fail(FMM_ERR_INVALID_ARGUMENT, "excluded index out of range");
+    cudaStream_t st = pl.tree->ctx->stream;
+    sfmm::DevBuf<int64_t> dptr;
+    sfmm::DevBuf<int32_t> dcol;
+    dptr.alloc(n + 1, st);
+    dcol.alloc(std::max<int64_t>(nnz, 1), st);
+    SFMM_CUDA(cudaMemcpyAsync(dptr.ptr, row_ptr, size_t(n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
+    if (nnz) SFMM_CUDA(cudaMemcpyAsync(dcol.ptr, cols, size_t(nnz) * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    sfmm::plan_set_exclusions(pl, dptr.ptr, dcol.ptr, near_too);
+    SFMM_CUDA(cudaStreamSynchronize(st));
     API_CATCH
 }
 

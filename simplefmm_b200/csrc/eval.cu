@@ -471,6 +471,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     SFMM_CUDA(cudaEventRecord(pl.ev[4], st));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
     SFMM_CHECK_LAUNCH();
+    if (pl.ex_on) apply_exclusions(pl, Q, pot, field);
     SFMM_CUDA(cudaEventRecord(pl.ev[5], st));
 }
 

@@ -80,6 +80,12 @@ struct Plan {
     int rfrag_nf = 0;
     DevBuf<float> rf32, tz32, tzl32;
     int rf32_nf = 0, tz32_nf = 0;
+    // excluded source lists (self_generator / is_self): CSR over original target
+    // indices, original -> sorted index, sorted point -> leaf
+    DevBuf<int64_t> ex_ptr;
+    DevBuf<int32_t> ex_col, ex_inv, ex_leaf;
+    int ex_near_too = 0;
+    bool ex_on = false;
     DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
@@ -93,5 +99,9 @@ void plan_init(Plan& pl);
 void build_m2l_fragments(Plan& pl, cudaStream_t st);
 void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
 void plan_read_timings(Plan& pl, double* ms6);
+// Exclusions (exclude.cu): ptr / cols are device arrays (n + 1, ptr[n]).
+void plan_set_exclusions(Plan& pl, const int64_t* ptr, const int32_t* cols, int near_too);
+void plan_clear_exclusions(Plan& pl);
+void apply_exclusions(const Plan& pl, const double* Q, double* pot, double* field);
 
 }  // namespace sfmm

@@ -209,7 +209,10 @@ struct Tree {
 struct Plan;
 
 // tree.cu
-void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg);
+// corner3 / width: an explicit root cube (Box(corner, width, ...), box.hpp:73-82)
+// instead of the one fitted to the points (box.hpp:84-107); corner3 == nullptr fits.
+void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg,
+                const double* corner3 = nullptr, double width = 0.0);
 int64_t tree_export(const Tree& t, int level, int what, void* host_out);
 
 // direct.cu

@@ -534,7 +534,8 @@ T read_one(const T* d, cudaStream_t s)
 
 }  // namespace
 
-void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vertical_axis, double phideg)
+void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vertical_axis, double phideg,
+                const double* corner3, double width)
 {
     cudaStream_t st = t.ctx->stream;
     const int64_t n = t.n;
@@ -562,7 +563,15 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     b.rotated = phideg != 0.0;
     b.cphi = std::cos(phi);
     b.sphi = std::sin(phi);
-    {
+    if (corner3) {
+        // explicit cube: corner in the (rotated) key frame, as the reference stores it
+        SFMM_REQUIRE(width > 0 && std::isfinite(width), FMM_ERR_INVALID_ARGUMENT, "box width must be positive");
+        b.width = width;
+        for (int a = 0; a < 3; ++a) b.corner[a] = corner3[a];
+        b.status = FMM_OK;
+        t.d_box.alloc(1, st);
+        SFMM_CUDA(cudaMemcpyAsync(t.d_box.ptr, &b, sizeof(b), cudaMemcpyHostToDevice, st));
+    } else {
         const int nb = static_cast<int>(std::min<int64_t>(kBoxBlocks, (n + 255) / 256));
         DevBuf<double> partial;
         partial.alloc(6 * nb, st);

@@ -33,6 +33,25 @@ def load_golden(name):
     return d
 
 
+def golden_tree(sf, g, ctx):
+    """The library's tree for a golden case (explicit root cube if the case has one)."""
+    box = (g["box_corner"], float(g["box_width"][0])) if "box_corner" in g else None
+    return sf.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"], ctx=ctx, box=box)
+
+
+def golden_exclusions(g):
+    """(row_ptr, cols, near_too) of a case's self_generator {i, i+s1, i+s2}, or None."""
+    if "strides" not in g:
+        return None
+    n = g["n"]
+    s1, s2 = (int(x) for x in g["strides"])
+    i = np.arange(n)
+    cols = np.stack([i, (i + s1) % n, (i + s2) % n], axis=1).reshape(-1).astype(np.int32)
+    row_ptr = np.arange(0, 3 * n + 1, 3, dtype=np.int64)
+    near_too = bool(g["flags"] & 128)
+    return row_ptr, cols, near_too
+
+
 TREE_KEYS = ("CNODE", "ILEAF", "IDXP", "IDXV", "ILP", "ILV", "CLP", "CLV", "PL", "NLP", "NLV")
 
 

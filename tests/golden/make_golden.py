@@ -36,7 +36,15 @@ CASES = {
     "axis0_n3000_p6": ("plummer", 3000, 19, 6, 20, 32, 0, 0.0, T | POT, "uniform", 1),
     "phi30_n3000_p6": ("uniform", 3000, 20, 6, 20, 32, 2, 30.0, T | POT, "uniform", 1),
     "uniform_n3000_p12": ("uniform", 3000, 21, 12, 20, 64, 2, 0.0, POT | FIELD, "uniform", 1),
+    "box_n3000_p6": ("uniform", 3000, 22, 6, 20, 64, 2, 0.0, T | POT | FIELD | refio.FLAG_BOX, "uniform", 1),
+    "exclude_n3000_p6": ("plummer", 3000, 23, 6, 20, 32, 2, 0.0, POT | FIELD | refio.FLAG_EXCLUDE, "uniform", 1),
+    "exclude_far_n3000_p6": ("plummer", 3000, 24, 6, 20, 32, 2, 0.0, POT | FIELD | refio.FLAG_EXCLUDE_FAR,
+                             "uniform", 1),
 }
+
+# explicit root cube (corner, width) and exclusion strides of the cases above
+BOXES = {"box_n3000_p6": ((-0.25, -0.5, -0.125), 2.0)}
+STRIDES = {"exclude_n3000_p6": (1, 1777), "exclude_far_n3000_p6": (1, 1777)}
 
 
 def make_case(name, spec):
@@ -44,8 +52,13 @@ def make_case(name, spec):
     pos = W.points(dist, n, seed)
     q = W.charges(n, seed, qkind, qdim)
     out = refio.run_reference(pos, q, p=p, max_level=max_level, max_ppn=ppn, vertical_axis=va,
-                              phideg=phideg, flags=flags, native=True)
+                              phideg=phideg, flags=flags, native=True, box=BOXES.get(name), strides=STRIDES.get(name))
     arrays = {k: v for k, v in out.items() if not k.startswith("T_")}
+    if name in BOXES:
+        arrays["box_corner"] = np.array(BOXES[name][0])
+        arrays["box_width"] = np.array([BOXES[name][1]])
+    if name in STRIDES:
+        arrays["strides"] = np.array(STRIDES[name])
     meta = np.array([n, seed, p, max_level, ppn, va, flags, qdim], dtype=np.int64)
     np.savez_compressed(HERE / f"{name}.npz", pos=pos, q=q, meta=meta, phideg=np.array([phideg]),
                         dist=np.array([dist]), **arrays)
@@ -54,7 +67,10 @@ def make_case(name, spec):
 def main():
     if not refio.have_reference(native=True):
         sys.exit("oracle/_ref/ref_driver_native is not built (make -C oracle ref)")
+    only = set(sys.argv[1:])
     for name, spec in CASES.items():
+        if only and name not in only:
+            continue
         make_case(name, spec)
         print("wrote", name)
 

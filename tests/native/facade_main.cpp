@@ -58,3 +58,16 @@ int main()
     std::printf("Relative l2 error of field = %.3e\n", std::sqrt(nf / df));
     return (std::sqrt(np / dp) < 1e-4 && std::sqrt(nf / df) < 1e-3) ? 0 : 1;
 }
+
+// Compile-time check of the rest of the facade API (explicit cube,
+// self_generator / is_self); exercised through the C ABI by the GPU tests.
+[[maybe_unused]] static void facade_api_compiles(std::vector<Vector<double, 3>>& pos, std::vector<Vector<double, 1>>& q,
+                                                 std::vector<Vector<double, 1>>& u)
+{
+    Box<double, 3, Vector> box(Vector<double, 3>{{0.0, 0.0, 0.0}}, 1.0, 2, 0.0);
+    OctreePartitioner<double, Vector> part(pos, box);
+    part.refine(20, 64);
+    FMM3D<double, 1, 6, Vector> fmm(part, 0, [](int i) { return std::vector<int>{i, i + 1}; });
+    fmm.rinv(q.data(), u.data());
+    fmm.rinv(q.data(), u.data(), [](int i, int j) { return j == i || j == i + 1; });
+}

@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import simplefmm_b200 as sf
-from conftest import golden_cases, load_golden, rel_err_per_target, rel_l2, tree_keys
+from conftest import golden_cases, golden_exclusions, golden_tree, load_golden, rel_err_per_target, rel_l2, tree_keys
 from oracle import pyoracle
 from simplefmm_b200 import workloads as W
 
@@ -27,7 +27,7 @@ def ctx():
 @pytest.mark.parametrize("name", golden_cases())
 def test_tree_bit_exact(ctx, name):
     g = load_golden(name)
-    t = sf.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"], ctx=ctx)
+    t = golden_tree(sf, g, ctx)
     d = t.dump()
     assert t.depth == int(g["DEPTH"][0])
     if "CNODE0" not in g:
@@ -40,8 +40,11 @@ def test_tree_bit_exact(ctx, name):
 @pytest.mark.parametrize("name", golden_cases())
 def test_results_match_reference(ctx, name):
     g = load_golden(name)
-    t = sf.Tree(g["pos"], g["max_level"], g["max_ppn"], g["vertical_axis"], g["phideg"], ctx=ctx)
+    t = golden_tree(sf, g, ctx)
     plan = sf.Plan(t, g["p"], g["qdim"])
+    ex = golden_exclusions(g)
+    if ex is not None:
+        plan.set_exclusions(*ex)
     sp, sf_ = pyoracle.error_scales(g["pos"], g["q"])
     n = g["n"]
     if g["qdim"] == 1:
