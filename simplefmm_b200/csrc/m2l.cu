@@ -887,6 +887,13 @@ struct MmaMeta {
     int src[8], bq[8], sb[8], pidx[8];
 };
 
+// column table of a tile of C columns
+template<int C>
+struct MetaC {
+    int cls, ncol, dsq, pad;
+    int src[C], bq[C], sb[C], pidx[C];
+};
+
 // Compile-time loop: f(std::integral_constant<int, I>) for I in [B, E).
 template<int B, int E, typename F>
 __device__ __forceinline__ void static_for(F&& f)
@@ -898,9 +905,14 @@ __device__ __forceinline__ void static_for(F&& f)
 }
 
 // padded leading dimension of a [col][row] operand buffer: >= rows + 4 (K
-// chunks read up to 3 rows past an order) and = 4 mod 16 doubles, which
+// chunks read up to 3 rows past an order) and = 4 or 12 mod 16 doubles, which
 // makes the B-fragment loads (4 rows x 8 columns) bank-conflict free
-__host__ __device__ constexpr int mma_ld(int rows) { return ((rows + 4 + 11) / 16) * 16 + 4; }
+__host__ __device__ constexpr int mma_ld(int rows)
+{
+    int ld = rows + 4;
+    while (ld % 16 != 4 && ld % 16 != 12) ++ld;
+    return ld;
+}
 // rotation jobs (n, rt), n = P..0: index of the first job of order n
 __host__ __device__ constexpr int rot_job0(int P, int n)
 {
@@ -916,53 +928,53 @@ __host__ __device__ constexpr int tz_job0(int P, int k)
     return s;
 }
 
-template<int P>
+template<int P, int NS>
 struct MmaLayout {
+    static constexpr int NC = 8 * NS;                           // columns per tile (NS MMA N-tiles)
     static constexpr int T = (P + 1) * (P + 2) / 2;
     static constexpr int T1 = (P + 2) * (P + 3) / 2;
     static constexpr int LD = mma_ld(T), LD1 = mma_ld(T1);        // column strides (doubles)
-    static constexpr int ent_src = 0;
-    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
-    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
+    static constexpr int kids = 0;                                 // ilist offsets of the 8 children
+    static constexpr int sorted = al16(kids + 4 * 9);
     static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
     static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
     static constexpr int cls_off = al16(cls_cnt + 4 * 72);
     static constexpr int bat_off = al16(cls_off + 4 * 72);
     static constexpr int meta = al16(bat_off + 4 * 72);
-    static constexpr int tm = al16(meta + int(sizeof(MmaMeta)) * 3);
-    static constexpr int Xraw = al16(tm + T1);                    // 2 x [col][T] complex (cp.async)
-    static constexpr int X = al16(Xraw + 2 * 8 * T * 16);          // re, im: [col][LD] doubles each
-    static constexpr int W = al16(X + 2 * 8 * LD * 8);             // azimuth-major rows
-    static constexpr int LzA = al16(W + 2 * 8 * LD * 8);
-    static constexpr int LzB = al16(LzA + 2 * 8 * LD * 8);         // [col][LD1]
-    static constexpr int acc = al16(LzB + 2 * 8 * LD1 * 8);        // [8 qd][T] then [8 qd][T1] complex
+    static constexpr int tm = al16(meta + int(sizeof(MetaC<NC>)) * 3);
+    static constexpr int Xraw = al16(tm + T1);                    // [col][T] complex (cp.async)
+    static constexpr int X = al16(Xraw + NC * T * 16);              // re, im: [col][LD] doubles each
+    static constexpr int W = al16(X + 2 * NC * LD * 8);             // azimuth-major rows
+    static constexpr int LzA = al16(W + 2 * NC * LD * 8);
+    static constexpr int LzB = al16(LzA + 2 * NC * LD * 8);         // [col][LD1]
+    static constexpr int acc = al16(LzB + 2 * NC * LD1 * 8);        // [8 qd][T] then [8 qd][T1] complex
     __host__ __device__ static constexpr int total(int qd) { return al16(acc + 16 * 8 * qd * (T + T1)); }
 };
 
-template<int P>
-__global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int64_t g1)
+template<int P, int NS, int NW>
+__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a, int64_t g0, int64_t g1)
 {
-    using L = MmaLayout<P>;
-    constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 256;
+    using L = MmaLayout<P, NS>;
+    constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 32 * NW, NC = L::NC;
+    using Meta = MetaC<NC>;
     extern __shared__ __align__(16) unsigned char sm[];
-    int* ent_src = reinterpret_cast<int*>(sm + L::ent_src);
-    int* ent_code = reinterpret_cast<int*>(sm + L::ent_code);
+    int* kids = reinterpret_cast<int*>(sm + L::kids);
     short* sorted = reinterpret_cast<short*>(sm + L::sorted);
     unsigned char* cls = sm + L::cls;
     int* cls_cnt = reinterpret_cast<int*>(sm + L::cls_cnt);
     int* cls_off = reinterpret_cast<int*>(sm + L::cls_off);
     int* bat_off = reinterpret_cast<int*>(sm + L::bat_off);
-    MmaMeta* meta = reinterpret_cast<MmaMeta*>(sm + L::meta);
+    Meta* meta = reinterpret_cast<Meta*>(sm + L::meta);
     unsigned char* tm = sm + L::tm;
     cplx* Xraw = reinterpret_cast<cplx*>(sm + L::Xraw);
     double* Xre = reinterpret_cast<double*>(sm + L::X);
-    double* Xim = Xre + 8 * LD;
+    double* Xim = Xre + NC * LD;
     double* Wre = reinterpret_cast<double*>(sm + L::W);
-    double* Wim = Wre + 8 * LD;
+    double* Wim = Wre + NC * LD;
     double* Are = reinterpret_cast<double*>(sm + L::LzA);
-    double* Aim = Are + 8 * LD;
+    double* Aim = Are + NC * LD;
     double* Bre = reinterpret_cast<double*>(sm + L::LzB);
-    double* Bim = Bre + 8 * LD1;
+    double* Bim = Bre + NC * LD1;
     const int qd = a.qdim;
     cplx* accA = reinterpret_cast<cplx*>(sm + L::acc);
     cplx* accB = accA + 8 * qd * T;
@@ -984,20 +996,22 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
     const int NF = a.rfrag_nf;
 
     // column table of tile b (threads k < 8); c: class cursor
-    auto make_meta = [&](int b, int k, MmaMeta& M, int& c) {
+    auto make_meta = [&](int b, int k, Meta& M, int& c) {
         while (bat_off[c + 1] <= b) ++c;
-        const int col0 = (b - bat_off[c]) * 8;
-        const int ncol = min(8, cls_cnt[c] * qd - col0);
+        const int col0 = (b - bat_off[c]) * NC;
+        const int ncol = min(NC, cls_cnt[c] * qd - col0);
         if (k < ncol) {
             const int col = col0 + k;
             const int pair = col / qd;
             const int e = sorted[cls_off[c] + pair];
-            const int code = ent_code[e];
+            const int code = a.il_code[kids[0] + e];
             const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
             const int bq = col - pair * qd;
-            M.src[k] = ent_src[e];
+            int slot = 0;
+            while (kids[slot + 1] - kids[0] <= e) ++slot;
+            M.src[k] = a.il_src[kids[0] + e];
             M.bq[k] = bq;
-            M.sb[k] = ((code >> 9) & 7) * qd + bq;
+            M.sb[k] = slot * qd + bq;
             M.pidx[k] = 7 * (dj + 3) + (di + 3);
             if (k == 0) {
                 M.cls = c;
@@ -1013,10 +1027,10 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
     };
     // raw source moments of tile b -> Xraw[b & 1] (asynchronous)
     auto issue = [&](int b) {
-        const MmaMeta& M = meta[b % 3];
+        const Meta& M = meta[b % 3];
         const int ncol = M.ncol;
-        cplx* xr = Xraw + (b & 1) * 8 * T;
-        for (int e = tid; e < 8 * T; e += NT) {
+        cplx* xr = Xraw;
+        for (int e = tid; e < NC * T; e += NT) {
             const int c = e / T, t = e - c * T;
             if (c < ncol) cp_async16(xr + e, a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
         }
@@ -1024,10 +1038,10 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
     };
     // X = e^{i m phi} M for tile b, column-major
     auto phase_in = [&](int b) {
-        const MmaMeta& M = meta[b % 3];
+        const Meta& M = meta[b % 3];
         const int ncol = M.ncol;
-        const cplx* xr = Xraw + (b & 1) * 8 * T;
-        for (int e = tid; e < 8 * T; e += NT) {
+        const cplx* xr = Xraw;
+        for (int e = tid; e < NC * T; e += NT) {
             const int c = e / T, t = e - c * T;
             if (c < ncol) {
                 const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
@@ -1046,16 +1060,11 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
         // ---- group set-up: gather, stable class sort, tiles
         {
             const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
-            for (int s = 0; s < nc; ++s) {
-                const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
-                for (int e = q0 + tid; e < q1; e += NT) {
-                    const int code = a.il_code[e0 + e];
-                    ent_src[e] = a.il_src[e0 + e];
-                    ent_code[e] = code | (s << 9);
-                    cls[e] = static_cast<unsigned char>(
-                        rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
-                }
+            for (int e = tid; e < E; e += NT) {
+                const int code = a.il_code[e0 + e];
+                cls[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
             }
+            if (tid <= 8) kids[tid] = a.il_ptr[cb + min(tid, nc)];
             for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = cplx{0, 0};
             __syncthreads();
             for (int cl = tid; cl < kNumClasses; cl += NT) {
@@ -1070,7 +1079,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                     cls_off[c] = s;
                     bat_off[c] = k;
                     s += cls_cnt[c];
-                    k += (cls_cnt[c] * qd + 7) / 8;
+                    k += (cls_cnt[c] * qd + NC - 1) / NC;
                 }
                 cls_off[kNumClasses] = s;
                 bat_off[kNumClasses] = k;
@@ -1085,27 +1094,28 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
         }
         const int nbat = bat_off[kNumClasses];
         int cur = 0;                                      // class cursor of threads < 8
-        if (tid < 8 && nbat > 0) make_meta(0, tid, meta[0], cur);
+        if (tid < NC && nbat > 0) make_meta(0, tid, meta[0], cur);
         __syncthreads();
         if (nbat > 0) issue(0);
-        if (tid < 8 && nbat > 1) make_meta(1, tid, meta[1], cur);
+        if (tid < NC && nbat > 1) make_meta(1, tid, meta[1], cur);
         cp_async_wait_all();
         __syncthreads();
         if (nbat > 0) phase_in(0);
-        if (nbat > 1) issue(1);
         __syncthreads();
 
         for (int b = 0; b < nbat; ++b) {
-            const MmaMeta& M = meta[b % 3];
+            const Meta& M = meta[b % 3];
             const double* ipw = a.ipow + (int64_t(lt) * 28 + M.dsq) * a.ipow_w;
             const double* rfc = rf + int64_t(M.cls) * NF * 4 * 32 + lane;
+            // tile b + 1's moments: the staging buffer is free since phase_in(b)
+            if (b + 1 < nbat) issue(b + 1);
             // ---- rotation: jobs (n, rt), largest orders first, round robin over warps
             static_for<0, P + 1>([&](auto nn) {
                 constexpr int n = P - decltype(nn)::value;
                 constexpr int KC = mma_kc(n), base = n * (n + 1) / 2;
                 static_for<0, mma_rt(n)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
-                    if ((rot_job0(P, n) + rt) % 8 != warp) return;
+                    if ((rot_job0(P, n) + rt) % NW != warp) return;
                     const double* fr = rfc + (mma_foff(n) + rt * KC) * 4 * 32;
                     double aP[KC], aQ[KC];
 #pragma unroll
@@ -1113,20 +1123,25 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                         aP[kc] = __ldg(fr + (kc * 4 + 0) * 32);
                         aQ[kc] = __ldg(fr + (kc * 4 + 1) * 32);
                     }
-                    double r0 = 0, r1 = 0, i0 = 0, i1 = 0;
+                    double r0[NS] = {}, r1[NS] = {}, i0[NS] = {}, i1[NS] = {};
 #pragma unroll
-                    for (int kc = 0; kc < KC; ++kc) {
-                        mma884(r0, r1, aP[kc], Xre[bofs + base + 4 * kc]);
-                        mma884(i0, i1, aQ[kc], Xim[bofs + base + 4 * kc]);
-                    }
+                    for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) {
+                            mma884(r0[q], r1[q], aP[kc], Xre[bofs + q * 8 * LD + base + 4 * kc]);
+                            mma884(i0[q], i1[q], aQ[kc], Xim[bofs + q * 8 * LD + base + 4 * kc]);
+                        }
                     const int m = 8 * rt + lr;
                     if (m <= n) {
                         const double sc = n ? ipw[n - 1] : 1.0;
                         const int u = az_off(P, m) + (n - m);
-                        Wre[d0 + u] = r0 * sc;
-                        Wre[d1 + u] = r1 * sc;
-                        Wim[d0 + u] = i0 * sc;
-                        Wim[d1 + u] = i1 * sc;
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) {
+                            Wre[d0 + q * 8 * LD + u] = r0[q] * sc;
+                            Wre[d1 + q * 8 * LD + u] = r1[q] * sc;
+                            Wim[d0 + q * 8 * LD + u] = i0[q] * sc;
+                            Wim[d1 + q * 8 * LD + u] = i1[q] * sc;
+                        }
                     }
                 });
             });
@@ -1137,51 +1152,65 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                 constexpr int KC = tz_kc(P, k), u0 = az_off(P, k);
                 static_for<0, tz_rt(P, k)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
-                    if ((tz_job0(P, k) + rt) % 8 != warp) return;
+                    if ((tz_job0(P, k) + rt) % NW != warp) return;
                     const double* fz = a.tzfrag + (tz_foff(P, k) + rt * KC) * 32 + lane;
                     double az[KC > 0 ? KC : 1];
 #pragma unroll
                     for (int kc = 0; kc < KC; ++kc) az[kc] = __ldg(fz + kc * 32);
-                    double r0 = 0, r1 = 0, i0 = 0, i1 = 0;
+                    double r0[NS] = {}, r1[NS] = {}, i0[NS] = {}, i1[NS] = {};
 #pragma unroll
-                    for (int kc = 0; kc < KC; ++kc) {
-                        mma884(r0, r1, az[kc], Wre[bofs + u0 + 4 * kc]);
-                        mma884(i0, i1, az[kc], Wim[bofs + u0 + 4 * kc]);
-                    }
+                    for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) {
+                            mma884(r0[q], r1[q], az[kc], Wre[bofs + q * 8 * LD + u0 + 4 * kc]);
+                            mma884(i0[q], i1[q], az[kc], Wim[bofs + q * 8 * LD + u0 + 4 * kc]);
+                        }
                     const int j = k + 8 * rt + lr;
                     if (j <= P + 1) {
                         const double sc = ipw[j];
                         const int t1 = j * (j + 1) / 2 + k;
-                        Bre[e0 + t1] = r0 * sc;
-                        Bre[e1 + t1] = r1 * sc;
-                        Bim[e0 + t1] = i0 * sc;
-                        Bim[e1 + t1] = i1 * sc;
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) {
+                            Bre[e0 + q * 8 * LD1 + t1] = r0[q] * sc;
+                            Bre[e1 + q * 8 * LD1 + t1] = r1[q] * sc;
+                            Bim[e0 + q * 8 * LD1 + t1] = i0[q] * sc;
+                            Bim[e1 + q * 8 * LD1 + t1] = i1[q] * sc;
+                        }
                         if constexpr (k <= P) {
                             if (j <= P) {
                                 const double tl = a.tzl[k * (P + 2) + j];
                                 constexpr int up = u0 + (P - k);          // n' = p
-                                Are[d0 + t1] = fma(tl, Wre[d0 + up], r0) * sc;
-                                Are[d1 + t1] = fma(tl, Wre[d1 + up], r1) * sc;
-                                Aim[d0 + t1] = fma(tl, Wim[d0 + up], i0) * sc;
-                                Aim[d1 + t1] = fma(tl, Wim[d1 + up], i1) * sc;
+#pragma unroll
+                                for (int q = 0; q < NS; ++q) {
+                                    const int o0 = d0 + q * 8 * LD, o1 = d1 + q * 8 * LD;
+                                    Are[o0 + t1] = fma(tl, Wre[o0 + up], r0[q]) * sc;
+                                    Are[o1 + t1] = fma(tl, Wre[o1 + up], r1[q]) * sc;
+                                    Aim[o0 + t1] = fma(tl, Wim[o0 + up], i0[q]) * sc;
+                                    Aim[o1 + t1] = fma(tl, Wim[o1 + up], i1[q]) * sc;
+                                }
                             }
                         }
                     }
                 });
             });
             // column table of tile b + 2 (its ring slot is free)
-            if (tid < 8 && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
+            if (tid < NC && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
             __syncthreads();
             // ---- inverse rotation + phase, in place: one warp per order j (all its rows)
             {
-                const int pc0 = M.pidx[2 * lc] * (P + 2), pc1 = M.pidx[2 * lc + 1] * (P + 2);
+                int pc0[NS], pc1[NS];
+#pragma unroll
+                for (int q = 0; q < NS; ++q) {
+                    pc0[q] = M.pidx[8 * q + 2 * lc] * (P + 2);
+                    pc1[q] = M.pidx[8 * q + 2 * lc + 1] * (P + 2);
+                }
                 static_for<0, P + 2>([&](auto jj) {
                     constexpr int j = P + 1 - decltype(jj)::value;
-                    if (decltype(jj)::value % 8 != warp) return;
+                    if (decltype(jj)::value % NW != warp) return;
                     constexpr int KC = mma_kc(j), RT = mma_rt(j), base = j * (j + 1) / 2;
                     constexpr bool hasA = j <= P;
                     const double* fr = rfc + mma_foff(j) * 4 * 32;
-                    double ar[RT][2] = {}, ai[RT][2] = {}, br[RT][2] = {}, bi[RT][2] = {};
+                    double ar[RT][NS][2] = {}, ai[RT][NS][2] = {}, br[RT][NS][2] = {}, bi[RT][NS][2] = {};
 #pragma unroll
                     for (int rt = 0; rt < RT; ++rt) {
                         double aPB[KC], aQB[KC];
@@ -1191,14 +1220,16 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                             aQB[kc] = __ldg(fr + ((rt * KC + kc) * 4 + 3) * 32);
                         }
 #pragma unroll
-                        for (int kc = 0; kc < KC; ++kc) {
-                            mma884(br[rt][0], br[rt][1], aPB[kc], Bre[bofs1 + base + 4 * kc]);
-                            mma884(bi[rt][0], bi[rt][1], aQB[kc], Bim[bofs1 + base + 4 * kc]);
-                            if constexpr (hasA) {
-                                mma884(ar[rt][0], ar[rt][1], aPB[kc], Are[bofs + base + 4 * kc]);
-                                mma884(ai[rt][0], ai[rt][1], aQB[kc], Aim[bofs + base + 4 * kc]);
+                        for (int kc = 0; kc < KC; ++kc)
+#pragma unroll
+                            for (int q = 0; q < NS; ++q) {
+                                mma884(br[rt][q][0], br[rt][q][1], aPB[kc], Bre[bofs1 + q * 8 * LD1 + base + 4 * kc]);
+                                mma884(bi[rt][q][0], bi[rt][q][1], aQB[kc], Bim[bofs1 + q * 8 * LD1 + base + 4 * kc]);
+                                if constexpr (hasA) {
+                                    mma884(ar[rt][q][0], ar[rt][q][1], aPB[kc], Are[bofs + q * 8 * LD + base + 4 * kc]);
+                                    mma884(ai[rt][q][0], ai[rt][q][1], aQB[kc], Aim[bofs + q * 8 * LD + base + 4 * kc]);
+                                }
                             }
-                        }
                     }
                     __syncwarp();
 #pragma unroll
@@ -1206,17 +1237,22 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                         const int m = 8 * rt + lr;
                         if (m > j) continue;
                         const int t = base + m;
-                        const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0 + m);
-                        const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1 + m);
-                        Bre[e0 + t] = f0.x * br[rt][0] + f0.y * bi[rt][0];
-                        Bim[e0 + t] = f0.x * bi[rt][0] - f0.y * br[rt][0];
-                        Bre[e1 + t] = f1.x * br[rt][1] + f1.y * bi[rt][1];
-                        Bim[e1 + t] = f1.x * bi[rt][1] - f1.y * br[rt][1];
-                        if constexpr (hasA) {
-                            Are[d0 + t] = f0.x * ar[rt][0] + f0.y * ai[rt][0];
-                            Aim[d0 + t] = f0.x * ai[rt][0] - f0.y * ar[rt][0];
-                            Are[d1 + t] = f1.x * ar[rt][1] + f1.y * ai[rt][1];
-                            Aim[d1 + t] = f1.x * ai[rt][1] - f1.y * ar[rt][1];
+#pragma unroll
+                        for (int q = 0; q < NS; ++q) {
+                            const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0[q] + m);
+                            const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1[q] + m);
+                            const int b0 = e0 + q * 8 * LD1 + t, b1 = e1 + q * 8 * LD1 + t;
+                            Bre[b0] = f0.x * br[rt][q][0] + f0.y * bi[rt][q][0];
+                            Bim[b0] = f0.x * bi[rt][q][0] - f0.y * br[rt][q][0];
+                            Bre[b1] = f1.x * br[rt][q][1] + f1.y * bi[rt][q][1];
+                            Bim[b1] = f1.x * bi[rt][q][1] - f1.y * br[rt][q][1];
+                            if constexpr (hasA) {
+                                const int a0 = d0 + q * 8 * LD + t, a1 = d1 + q * 8 * LD + t;
+                                Are[a0] = f0.x * ar[rt][q][0] + f0.y * ai[rt][q][0];
+                                Aim[a0] = f0.x * ai[rt][q][0] - f0.y * ar[rt][q][0];
+                                Are[a1] = f1.x * ar[rt][q][1] + f1.y * ai[rt][q][1];
+                                Aim[a1] = f1.x * ai[rt][q][1] - f1.y * ar[rt][q][1];
+                            }
                         }
                     }
                 });
@@ -1226,9 +1262,9 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
             // ---- accumulate tile b into the targets (column order); phase tile b + 1 in
             {
                 const int ncol = M.ncol;
-                int sb[8];
+                int sb[NC];
 #pragma unroll
-                for (int c = 0; c < 8; ++c) sb[c] = M.sb[c];
+                for (int c = 0; c < NC; ++c) sb[c] = M.sb[c];
                 for (int t = tid; t < T + T1; t += NT) {
                     const bool isA = t < T;
                     const int r = isA ? t : t - T;
@@ -1238,7 +1274,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                     cplx* acc = isA ? accA + r : accB + r;
                     const int stride = isA ? T : T1;
 #pragma unroll
-                    for (int c = 0; c < 8; ++c)
+                    for (int c = 0; c < NC; ++c)
                         if (c < ncol) {
                             cplx& d = acc[sb[c] * stride];
                             d.re += sre[c * ld];
@@ -1246,7 +1282,6 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
                         }
                 }
                 if (b + 1 < nbat) phase_in(b + 1);
-                if (b + 2 < nbat) issue(b + 2);
             }
             __syncthreads();
         }
@@ -1258,20 +1293,20 @@ __global__ void __launch_bounds__(256, 2) k_m2l_mma(EvalArgs a, int64_t g0, int6
     }
 }
 
-template<int P>
+template<int P, int NS, int NW>
 bool try_launch_mma(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
-    const size_t smem = MmaLayout<P>::total(a.qdim);
+    const size_t smem = MmaLayout<P, NS>::total(a.qdim);
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    allow_max_smem(k_m2l_mma<P>);
+    allow_max_smem(k_m2l_mma<P, NS, NW>);
     int per_sm = 0;
-    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P>, 256, smem));
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P, NS, NW>, 32 * NW, smem));
     if (per_sm < 1) return false;
     const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
-    k_m2l_mma<P><<<static_cast<unsigned>(grid), 256, smem, st>>>(a, g0, g1);
+    k_m2l_mma<P, NS, NW><<<static_cast<unsigned>(grid), 32 * NW, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
     return true;
 }
@@ -1871,7 +1906,7 @@ void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream
 {
     if constexpr (P >= 2) {
         if (a.mixed && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
-        if (try_launch_mma<P>(a, g0, g1, sms, st)) return;
+        if (try_launch_mma<P, 1, 8>(a, g0, g1, sms, st)) return;
     }
     if constexpr (P >= 2 && P <= 12) {
         // two blocks per SM of 4-column batches measured fastest up to p = 10
