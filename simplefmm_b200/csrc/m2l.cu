@@ -1393,8 +1393,13 @@ __host__ __device__ constexpr int tf_zjob0(int P, int k)
     for (int i = 0; i < k; ++i) s += tf_zrt(P, i);
     return s;
 }
-// column stride of an FP32 operand buffer: >= rows + 8, = 4 mod 32 (conflict-free fragments)
-__host__ __device__ constexpr int tf_ld(int rows) { return ((rows + 8 + 27) / 32) * 32 + 4; }
+// column stride of an FP32 operand buffer: >= rows + 8, = 4 mod 8 (conflict-free fragments)
+__host__ __device__ constexpr int tf_ld(int rows)
+{
+    int ld = rows + 8;
+    while (ld % 8 != 4) ++ld;
+    return ld;
+}
 // |d|^2 of a rotation class (class = 7 t2i + dk + 3, fmm.hpp:171)
 __host__ __device__ inline int class_dsq(int c)
 {
@@ -1424,17 +1429,13 @@ struct FragA {
     unsigned h[4], l[4];
 };
 
-__device__ __forceinline__ FragA split_a(const float4 v)
+
+// A fragment stored pre-split: p[0] the TF32 high parts, p[32] the low parts
+__device__ __forceinline__ FragA load_a(const float4* p)
 {
-    FragA f;
-    const float e[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const Tf32x2 s = split_tf32(e[i]);
-        f.h[i] = s.h;
-        f.l[i] = s.l;
-    }
-    return f;
+    const float4 h = __ldg(p), l = __ldg(p + 32);
+    return FragA{{__float_as_uint(h.x), __float_as_uint(h.y), __float_as_uint(h.z), __float_as_uint(h.w)},
+                 {__float_as_uint(l.x), __float_as_uint(l.y), __float_as_uint(l.z), __float_as_uint(l.w)}};
 }
 
 __device__ __forceinline__ void mma1688(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1)
@@ -1458,9 +1459,8 @@ struct MixLayout {
     static constexpr int T = (P + 1) * (P + 2) / 2;
     static constexpr int T1 = (P + 2) * (P + 3) / 2;
     static constexpr int LD = tf_ld(T), LD1 = tf_ld(T1);          // column strides (floats)
-    static constexpr int ent_src = 0;
-    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
-    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
+    static constexpr int kids = 0;                                 // ilist offsets of the 8 children
+    static constexpr int sorted = al16(kids + 4 * 9);
     static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
     static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
     static constexpr int cls_off = al16(cls_cnt + 4 * 72);
@@ -1470,8 +1470,8 @@ struct MixLayout {
     static constexpr int tn = al16(tm + T1);                       // order n of coefficient t
     static constexpr int offs = al16(tn + T1);                     // fragment offsets: foff[P+3], zoff[P+3]
     static constexpr int spow = al16(offs + 8 * (P + 3));          // s^-k, k = 0..P+2 (doubles)
-    static constexpr int Xraw = al16(spow + 8 * (P + 3));          // 2 x [col][T] complex (cp.async)
-    static constexpr int X = al16(Xraw + 2 * 8 * T * 16);          // re, im: [col][LD] floats each
+    static constexpr int Xraw = al16(spow + 8 * (P + 3));          // [col][T] complex (cp.async)
+    static constexpr int X = al16(Xraw + 8 * T * 16);              // re, im: [col][LD] floats each
     static constexpr int W = al16(X + 2 * 8 * LD * 4);
     static constexpr int LzA = al16(W + 2 * 8 * LD * 4);
     static constexpr int LzB = al16(LzA + 2 * 8 * LD * 4);         // [col][LD1]
@@ -1480,13 +1480,12 @@ struct MixLayout {
 };
 
 template<int P>
-__global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int64_t g1)
+__global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int64_t g1)
 {
     using L = MixLayout<P>;
     constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 256;
     extern __shared__ __align__(16) unsigned char sm[];
-    int* ent_src = reinterpret_cast<int*>(sm + L::ent_src);
-    int* ent_code = reinterpret_cast<int*>(sm + L::ent_code);
+    int* kids = reinterpret_cast<int*>(sm + L::kids);
     short* sorted = reinterpret_cast<short*>(sm + L::sorted);
     unsigned char* cls = sm + L::cls;
     int* cls_cnt = reinterpret_cast<int*>(sm + L::cls_cnt);
@@ -1539,12 +1538,14 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
             const int col = col0 + k;
             const int pair = col / qd;
             const int e = sorted[cls_off[c] + pair];
-            const int code = ent_code[e];
+            const int code = a.il_code[kids[0] + e];
             const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
             const int bq = col - pair * qd;
-            M.src[k] = ent_src[e];
+            int slot = 0;
+            while (kids[slot + 1] - kids[0] <= e) ++slot;
+            M.src[k] = a.il_src[kids[0] + e];
             M.bq[k] = bq;
-            M.sb[k] = ((code >> 9) & 7) * qd + bq;
+            M.sb[k] = slot * qd + bq;
             M.pidx[k] = 7 * (dj + 3) + (di + 3);
             if (k == 0) {
                 M.cls = c;
@@ -1561,7 +1562,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
     auto issue = [&](int b) {
         const MmaMeta& M = meta[b % 3];
         const int ncol = M.ncol;
-        cplx* xr = Xraw + (b & 1) * 8 * T;
+        cplx* xr = Xraw;
         for (int e = tid; e < 8 * T; e += NT) {
             const int c = e / T, t = e - c * T;
             if (c < ncol) cp_async16(xr + e, a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
@@ -1572,7 +1573,7 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
     auto phase_in = [&](int b) {
         const MmaMeta& M = meta[b % 3];
         const int ncol = M.ncol;
-        const cplx* xr = Xraw + (b & 1) * 8 * T;
+        const cplx* xr = Xraw;
         for (int e = tid; e < 8 * T; e += NT) {
             const int c = e / T, t = e - c * T;
             if (c < ncol) {
@@ -1592,16 +1593,11 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
         const int lt = level_of(a, g) + 1;
         {
             const int e0 = a.il_ptr[cb], E = a.il_ptr[cb + nc] - e0;
-            for (int s = 0; s < nc; ++s) {
-                const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
-                for (int e = q0 + tid; e < q1; e += NT) {
-                    const int code = a.il_code[e0 + e];
-                    ent_src[e] = a.il_src[e0 + e];
-                    ent_code[e] = code | (s << 9);
-                    cls[e] = static_cast<unsigned char>(
-                        rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
-                }
+            for (int e = tid; e < E; e += NT) {
+                const int code = a.il_code[e0 + e];
+                cls[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
             }
+            if (tid <= 8) kids[tid] = a.il_ptr[cb + min(tid, nc)];
             for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = cplx{0, 0};
             if (tid == 0) {
                 // s^-k for the box size s of the targets' (= sources') level
@@ -1647,14 +1643,15 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
         cp_async_wait_all();
         __syncthreads();
         if (nbat > 0) phase_in(0);
-        if (nbat > 1) issue(1);
         __syncthreads();
 
         for (int b = 0; b < nbat; ++b) {
             const MmaMeta& M = meta[b % 3];
-            const float4* rfc = rf + int64_t(M.cls) * NF * 4 * 32 + lane;
-            const float4* tzc = tzf + int64_t(M.cls) * NFZ * 32 + lane;
+            const float4* rfc = rf + int64_t(M.cls) * NF * 4 * 64 + lane;
+            const float4* tzc = tzf + int64_t(M.cls) * NFZ * 64 + lane;
             const float* tlc = a.tzl32 + M.cls * (P + 1) * (P + 2);
+            // tile b + 1's moments: the staging buffer is free since phase_in(b)
+            if (b + 1 < nbat) issue(b + 1);
             // ---- rotation: jobs (n, rt), largest orders first, round robin over
             // warps; one copy of the job body (runtime n) keeps the code small
             {
@@ -1665,12 +1662,12 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
 #pragma unroll 1
                     for (int rt = 0; rt < RT; ++rt, ++job) {
                         if ((job & 7) != warp) continue;
-                        const float4* fr = rfc + (foff[n] + rt * KC) * 4 * 32;
+                        const float4* fr = rfc + (foff[n] + rt * KC) * 4 * 64;
                         float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
 #pragma unroll 1
                         for (int kc = 0; kc < KC; ++kc) {
-                            const FragA aP = split_a(__ldg(fr + (kc * 4 + 0) * 32));
-                            const FragA aQ = split_a(__ldg(fr + (kc * 4 + 1) * 32));
+                            const FragA aP = load_a(fr + (kc * 4 + 0) * 64);
+                            const FragA aQ = load_a(fr + (kc * 4 + 1) * 64);
                             const int ro = bofs + base + 8 * kc;
                             mma3x(r, aP, Xre[ro], Xre[ro + 4]);
                             mma3x(im, aQ, Xim[ro], Xim[ro + 4]);
@@ -1699,11 +1696,11 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
 #pragma unroll 1
                     for (int rt = 0; rt < RT; ++rt, ++job) {
                         if ((job & 7) != warp) continue;
-                        const float4* fz = tzc + (zoff[k] + rt * KC) * 32;
+                        const float4* fz = tzc + (zoff[k] + rt * KC) * 64;
                         float r[4] = {0, 0, 0, 0}, im[4] = {0, 0, 0, 0};
 #pragma unroll 1
                         for (int kc = 0; kc < KC; ++kc) {
-                            const FragA az = split_a(__ldg(fz + kc * 32));
+                            const FragA az = load_a(fz + kc * 64);
                             const int ro = bofs + u0 + 8 * kc;
                             mma3x(r, az, Wre[ro], Wre[ro + 4]);
                             mma3x(im, az, Wim[ro], Wim[ro + 4]);
@@ -1740,15 +1737,15 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
                 for (int j = P + 1 - warp; j >= 0; j -= 8) {
                     const int KC = tf_kc(j), RT = tf_rt(j), base = j * (j + 1) / 2;
                     const bool hasA = j <= P;
-                    const float4* fr = rfc + foff[j] * 4 * 32;
+                    const float4* fr = rfc + foff[j] * 4 * 64;
                     float ar[RTM][4] = {}, ai[RTM][4] = {}, br[RTM][4] = {}, bi[RTM][4] = {};
 #pragma unroll
                     for (int rt = 0; rt < RTM; ++rt) {
                         if (rt >= RT) break;
 #pragma unroll 1
                         for (int kc = 0; kc < KC; ++kc) {
-                            const FragA aPB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 2) * 32));
-                            const FragA aQB = split_a(__ldg(fr + ((rt * KC + kc) * 4 + 3) * 32));
+                            const FragA aPB = load_a(fr + ((rt * KC + kc) * 4 + 2) * 64);
+                            const FragA aQB = load_a(fr + ((rt * KC + kc) * 4 + 3) * 64);
                             const int ro1 = bofs1 + base + 8 * kc;
                             mma3x(br[rt], aPB, Bre[ro1], Bre[ro1 + 4]);
                             mma3x(bi[rt], aQB, Bim[ro1], Bim[ro1 + 4]);
@@ -1812,7 +1809,6 @@ __global__ void __launch_bounds__(256, 2) k_m2l_tf32(EvalArgs a, int64_t g0, int
                         }
                 }
                 if (b + 1 < nbat) phase_in(b + 1);
-                if (b + 2 < nbat) issue(b + 2);
             }
             __syncthreads();
         }
@@ -1864,7 +1860,14 @@ __global__ void k_frag_rot32(const double* __restrict__ rot, const int* __restri
                        ? static_cast<float>(rot[int64_t(c) * rot_len + rot_off[n] + mat * (n + 1) * (n + 1) + row * (n + 1) + col])
                        : 0.f;
         }
-        out[idx] = make_float4(v[0], v[1], v[2], v[3]);
+        float h[4], l[4];
+        for (int q = 0; q < 4; ++q) {
+            h[q] = __uint_as_float(to_tf32(v[q]));
+            l[q] = __uint_as_float(to_tf32(v[q] - h[q]));
+        }
+        const int64_t o = (idx >> 5) * 64 + lane;       // [fragment][hi, lo][lane]
+        out[o] = make_float4(h[0], h[1], h[2], h[3]);
+        out[o + 32] = make_float4(l[0], l[1], l[2], l[3]);
     }
 }
 
@@ -1888,7 +1891,14 @@ __global__ void k_frag_tz32(const double* __restrict__ tzx, const int* __restric
                        ? static_cast<float>(tzx[tzx_off[k] + (j - k) * (P + 1 - k) + (np - k)] * pow(rho, -(j + np + 1)))
                        : 0.f;
         }
-        out[idx] = make_float4(v[0], v[1], v[2], v[3]);
+        float h[4], l[4];
+        for (int q = 0; q < 4; ++q) {
+            h[q] = __uint_as_float(to_tf32(v[q]));
+            l[q] = __uint_as_float(to_tf32(v[q] - h[q]));
+        }
+        const int64_t o = (idx >> 5) * 64 + lane;
+        out[o] = make_float4(h[0], h[1], h[2], h[3]);
+        out[o + 32] = make_float4(l[0], l[1], l[2], l[3]);
     }
     const int ntl = kNumClasses * (P + 1) * (P + 2);
     for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < ntl; idx += gridDim.x * blockDim.x) {
@@ -1938,8 +1948,8 @@ void build_m2l_fragments(Plan& pl, cudaStream_t st)
     if (pl.precision == FMM_PRECISION_MIXED) {
         pl.rf32_nf = tf_foff(P + 2);
         pl.tz32_nf = std::max(tf_zoff(P, P + 2), 1);
-        pl.rf32.alloc(size_t(kNumClasses) * pl.rf32_nf * 4 * 32 * 4, st);
-        pl.tz32.alloc(size_t(kNumClasses) * pl.tz32_nf * 32 * 4, st);
+        pl.rf32.alloc(size_t(kNumClasses) * pl.rf32_nf * 4 * 64 * 4, st);     // float4, high and low parts
+        pl.tz32.alloc(size_t(kNumClasses) * pl.tz32_nf * 64 * 4, st);
         pl.tzl32.alloc(size_t(kNumClasses) * (P + 1) * (P + 2), st);
         k_frag_rot32<<<256, 256, 0, st>>>(pl.rot.ptr, pl.rot_off.ptr, pl.rot_len, P, pl.rf32_nf,
                                           reinterpret_cast<float4*>(pl.rf32.ptr));
