@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                     }
                 }
                 __syncwarp();
+#pragma unroll 2
                 for (int k = s; k < fill; k += slices) {
                     const double2 xy = sxy[k], zq = szq[k];
                     double2 qq = make_double2(0, 0);
@@ -336,14 +337,15 @@ void launch_fp64(const EvalArgs& a, int sms, cudaStream_t st)
     SFMM_CHECK_LAUNCH();
 }
 
-// Measured on 4M Plummer points, p = 10 (kChunk 128): FP64 with 4 passes and
-// two blocks per SM (128 registers) 58.9 ms; 3 passes / 3 blocks 77.1 ms and
-// 2 passes / 4 blocks 83.4 ms (both spill).  FP32 with 4 passes and one block
-// per SM 45.1 ms; two blocks (spilling) 49.8 ms.
+// Measured (kChunk 128): FP64 on 4M Plummer points, p = 10: 4 passes and two
+// blocks per SM (128 registers) 58.9 ms; 3 passes / 3 blocks 77.1 ms and
+// 2 passes / 4 blocks 83.4 ms (both spill).  FP32, 4M Plummer / 16M uniform:
+// 4 passes, one block per SM 45.2 / 74.5 ms; 3 passes, two blocks 52.5 / 48.9 ms;
+// 2 passes, two blocks 52.7 / 51.1 ms; 2 passes, three blocks 69.7 / 46.2 ms.
 template<int QD, bool POT, bool FLD>
 void launch(const EvalArgs& a, int sms, cudaStream_t st)
 {
-    if (a.mixed) return launch_mixed<QD, POT, FLD, 4, 1>(a, sms, st);
+    if (a.mixed) return launch_mixed<QD, POT, FLD, 3, 2>(a, sms, st);
     return launch_fp64<QD, POT, FLD, 4, 2>(a, sms, st);
 }
 
