@@ -144,6 +144,16 @@ int fmm_rinv(fmm_plan* plan, const double* Q, double* U, int gradient, int where
    formulation of fmm.hpp:234-253 and 549-551. */
 int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, int where);
 
+/* Capture one evaluation of device arrays Q / pot / field (what fmm_evaluate
+   with FMM_DEVICE does) as a CUDA graph, and launch it again on the context's
+   stream with fmm_plan_replay -- for callers that evaluate the same tree
+   repeatedly with new charges written into Q (no counterpart in the
+   reference).  Capturing computes nothing; each replay computes and, like
+   fmm_evaluate, accumulates into pot / field.  Needs a context on its own
+   stream (not a default stream). */
+int fmm_plan_capture(fmm_plan* plan, const double* Q, double* pot, double* field);
+int fmm_plan_replay(fmm_plan* plan);
+
 /* Device time (ms) of each phase of the last evaluation: [0] P2M+M2M,
    [1] M2L, [2] L2L+L2P, [3] P2P, [4] total; and of the last tree build [5]. */
 int fmm_plan_timings(const fmm_plan* plan, double* ms6);

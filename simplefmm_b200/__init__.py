@@ -62,6 +62,8 @@ def load_library():
         "fmm_tree_destroy": ([vp], i32),
         "fmm_tree_build_box": ([vp, vp, i64, i32, C.POINTER(dbl), dbl, i32, i32, i32, dbl, C.POINTER(vp)], i32),
         "fmm_plan_set_exclusions": ([vp, vp, vp, i32, i32], i32),
+        "fmm_plan_capture": ([vp, vp, vp, vp], i32),
+        "fmm_plan_replay": ([vp], i32),
         "fmm_tree_depth": ([vp, C.POINTER(i32)], i32),
         "fmm_tree_box": ([vp, C.POINTER(dbl), C.POINTER(dbl)], i32),
         "fmm_tree_export_size": ([vp, i32, i32, C.POINTER(i64)], i32),
@@ -289,6 +291,20 @@ class Plan:
         cl = np.ascontiguousarray(cols, dtype=np.int32)
         _check(L.fmm_plan_set_exclusions(self._h, C.c_void_p(rp.ctypes.data), C.c_void_p(cl.ctypes.data), HOST,
                                          int(bool(near_too))))
+
+    def capture(self, Q, pot=None, field=None):
+        """Capture evaluate(Q, pot, field) on device arrays as a CUDA graph (see replay)."""
+        ptrs = []
+        for arr in (Q, pot, field):
+            addr, where = _ptr(arr)
+            if arr is not None and where != DEVICE:
+                raise FMMError(1, "capture takes device arrays")
+            ptrs.append(C.c_void_p(addr) if arr is not None else None)
+        _check(load_library().fmm_plan_capture(self._h, *ptrs))
+
+    def replay(self):
+        """Launch the captured evaluation again (asynchronous on the context's stream)."""
+        _check(load_library().fmm_plan_replay(self._h))
 
     def timings(self) -> dict:
         t = (C.c_double * 6)()

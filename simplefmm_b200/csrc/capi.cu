@@ -346,9 +346,56 @@ int fmm_plan_destroy(fmm_plan* plan)
     SFMM_CUDA(cudaStreamSynchronize(plan->pl.tree->ctx->stream));
     for (auto& e : plan->pl.ev)
         if (e) cudaEventDestroy(e);
+    if (plan->pl.graph_exec) cudaGraphExecDestroy(plan->pl.graph_exec);
+    if (plan->pl.graph) cudaGraphDestroy(plan->pl.graph);
     fmm_tree* owner = plan->owner;
     delete plan;
     release_tree(owner);
+    API_CATCH
+}
+
+int fmm_plan_capture(fmm_plan* plan, const double* Q, double* pot, double* field)
+{
+    API_TRY
+    if (!plan || !Q) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    if (!pot && !field) return fail(FMM_ERR_INVALID_ARGUMENT, "nothing to evaluate");
+    sfmm::Plan& pl = plan->pl;
+    if (field && pl.qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs N = 1 or N = 3 charges");
+    sfmm::Context& c = *pl.tree->ctx;
+    bind(c);
+    if (c.stream == nullptr || c.stream == cudaStreamLegacy || c.stream == cudaStreamPerThread)
+        return fail(FMM_ERR_UNSUPPORTED, "capture needs the context's own stream, not a default stream");
+    SFMM_CUDA(cudaStreamSynchronize(c.stream));
+    if (pl.graph_exec) {
+        cudaGraphExecDestroy(pl.graph_exec);
+        pl.graph_exec = nullptr;
+    }
+    if (pl.graph) {
+        cudaGraphDestroy(pl.graph);
+        pl.graph = nullptr;
+    }
+    SFMM_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        sfmm::plan_evaluate(pl, Q, pot, field);
+    } catch (...) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(c.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    SFMM_CUDA(cudaStreamEndCapture(c.stream, &pl.graph));
+    SFMM_CUDA(cudaGraphInstantiate(&pl.graph_exec, pl.graph, 0));
+    API_CATCH
+}
+
+int fmm_plan_replay(fmm_plan* plan)
+{
+    API_TRY
+    if (!plan) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL plan");
+    sfmm::Plan& pl = plan->pl;
+    if (!pl.graph_exec) return fail(FMM_ERR_INVALID_ARGUMENT, "nothing captured (fmm_plan_capture)");
+    bind(*pl.tree->ctx);
+    SFMM_CUDA(cudaGraphLaunch(pl.graph_exec, pl.tree->ctx->stream));
     API_CATCH
 }
 

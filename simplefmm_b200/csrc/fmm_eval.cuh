@@ -91,6 +91,9 @@ struct Plan {
     DevBuf<double> qs, out, out2;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
     cudaEvent_t ev[6] = {};
+    // one captured evaluation (fmm_plan_capture / fmm_plan_replay)
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
 };
 
 void plan_init(Plan& pl);

@@ -189,3 +189,30 @@ def test_handles_destroyed_in_any_order(order):
     for name in order.split("-")[1:]:
         fn, h = handles[name]
         assert fn(h) == 0
+
+
+def test_captured_evaluation_replays_like_evaluate():
+    """fmm_plan_capture / fmm_plan_replay: the graph of one evaluation, replayed
+    with new charges written into the captured array, gives what evaluate gives."""
+    torch = pytest.importorskip("torch")
+    ctx = sf.Context(0)                                 # its own stream: capturable
+    n = 50_000
+    pos = W.points("plummer", n, 31)
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    plan = sf.Plan(t, 8, 1)
+    q_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    pot_d = torch.zeros(n, dtype=torch.float64, device="cuda")
+    fld_d = torch.zeros(n, 3, dtype=torch.float64, device="cuda")
+    plan.capture(q_d, pot_d, fld_d)
+    for seed in (32, 33):
+        q = W.charges(n, seed)
+        q_d.copy_(torch.from_numpy(q))
+        pot_d.zero_()
+        fld_d.zero_()
+        torch.cuda.synchronize()
+        plan.replay()
+        ctx.synchronize()
+        pot, fld = np.zeros(n), np.zeros((n, 3))
+        plan.evaluate(q, pot, fld)
+        np.testing.assert_array_equal(pot_d.cpu().numpy(), pot)
+        np.testing.assert_array_equal(fld_d.cpu().numpy(), fld)
