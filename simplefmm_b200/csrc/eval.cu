@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <tuple>
 
 #include "eval_util.cuh"
 #include "fmm_tables.h"
@@ -294,34 +295,50 @@ static void upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s)
     if (!h.empty()) SFMM_CUDA(cudaMemcpyAsync(d.ptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s));
 }
 
+// Device operator tables per (device, p, precision), shared by all plans.
+static std::shared_ptr<PlanTables> tables_on_device(int device, int p, bool mixed, cudaStream_t st)
+{
+    static std::mutex mu;
+    static auto* cache = new std::map<std::tuple<int, int, bool>, std::shared_ptr<PlanTables>>();   // kept until exit
+    std::lock_guard<std::mutex> lk(mu);
+    auto& slot = (*cache)[std::make_tuple(device, p, mixed)];
+    if (slot) return slot;
+    const auto tb = tables_for(p);
+    const auto tb1 = tables_for(p + 1);
+    auto t = std::make_shared<PlanTables>();
+    t->rot_len = tb1->rot_len;
+    t->tzx_len = static_cast<int>(tb->tzx.size());
+    upload(t->rot, tb1->rot, st);
+    upload(t->rot_off, tb1->rot_off, st);
+    upload(t->tzx, tb->tzx, st);
+    upload(t->tzx_off, tb->tzx_off, st);
+    upload(t->eil, tb1->eil, st);
+    upload(t->echild, tb->echild, st);
+    upload(t->eparent, tb->eparent, st);
+    upload(t->eparent1, tb1->eparent, st);
+    upload(t->m2m_ptr, tb->m2m_ptr, st);
+    upload(t->m2m_code, tb->m2m_code, st);
+    upload(t->m2m_g, tb->m2m_g, st);
+    upload(t->l2l_ptr, tb->l2l_ptr, st);
+    upload(t->l2l_code, tb->l2l_code, st);
+    upload(t->l2l_g, tb->l2l_g, st);
+    upload(t->l2l1_ptr, tb1->l2l_ptr, st);
+    upload(t->l2l1_code, tb1->l2l_code, st);
+    upload(t->l2l1_g, tb1->l2l_g, st);
+    build_m2l_fragments(*t, p, mixed, st);
+    SFMM_CUDA(cudaStreamSynchronize(st));         // other streams read it from now on
+    slot = t;
+    return t;
+}
+
 void plan_init(Plan& pl)
 {
     Tree& t = *pl.tree;
     cudaStream_t st = t.ctx->stream;
     upload_harm_coef(t.ctx->device);
-    const auto tb = tables_for(pl.p);
-    const auto tb1 = tables_for(pl.p + 1);
-    pl.T = tb->T;
-    pl.T1 = tb1->T;
-    pl.rot_len = tb1->rot_len;
-    pl.tzx_len = static_cast<int>(tb->tzx.size());
-    upload(pl.rot, tb1->rot, st);
-    upload(pl.rot_off, tb1->rot_off, st);
-    upload(pl.tzx, tb->tzx, st);
-    upload(pl.tzx_off, tb->tzx_off, st);
-    upload(pl.eil, tb1->eil, st);
-    upload(pl.echild, tb->echild, st);
-    upload(pl.eparent, tb->eparent, st);
-    upload(pl.eparent1, tb1->eparent, st);
-    upload(pl.m2m_ptr, tb->m2m_ptr, st);
-    upload(pl.m2m_code, tb->m2m_code, st);
-    upload(pl.m2m_g, tb->m2m_g, st);
-    upload(pl.l2l_ptr, tb->l2l_ptr, st);
-    upload(pl.l2l_code, tb->l2l_code, st);
-    upload(pl.l2l_g, tb->l2l_g, st);
-    upload(pl.l2l1_ptr, tb1->l2l_ptr, st);
-    upload(pl.l2l1_code, tb1->l2l_code, st);
-    upload(pl.l2l1_g, tb1->l2l_g, st);
+    pl.T = (pl.p + 1) * (pl.p + 2) / 2;
+    pl.T1 = (pl.p + 2) * (pl.p + 3) / 2;
+    pl.tab = tables_on_device(t.ctx->device, pl.p, pl.precision == FMM_PRECISION_MIXED, st);
     // rho^{-(k+1)} per (level, |d|^2), k = 0..2p+2, formed as fmm.hpp:629-633 does
     pl.ipow_w = 2 * pl.p + 3;
     std::vector<double> ipw(size_t(t.depth + 1) * 28 * pl.ipow_w, 0.0);
@@ -333,7 +350,6 @@ void plan_init(Plan& pl)
             for (int k = 0; k + 1 < pl.ipow_w; ++k) r[k + 1] = r[k] / rho;
         }
     upload(pl.ipow, ipw, st);
-    build_m2l_fragments(pl, st);
     pl.M.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LA.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
@@ -382,36 +398,36 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.mixed = pl.precision == FMM_PRECISION_MIXED;
     a.kf = a.want_pot ? pl.qdim : 0;
     a.K = a.kf + (a.want_field ? 3 : 0);
-    a.rot = pl.rot.ptr;
-    a.rot_off = pl.rot_off.ptr;
-    a.rot_len = pl.rot_len;
-    a.tzx = pl.tzx.ptr;
-    a.tzx_off = pl.tzx_off.ptr;
-    a.tzx_len = pl.tzx_len;
-    a.eil = reinterpret_cast<const cplx*>(pl.eil.ptr);
-    a.echild = reinterpret_cast<const cplx*>(pl.echild.ptr);
-    a.eparent = reinterpret_cast<const cplx*>(pl.eparent.ptr);
-    a.eparent1 = reinterpret_cast<const cplx*>(pl.eparent1.ptr);
-    a.m2m_ptr = pl.m2m_ptr.ptr;
-    a.m2m_code = pl.m2m_code.ptr;
-    a.m2m_g = pl.m2m_g.ptr;
-    a.l2l_ptr = pl.l2l_ptr.ptr;
-    a.l2l_code = pl.l2l_code.ptr;
-    a.l2l_g = pl.l2l_g.ptr;
-    a.l2l1_ptr = pl.l2l1_ptr.ptr;
-    a.l2l1_code = pl.l2l1_code.ptr;
-    a.l2l1_g = pl.l2l1_g.ptr;
+    a.rot = pl.tab->rot.ptr;
+    a.rot_off = pl.tab->rot_off.ptr;
+    a.rot_len = pl.tab->rot_len;
+    a.tzx = pl.tab->tzx.ptr;
+    a.tzx_off = pl.tab->tzx_off.ptr;
+    a.tzx_len = pl.tab->tzx_len;
+    a.eil = reinterpret_cast<const cplx*>(pl.tab->eil.ptr);
+    a.echild = reinterpret_cast<const cplx*>(pl.tab->echild.ptr);
+    a.eparent = reinterpret_cast<const cplx*>(pl.tab->eparent.ptr);
+    a.eparent1 = reinterpret_cast<const cplx*>(pl.tab->eparent1.ptr);
+    a.m2m_ptr = pl.tab->m2m_ptr.ptr;
+    a.m2m_code = pl.tab->m2m_code.ptr;
+    a.m2m_g = pl.tab->m2m_g.ptr;
+    a.l2l_ptr = pl.tab->l2l_ptr.ptr;
+    a.l2l_code = pl.tab->l2l_code.ptr;
+    a.l2l_g = pl.tab->l2l_g.ptr;
+    a.l2l1_ptr = pl.tab->l2l1_ptr.ptr;
+    a.l2l1_code = pl.tab->l2l1_code.ptr;
+    a.l2l1_g = pl.tab->l2l1_g.ptr;
     a.ipow = pl.ipow.ptr;
     a.ipow_w = pl.ipow_w;
-    a.rfrag = pl.rfrag.ptr;
-    a.rfrag_nf = pl.rfrag_nf;
-    a.tzfrag = pl.tzfrag.ptr;
-    a.tzl = pl.tzl.ptr;
-    a.rf32 = pl.rf32.ptr;
-    a.rf32_nf = pl.rf32_nf;
-    a.tz32 = pl.tz32.ptr;
-    a.tz32_nf = pl.tz32_nf;
-    a.tzl32 = pl.tzl32.ptr;
+    a.rfrag = pl.tab->rfrag.ptr;
+    a.rfrag_nf = pl.tab->rfrag_nf;
+    a.tzfrag = pl.tab->tzfrag.ptr;
+    a.tzl = pl.tab->tzl.ptr;
+    a.rf32 = pl.tab->rf32.ptr;
+    a.rf32_nf = pl.tab->rf32_nf;
+    a.tz32 = pl.tab->tz32.ptr;
+    a.tz32_nf = pl.tab->tz32_nf;
+    a.tzl32 = pl.tab->tzl32.ptr;
     a.M = reinterpret_cast<cplx*>(pl.M.ptr);
     a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
     a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);

@@ -3,6 +3,8 @@
 
 #include "fmm_internal.cuh"
 
+#include <memory>
+
 namespace sfmm {
 
 // Everything a kernel of one evaluation reads, passed by value.
@@ -71,22 +73,31 @@ struct EvalArgs {
     double* out2;                        // near field per component, sorted order
 };
 
-struct Plan {
-    Tree* tree = nullptr;
-    int p = 0, T = 0, T1 = 0, qdim = 1, precision = FMM_PRECISION_FP64;
-    int rot_len = 0, tzx_len = 0, ipow_w = 0;
-    DevBuf<double> rot, tzx, eil, echild, eparent, eparent1, m2m_g, l2l_g, l2l1_g, ipow;
+// Operator tables of one expansion order on one device: immutable once built,
+// shared by every plan of that (device, p, precision) (built once, on the
+// first plan's stream, then kept until the process exits).
+struct PlanTables {
+    int rot_len = 0, tzx_len = 0;
+    DevBuf<double> rot, tzx, eil, echild, eparent, eparent1, m2m_g, l2l_g, l2l1_g;
+    DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
     DevBuf<double> rfrag, tzfrag, tzl;
     int rfrag_nf = 0;
     DevBuf<float> rf32, tz32, tzl32;
     int rf32_nf = 0, tz32_nf = 0;
+};
+
+struct Plan {
+    Tree* tree = nullptr;
+    int p = 0, T = 0, T1 = 0, qdim = 1, precision = FMM_PRECISION_FP64;
+    int ipow_w = 0;
+    std::shared_ptr<PlanTables> tab;
+    DevBuf<double> ipow;
     // excluded source lists (self_generator / is_self): CSR over original target
     // indices, original -> sorted index, sorted point -> leaf
     DevBuf<int64_t> ex_ptr;
     DevBuf<int32_t> ex_col, ex_inv, ex_leaf;
     int ex_near_too = 0;
     bool ex_on = false;
-    DevBuf<int> rot_off, tzx_off, m2m_ptr, m2m_code, l2l_ptr, l2l_code, l2l1_ptr, l2l1_code;
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
@@ -97,9 +108,9 @@ struct Plan {
 };
 
 void plan_init(Plan& pl);
-// Fills pl.rfrag / pl.tzfrag / pl.tzl from the uploaded rotation and
-// translation tables (m2l.cu).
-void build_m2l_fragments(Plan& pl, cudaStream_t st);
+// Fills the fragment-order operators of tb (rfrag / tzfrag / tzl, and the
+// FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
+void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);
 void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
 void plan_read_timings(Plan& pl, double* ms6);
 // Exclusions (exclude.cu): ptr / cols are device arrays (n + 1, ptr[n]).

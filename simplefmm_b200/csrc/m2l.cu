@@ -1933,29 +1933,28 @@ void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream
 
 }  // namespace
 
-void build_m2l_fragments(Plan& pl, cudaStream_t st)
+void build_m2l_fragments(PlanTables& tb, int P, bool mixed, cudaStream_t st)
 {
-    const int P = pl.p;
-    pl.rfrag_nf = mma_foff(P + 2);
-    pl.rfrag.alloc(size_t(kNumClasses) * pl.rfrag_nf * 4 * 32, st);
+    tb.rfrag_nf = mma_foff(P + 2);
+    tb.rfrag.alloc(size_t(kNumClasses) * tb.rfrag_nf * 4 * 32, st);
     const int nfz = std::max(tz_foff(P, P + 2), 1);
-    pl.tzfrag.alloc(size_t(nfz) * 32, st);
-    pl.tzl.alloc(size_t(P + 1) * (P + 2), st);
-    k_frag_rot<<<256, 256, 0, st>>>(pl.rot.ptr, pl.rot_off.ptr, pl.rot_len, P, pl.rfrag_nf, pl.rfrag.ptr);
+    tb.tzfrag.alloc(size_t(nfz) * 32, st);
+    tb.tzl.alloc(size_t(P + 1) * (P + 2), st);
+    k_frag_rot<<<256, 256, 0, st>>>(tb.rot.ptr, tb.rot_off.ptr, tb.rot_len, P, tb.rfrag_nf, tb.rfrag.ptr);
     SFMM_CHECK_LAUNCH();
-    k_frag_tz<<<16, 256, 0, st>>>(pl.tzx.ptr, pl.tzx_off.ptr, P, tz_foff(P, P + 2), pl.tzfrag.ptr, pl.tzl.ptr);
+    k_frag_tz<<<16, 256, 0, st>>>(tb.tzx.ptr, tb.tzx_off.ptr, P, tz_foff(P, P + 2), tb.tzfrag.ptr, tb.tzl.ptr);
     SFMM_CHECK_LAUNCH();
-    if (pl.precision == FMM_PRECISION_MIXED) {
-        pl.rf32_nf = tf_foff(P + 2);
-        pl.tz32_nf = std::max(tf_zoff(P, P + 2), 1);
-        pl.rf32.alloc(size_t(kNumClasses) * pl.rf32_nf * 4 * 64 * 4, st);     // float4, high and low parts
-        pl.tz32.alloc(size_t(kNumClasses) * pl.tz32_nf * 64 * 4, st);
-        pl.tzl32.alloc(size_t(kNumClasses) * (P + 1) * (P + 2), st);
-        k_frag_rot32<<<256, 256, 0, st>>>(pl.rot.ptr, pl.rot_off.ptr, pl.rot_len, P, pl.rf32_nf,
-                                          reinterpret_cast<float4*>(pl.rf32.ptr));
+    if (mixed) {
+        tb.rf32_nf = tf_foff(P + 2);
+        tb.tz32_nf = std::max(tf_zoff(P, P + 2), 1);
+        tb.rf32.alloc(size_t(kNumClasses) * tb.rf32_nf * 4 * 64 * 4, st);     // float4, high and low parts
+        tb.tz32.alloc(size_t(kNumClasses) * tb.tz32_nf * 64 * 4, st);
+        tb.tzl32.alloc(size_t(kNumClasses) * (P + 1) * (P + 2), st);
+        k_frag_rot32<<<256, 256, 0, st>>>(tb.rot.ptr, tb.rot_off.ptr, tb.rot_len, P, tb.rf32_nf,
+                                          reinterpret_cast<float4*>(tb.rf32.ptr));
         SFMM_CHECK_LAUNCH();
-        k_frag_tz32<<<64, 256, 0, st>>>(pl.tzx.ptr, pl.tzx_off.ptr, P, tf_zoff(P, P + 2),
-                                        reinterpret_cast<float4*>(pl.tz32.ptr), pl.tzl32.ptr);
+        k_frag_tz32<<<64, 256, 0, st>>>(tb.tzx.ptr, tb.tzx_off.ptr, P, tf_zoff(P, P + 2),
+                                        reinterpret_cast<float4*>(tb.tz32.ptr), tb.tzl32.ptr);
         SFMM_CHECK_LAUNCH();
     }
 }
