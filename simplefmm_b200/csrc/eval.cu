@@ -353,6 +353,7 @@ void plan_init(Plan& pl)
     pl.M.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LA.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
+    if (pl.precision == FMM_PRECISION_MIXED) pl.m32.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     pl.out.alloc(size_t(t.n) * kmax, st);
@@ -428,6 +429,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.tz32 = pl.tab->tz32.ptr;
     a.tz32_nf = pl.tab->tz32_nf;
     a.tzl32 = pl.tab->tzl32.ptr;
+    a.m32 = pl.m32.ptr;
     a.M = reinterpret_cast<cplx*>(pl.M.ptr);
     a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
     a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);

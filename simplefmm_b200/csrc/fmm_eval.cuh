@@ -65,6 +65,7 @@ struct EvalArgs {
     const float* tz32;
     int tz32_nf;
     const float* tzl32;
+    float2* m32;                          // mixed: s^-n M (FP32) per node, written before the M2L
     cplx* M;
     cplx* LA;
     cplx* LB;
@@ -101,6 +102,7 @@ struct Plan {
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
+    DevBuf<float2> m32;                       // mixed precision: scaled FP32 source moments
     cudaEvent_t ev[6] = {};
     // one captured evaluation (fmm_plan_capture / fmm_plan_replay)
     cudaGraph_t graph = nullptr;

@@ -416,6 +416,11 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
@@ -1363,7 +1368,9 @@ __global__ void k_frag_tz(const double* __restrict__ tzx, const int* __restrict_
 // box size s of the level: X~_n = s^-n X_n in, L_j = s^-(j+1) L~_j out, and
 // the z-translation is pre-scaled per class by rho^-(j+n'+1) with rho the
 // centre distance in box sizes (2 .. sqrt 27), so every operand is O(1).
-// Moments and the per-target sums stay in FP64.
+// The scaled moments come in FP32 (k_m32, once per evaluation) and the
+// per-target sums are FP32, scaled by s^-(j+1) into the FP64 locals at the
+// end; four blocks per SM (64 registers, <= 56 KB shared memory at p = 12).
 
 __host__ __device__ constexpr int tf_rt(int n) { return (n + 16) / 16; }   // 16-row tiles of order n
 __host__ __device__ constexpr int tf_kc(int n) { return (n + 8) / 8; }     // 8-wide K chunks of order n
@@ -1469,18 +1476,17 @@ struct MixLayout {
     static constexpr int tm = al16(meta + int(sizeof(MmaMeta)) * 3);
     static constexpr int tn = al16(tm + T1);                       // order n of coefficient t
     static constexpr int offs = al16(tn + T1);                     // fragment offsets: foff[P+3], zoff[P+3]
-    static constexpr int spow = al16(offs + 8 * (P + 3));          // s^-k, k = 0..P+2 (doubles)
-    static constexpr int Xraw = al16(spow + 8 * (P + 3));          // [col][T] complex (cp.async)
-    static constexpr int X = al16(Xraw + 8 * T * 16);              // re, im: [col][LD] floats each
+    static constexpr int Xraw = al16(offs + 8 * (P + 3));          // [col][T] float2 (cp.async)
+    static constexpr int X = al16(Xraw + 8 * T * 8);               // re, im: [col][LD] floats each
     static constexpr int W = al16(X + 2 * 8 * LD * 4);
     static constexpr int LzA = al16(W + 2 * 8 * LD * 4);
     static constexpr int LzB = al16(LzA + 2 * 8 * LD * 4);         // [col][LD1]
-    static constexpr int acc = al16(LzB + 2 * 8 * LD1 * 4);        // FP64 complex [8 qd][T] then [8 qd][T1]
-    __host__ __device__ static constexpr int total(int qd) { return al16(acc + 16 * 8 * qd * (T + T1)); }
+    static constexpr int acc = al16(LzB + 2 * 8 * LD1 * 4);        // FP32 complex [8 qd][T] then [8 qd][T1]
+    __host__ __device__ static constexpr int total(int qd) { return al16(acc + 8 * 8 * qd * (T + T1)); }
 };
 
 template<int P>
-__global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int64_t g1)
+__global__ void __launch_bounds__(256, 4) k_m2l_tf32(EvalArgs a, int64_t g0, int64_t g1)
 {
     using L = MixLayout<P>;
     constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 256;
@@ -1496,8 +1502,7 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
     unsigned char* tn = sm + L::tn;
     int* foff = reinterpret_cast<int*>(sm + L::offs);
     int* zoff = foff + (P + 3);
-    double* spow = reinterpret_cast<double*>(sm + L::spow);
-    cplx* Xraw = reinterpret_cast<cplx*>(sm + L::Xraw);
+    float2* Xraw = reinterpret_cast<float2*>(sm + L::Xraw);
     float* Xre = reinterpret_cast<float*>(sm + L::X);
     float* Xim = Xre + 8 * LD;
     float* Wre = reinterpret_cast<float*>(sm + L::W);
@@ -1507,8 +1512,8 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
     float* Bre = reinterpret_cast<float*>(sm + L::LzB);
     float* Bim = Bre + 8 * LD1;
     const int qd = a.qdim;
-    cplx* accA = reinterpret_cast<cplx*>(sm + L::acc);
-    cplx* accB = accA + 8 * qd * T;
+    float2* accA = reinterpret_cast<float2*>(sm + L::acc);
+    float2* accB = accA + 8 * qd * T;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g8 = lane >> 2, t4 = lane & 3;                      // fragment group / thread in group
@@ -1562,26 +1567,26 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
     auto issue = [&](int b) {
         const MmaMeta& M = meta[b % 3];
         const int ncol = M.ncol;
-        cplx* xr = Xraw;
+        float2* xr = Xraw;
         for (int e = tid; e < 8 * T; e += NT) {
             const int c = e / T, t = e - c * T;
-            if (c < ncol) cp_async16(xr + e, a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
+            if (c < ncol) cp_async8(xr + e, a.m32 + (int64_t(M.src[c]) * qd + M.bq[c]) * T + t);
         }
         cp_async_commit();
     };
-    // X~ = s^-n e^{i m phi} M, rounded to FP32, column-major
+    // X~ = e^{i m phi} (s^-n M), column-major
     auto phase_in = [&](int b) {
         const MmaMeta& M = meta[b % 3];
         const int ncol = M.ncol;
-        const cplx* xr = Xraw;
+        const float2* xr = Xraw;
         for (int e = tid; e < 8 * T; e += NT) {
             const int c = e / T, t = e - c * T;
             if (c < ncol) {
                 const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
-                const cplx v = cmul(cplx{ph.x, ph.y}, xr[e]);
-                const double sc = spow[tn[t]];
-                Xre[c * LD + t] = static_cast<float>(v.re * sc);
-                Xim[c * LD + t] = static_cast<float>(v.im * sc);
+                const float pc = static_cast<float>(ph.x), ps = static_cast<float>(ph.y);
+                const float2 v = xr[e];
+                Xre[c * LD + t] = pc * v.x - ps * v.y;
+                Xim[c * LD + t] = ps * v.x + pc * v.y;
             }
         }
     };
@@ -1598,16 +1603,7 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
                 cls[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
             }
             if (tid <= 8) kids[tid] = a.il_ptr[cb + min(tid, nc)];
-            for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = cplx{0, 0};
-            if (tid == 0) {
-                // s^-k for the box size s of the targets' (= sources') level
-                const double sinv = double(1 << lt) / a.box->width;
-                double v = 1.0;
-                for (int k = 0; k <= P + 2; ++k) {
-                    spow[k] = v;
-                    v *= sinv;
-                }
-            }
+            for (int t = tid; t < 8 * qd * (T + T1); t += NT) accA[t] = make_float2(0.f, 0.f);
             __syncthreads();
             for (int cl = tid; cl < kNumClasses; cl += NT) {
                 int cnt = 0;
@@ -1785,7 +1781,7 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
             }
             cp_async_wait_all();
             __syncthreads();
-            // ---- accumulate (FP64, s^-(j+1) scale) in column order; phase tile b + 1 in
+            // ---- accumulate (FP32, scaled at the end) in column order; phase tile b + 1 in
             {
                 const int ncol = M.ncol;
                 int sb[8];
@@ -1794,29 +1790,53 @@ __global__ void __launch_bounds__(256, 3) k_m2l_tf32(EvalArgs a, int64_t g0, int
                 for (int t = tid; t < T + T1; t += NT) {
                     const bool isA = t < T;
                     const int r = isA ? t : t - T;
-                    const double sc = spow[tn[r] + 1];
                     const float* sre = isA ? Are + r : Bre + r;
                     const float* sim = isA ? Aim + r : Bim + r;
                     const int ld = isA ? LD : LD1;
-                    cplx* acc = isA ? accA + r : accB + r;
+                    float2* acc = isA ? accA + r : accB + r;
                     const int stride = isA ? T : T1;
 #pragma unroll
                     for (int c = 0; c < 8; ++c)
                         if (c < ncol) {
-                            cplx& d = acc[sb[c] * stride];
-                            d.re += sc * static_cast<double>(sre[c * ld]);
-                            d.im += sc * static_cast<double>(sim[c * ld]);
+                            float2& d = acc[sb[c] * stride];
+                            d.x += sre[c * ld];
+                            d.y += sim[c * ld];
                         }
                 }
                 if (b + 1 < nbat) phase_in(b + 1);
             }
             __syncthreads();
         }
+        // L_j = s^-(j+1) L~_j for the box size s of the targets' level
+        const double sinv = double(1 << lt) / a.box->width;
         if (a.want_pot)
-            for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = accA[e];
+            for (int e = tid; e < nc * qd * T; e += NT) {
+                const float2 v = accA[e];
+                const double sc = pow(sinv, double(tn[e % T] + 1));
+                a.LA[int64_t(cb) * qd * T + e] = cplx{sc * v.x, sc * v.y};
+            }
         if (a.want_field)
-            for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = accB[e];
+            for (int e = tid; e < nc * qd * T1; e += NT) {
+                const float2 v = accB[e];
+                const double sc = pow(sinv, double(tn[e % T1] + 1));
+                a.LB[int64_t(cb) * qd * T1 + e] = cplx{sc * v.x, sc * v.y};
+            }
         __syncthreads();
+    }
+}
+
+// s^-n M in FP32 (the mixed kernel's source moments), nodes [n0, n1)
+__global__ void k_m32(EvalArgs a, int64_t n0, int64_t n1)
+{
+    const int T = a.T;
+    const int64_t per = int64_t(a.qdim) * T, total = (n1 - n0) * per;
+    for (int64_t idx = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; idx < total; idx += int64_t(gridDim.x) * blockDim.x) {
+        const int64_t node = n0 + idx / per, e = node * per + idx % per;
+        int n, m;
+        tri_nm(static_cast<int>(idx % per % T), n, m);
+        const double sc = pow(double(1 << level_of(a, node)) / a.box->width, double(n));
+        const cplx v = a.M[e];
+        a.m32[e] = make_float2(static_cast<float>(v.re * sc), static_cast<float>(v.im * sc));
     }
 }
 
@@ -1831,7 +1851,12 @@ bool try_launch_tf32(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStr
     allow_max_smem(k_m2l_tf32<P>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_tf32<P>, 256, smem));
-    if (per_sm < 1) return false;
+    if (per_sm < 1 || a.m32 == nullptr) return false;
+    // sources of every interaction are boxes of levels >= 2
+    const int64_t n0 = a.lvl_off[2], n1 = a.lvl_off[a.depth + 1];
+    k_m32<<<static_cast<unsigned>(std::min<int64_t>((n1 - n0) * a.qdim * a.T / 256 + 1, int64_t(sms) * 16)), 256, 0, st>>>(a, n0,
+                                                                                                                        n1);
+    SFMM_CHECK_LAUNCH();
     const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
     k_m2l_tf32<P><<<static_cast<unsigned>(grid), 256, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
