@@ -438,6 +438,8 @@ def main():
                        "depth": tree.depth, **stats},
             "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": n_check},
             "phases_ms": {k: round(statistics.mean(ph[k] for ph in phases), 3) for k in phases[0]},
+            "step_ms": [round(x, 3) for x in times],
+            "tree_ms_per_step": [round(ph["tree_ms"], 3) for ph in phases],
             "roofline": {"bound": "fp64", "kernel": "k_m2l", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak,
                          "peak_source": "FP64 DGEMM (torch float64 matmul 8192^3) measured in this run",

@@ -65,21 +65,34 @@ inline void allow_max_smem(KernelT k)
 // user of the device's default pool can trim it between evaluations.
 cudaMemPool_t device_pool(int device);
 
+// Device allocation for DevBuf (memory.cu): blocks of at least 4 MiB are
+// cached by exact size when released and handed back to the next request of
+// that size on the same device, after the requesting stream has waited for
+// the releasing stream (an event recorded at release).  Repeated solves of
+// one size (time stepping, the bench) then reuse their own buffers and the
+// pool never grows between them: growing it stalled single allocations for
+// 0.4-0.9 s once several GB were in play.  The cache holds at most a third of
+// the device's memory (oldest blocks are freed first) and is emptied when an
+// allocation fails, before the allocation is retried.
+void* device_alloc(size_t bytes, int device, cudaStream_t s);        // throws FMM_ERR_OUT_OF_MEMORY
+void device_free(void* p, size_t bytes, int device, cudaStream_t s) noexcept;
+
 template<typename T>
 struct DevBuf {
     T* ptr = nullptr;
     size_t count = 0;
     cudaStream_t stream = nullptr;
+    int device = 0;
 
     DevBuf() = default;
     DevBuf(const DevBuf&) = delete;
     DevBuf& operator=(const DevBuf&) = delete;
-    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream) { o.ptr = nullptr; o.count = 0; }
+    DevBuf(DevBuf&& o) noexcept : ptr(o.ptr), count(o.count), stream(o.stream), device(o.device) { o.ptr = nullptr; o.count = 0; }
     DevBuf& operator=(DevBuf&& o) noexcept
     {
         if (this != &o) {
             release();
-            ptr = o.ptr; count = o.count; stream = o.stream;
+            ptr = o.ptr; count = o.count; stream = o.stream; device = o.device;
             o.ptr = nullptr; o.count = 0;
         }
         return *this;
@@ -90,18 +103,10 @@ struct DevBuf {
     {
         release();
         stream = s;
-        count = n;
         if (n) {
-            int dev = 0;
-            SFMM_CUDA(cudaGetDevice(&dev));
-            cudaError_t e = cudaMallocFromPoolAsync(reinterpret_cast<void**>(&ptr), n * sizeof(T), device_pool(dev), s);
-            if (e == cudaErrorMemoryAllocation) {
-                (void)cudaGetLastError();
-                ptr = nullptr;
-                count = 0;
-                throw Error(FMM_ERR_OUT_OF_MEMORY, "device allocation of " + std::to_string(n * sizeof(T)) + " bytes failed");
-            }
-            SFMM_CUDA(e);
+            SFMM_CUDA(cudaGetDevice(&device));
+            ptr = static_cast<T*>(device_alloc(n * sizeof(T), device, s));
+            count = n;
         }
     }
     // grow keeping the first `keep` elements
@@ -115,7 +120,7 @@ struct DevBuf {
     }
     void release() noexcept
     {
-        if (ptr) cudaFreeAsync(ptr, stream);
+        if (ptr) device_free(ptr, count * sizeof(T), device, stream);
         ptr = nullptr;
         count = 0;
     }
