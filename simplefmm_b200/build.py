@@ -34,6 +34,10 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
+def cuda_lib() -> Path:
+    return Path(nvcc()).resolve().parent.parent / "lib64"
+
+
 def _sources():
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp"))
 
@@ -64,7 +68,8 @@ def build(verbose: bool = False, extra_flags=None) -> Path:
         list(ex.map(run, jobs))
     objs = [BUILD / (s.stem + ".o") for s in _sources()]
     if jobs or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        run([nvcc()] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] + ["-lcudart"])
+        run([nvcc()] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] +
+            ["-lcudart", "-lcublas", "-Xlinker", "-rpath=" + str(cuda_lib())])
     return LIB
 
 

@@ -70,6 +70,8 @@ void release_context(fmm_context* ctx)
     if (!ctx || --ctx->refs > 0) return;
     cudaSetDevice(ctx->c.device);
     cudaStreamSynchronize(ctx->c.stream);
+    sfmm::release_blas(ctx->c);
+    cudaStreamSynchronize(ctx->c.stream);
     if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
 }

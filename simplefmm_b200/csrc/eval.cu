@@ -354,6 +354,7 @@ void plan_init(Plan& pl)
     pl.LA.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
     if (pl.precision == FMM_PRECISION_MIXED) pl.m32.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
+    shift_setup(pl);
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     pl.out.alloc(size_t(t.n) * kmax, st);
@@ -459,6 +460,10 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         const int w_m2m = warps_for(head, sm_m2m_w);
         allow_smem(k_m2m, head + sm_m2m_w * w_m2m);
         for (int l = t.depth - 1; l >= 2; --l) {
+            if (pl.shift_on) {
+                shift_m2m(pl, a, l, st);
+                continue;
+            }
             const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
             k_m2m<<<blocks_for(c, w_m2m, 65535), w_m2m * 32, head + sm_m2m_w * w_m2m, st>>>(a, l, t.lvl_off[l], c);
             SFMM_CHECK_LAUNCH();
@@ -471,6 +476,10 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         const int w_l2l = warps_for(head2, sm_l2l_w);
         allow_smem(k_l2l, head2 + sm_l2l_w * w_l2l);
         for (int l = 3; l <= t.depth; ++l) {
+            if (pl.shift_on) {
+                shift_l2l(pl, a, l, st);
+                continue;
+            }
             const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
             k_l2l<<<blocks_for(c, w_l2l, 65535), w_l2l * 32, head2 + sm_l2l_w * w_l2l, st>>>(a, l, t.lvl_off[l], c);
             SFMM_CHECK_LAUNCH();

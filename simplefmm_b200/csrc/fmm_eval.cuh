@@ -102,6 +102,12 @@ struct Plan {
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
+    // M2M / L2L as matrix products (shift.cu): per children level the octant
+    // maps, compact slots of the parents that have children, scratch rows
+    bool shift_on = false;
+    DevBuf<double> sh_ops, sh_x, sh_y;
+    DevBuf<int32_t> sh_slot, sh_list;
+    std::vector<int32_t> sh_S;
     DevBuf<float2> m32;                       // mixed precision: scaled FP32 source moments
     cudaEvent_t ev[6] = {};
     // one captured evaluation (fmm_plan_capture / fmm_plan_replay)
@@ -110,6 +116,12 @@ struct Plan {
 };
 
 void plan_init(Plan& pl);
+// shift.cu: set-up at plan creation, M2M into parent level lp, L2L into
+// children level lc, and the context's cuBLAS handle at context teardown
+void shift_setup(Plan& pl);
+void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st);
+void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st);
+void release_blas(Context& c) noexcept;
 // Fills the fragment-order operators of tb (rfrag / tzfrag / tzl, and the
 // FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
 void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);

@@ -165,6 +165,8 @@ struct Context {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int sm_count = 148;
+    void* blas = nullptr;                 // cuBLAS handle of the M2M / L2L products (shift.cu)
+    void* blas_ws = nullptr;              // its fixed workspace
 };
 
 // Device-resident octree: nodes of all levels concatenated level by level
