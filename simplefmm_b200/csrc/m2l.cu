@@ -933,7 +933,11 @@ __host__ __device__ constexpr int tz_job0(int P, int k)
     return s;
 }
 
-template<int P, int NS>
+// LEAN: no staging buffer for the moments (the phase-in reads them from
+// global memory) and the potential local's buffer shares X's (X is dead after
+// the rotation; one more barrier between accumulation and the next phase-in),
+// for four blocks per SM where that fits.
+template<int P, int NS, bool LEAN = false>
 struct MmaLayout {
     static constexpr int NC = 8 * NS;                           // columns per tile (NS MMA N-tiles)
     static constexpr int T = (P + 1) * (P + 2) / 2;
@@ -948,18 +952,18 @@ struct MmaLayout {
     static constexpr int meta = al16(bat_off + 4 * 72);
     static constexpr int tm = al16(meta + int(sizeof(MetaC<NC>)) * 3);
     static constexpr int Xraw = al16(tm + T1);                    // [col][T] complex (cp.async)
-    static constexpr int X = al16(Xraw + NC * T * 16);              // re, im: [col][LD] doubles each
+    static constexpr int X = LEAN ? Xraw : al16(Xraw + NC * T * 16); // re, im: [col][LD] doubles each
     static constexpr int W = al16(X + 2 * NC * LD * 8);             // azimuth-major rows
-    static constexpr int LzA = al16(W + 2 * NC * LD * 8);
-    static constexpr int LzB = al16(LzA + 2 * NC * LD * 8);         // [col][LD1]
+    static constexpr int LzA = LEAN ? X : al16(W + 2 * NC * LD * 8);
+    static constexpr int LzB = LEAN ? al16(W + 2 * NC * LD * 8) : al16(LzA + 2 * NC * LD * 8);   // [col][LD1]
     static constexpr int acc = al16(LzB + 2 * NC * LD1 * 8);        // [8 qd][T] then [8 qd][T1] complex
     __host__ __device__ static constexpr int total(int qd) { return al16(acc + 16 * 8 * qd * (T + T1)); }
 };
 
-template<int P, int NS, int NW>
-__global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a, int64_t g0, int64_t g1)
+template<int P, int NS, int NW, bool LEAN>
+__global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_mma(EvalArgs a, int64_t g0, int64_t g1)
 {
-    using L = MmaLayout<P, NS>;
+    using L = MmaLayout<P, NS, LEAN>;
     constexpr int T = L::T, T1 = L::T1, LD = L::LD, LD1 = L::LD1, NT = 32 * NW, NC = L::NC;
     using Meta = MetaC<NC>;
     extern __shared__ __align__(16) unsigned char sm[];
@@ -1032,6 +1036,7 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a
     };
     // raw source moments of tile b -> Xraw[b & 1] (asynchronous)
     auto issue = [&](int b) {
+        if constexpr (LEAN) return;
         const Meta& M = meta[b % 3];
         const int ncol = M.ncol;
         cplx* xr = Xraw;
@@ -1050,7 +1055,10 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a
             const int c = e / T, t = e - c * T;
             if (c < ncol) {
                 const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
-                const cplx v = cmul(cplx{ph.x, ph.y}, xr[e]);
+                cplx m;
+                if constexpr (LEAN) m = a.M[(int64_t(M.src[c]) * qd + M.bq[c]) * T + t];
+                else m = xr[e];
+                const cplx v = cmul(cplx{ph.x, ph.y}, m);
                 Xre[c * LD + t] = v.re;
                 Xim[c * LD + t] = v.im;
             }
@@ -1286,6 +1294,7 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a
                             d.im += sim[c * ld];
                         }
                 }
+                if constexpr (LEAN) __syncthreads();          // X shares the potential local's buffer
                 if (b + 1 < nbat) phase_in(b + 1);
             }
             __syncthreads();
@@ -1298,20 +1307,21 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? 3 : 1) k_m2l_mma(EvalArgs a
     }
 }
 
-template<int P, int NS, int NW>
+template<int P, int NS, int NW, bool LEAN>
 bool try_launch_mma(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
-    const size_t smem = MmaLayout<P, NS>::total(a.qdim);
+    const size_t smem = MmaLayout<P, NS, LEAN>::total(a.qdim);
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
     if (smem > size_t(optin)) return false;
-    allow_max_smem(k_m2l_mma<P, NS, NW>);
+    allow_max_smem(k_m2l_mma<P, NS, NW, LEAN>);
     int per_sm = 0;
-    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P, NS, NW>, 32 * NW, smem));
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P, NS, NW, LEAN>, 32 * NW, smem));
+    if (LEAN && per_sm < 4) return false;
     if (per_sm < 1) return false;
     const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
-    k_m2l_mma<P, NS, NW><<<static_cast<unsigned>(grid), 32 * NW, smem, st>>>(a, g0, g1);
+    k_m2l_mma<P, NS, NW, LEAN><<<static_cast<unsigned>(grid), 32 * NW, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
     return true;
 }
@@ -1941,7 +1951,8 @@ void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream
 {
     if constexpr (P >= 2) {
         if (a.mixed && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
-        if (try_launch_mma<P, 1, 8>(a, g0, g1, sms, st)) return;
+        if (try_launch_mma<P, 1, 8, true>(a, g0, g1, sms, st)) return;
+        if (try_launch_mma<P, 1, 8, false>(a, g0, g1, sms, st)) return;
     }
     if constexpr (P >= 2 && P <= 12) {
         // two blocks per SM of 4-column batches measured fastest up to p = 10
