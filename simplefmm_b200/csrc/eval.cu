@@ -31,12 +31,21 @@ namespace {
 
 constexpr int kMaxWarps = 8;
 
+// Charges into leaf order (qs, one array per component) and, for the FP64
+// near field, the packed source records (x y z q0 | q1 q2).
 __global__ void k_gather_q(const double* __restrict__ Q, const int32_t* __restrict__ order, int64_t n, int qdim,
-                           double* __restrict__ qs)
+                           double* __restrict__ qs, const double* __restrict__ pts, double4* __restrict__ src4,
+                           double2* __restrict__ src2)
 {
     for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         const int64_t o = order[i];
-        for (int b = 0; b < qdim; ++b) qs[b * n + i] = Q[o * qdim + b];
+        double q[3] = {0, 0, 0};
+        for (int b = 0; b < qdim; ++b) {
+            q[b] = Q[o * qdim + b];
+            qs[b * n + i] = q[b];
+        }
+        if (src4) src4[i] = make_double4(pts[i], pts[n + i], pts[2 * n + i], q[0]);
+        if (src2) src2[i] = make_double2(q[1], q[2]);
     }
 }
 
@@ -355,8 +364,13 @@ void plan_init(Plan& pl)
     pl.LB.alloc(size_t(t.n_nodes) * pl.qdim * pl.T1, st);
     if (pl.precision == FMM_PRECISION_MIXED) pl.m32.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     shift_setup(pl);
+    p2p_setup(pl);
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
+    if (pl.precision == FMM_PRECISION_FP64) {
+        pl.src4.alloc(size_t(t.n), st);
+        if (pl.qdim > 1) pl.src2.alloc(size_t(t.n), st);
+    }
     pl.out.alloc(size_t(t.n) * kmax, st);
     pl.out2.alloc(size_t(t.n) * kmax, st);
 }
@@ -435,6 +449,16 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.LA = reinterpret_cast<cplx*>(pl.LA.ptr);
     a.LB = reinterpret_cast<cplx*>(pl.LB.ptr);
     a.qs = pl.qs.ptr;
+    a.src4 = pl.src4.ptr;
+    a.src2 = pl.src2.ptr;
+    a.p2p_item = pl.p2p_item.ptr;
+    a.p2p_row = pl.p2p_row.ptr;
+    a.p2p_items = pl.p2p_items;
+    a.p2p_parts = pl.p2p_parts.ptr;
+    a.p2p_rowoff = pl.p2p_rowoff.ptr;
+    a.p2p_part = pl.p2p_part.ptr;
+    a.p2p_ctr = pl.p2p_ctr.ptr;
+    a.p2p_split = pl.p2p_rows > 0;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;
     if (a.K == 0) return;
@@ -444,7 +468,8 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     const int sms = t.ctx->sm_count;
 
     SFMM_CUDA(cudaEventRecord(pl.ev[0], st));
-    k_gather_q<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(Q, t.order.ptr, t.n, qd, pl.qs.ptr);
+    k_gather_q<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(Q, t.order.ptr, t.n, qd, pl.qs.ptr, t.pts.ptr,
+                                                               pl.src4.ptr, pl.src2.ptr);
     SFMM_CHECK_LAUNCH();
     SFMM_CUDA(cudaMemsetAsync(pl.out.ptr, 0, size_t(t.n) * K * sizeof(double), st));
     const bool far = t.depth >= 2;

@@ -70,6 +70,19 @@ struct EvalArgs {
     cplx* LA;
     cplx* LB;
     const double* qs;
+    const double4* src4;                  // FP64 near field: x y z q0 per point, leaf order
+    const double2* src2;                  // q1 q2 per point (qdim > 1)
+    // near-field work items (p2p.cu): (leaf, first range, offset in it,
+    // sources) and the item's first row of partial sums (-1: the leaf is
+    // one item and writes out2 directly); per leaf the number of parts and
+    // the first row; a counter the warps take items from
+    const int4* p2p_item;
+    const int32_t* p2p_row;
+    int64_t p2p_items;
+    const int32_t *p2p_parts, *p2p_rowoff;
+    double* p2p_part;
+    int* p2p_ctr;
+    int p2p_split;                        // some leaf has more than one part
     double* out;                         // far field per component, sorted order
     double* out2;                        // near field per component, sorted order
 };
@@ -101,6 +114,13 @@ struct Plan {
     bool ex_on = false;
     DevBuf<double2> M, LA, LB;
     DevBuf<double> qs, out, out2;
+    DevBuf<double4> src4;                     // FP64 near-field source records (p2p.cu)
+    DevBuf<double2> src2;
+    // near-field work items (p2p.cu, p2p_setup)
+    DevBuf<int4> p2p_item;
+    DevBuf<int32_t> p2p_row, p2p_parts, p2p_rowoff, p2p_ctr;
+    DevBuf<double> p2p_part;
+    int64_t p2p_items = 0, p2p_rows = 0;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
     // M2M / L2L as matrix products (shift.cu): per children level the octant
     // maps, compact slots of the parents that have children, scratch rows
@@ -122,6 +142,9 @@ void shift_setup(Plan& pl);
 void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st);
 void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st);
 void release_blas(Context& c) noexcept;
+// p2p.cu: near-field work items of the plan's tree (leaves with a large near
+// field split into parts), built at plan creation
+void p2p_setup(Plan& pl);
 // Fills the fragment-order operators of tb (rfrag / tzfrag / tzl, and the
 // FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
 void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);

@@ -2,13 +2,17 @@
 // its neighbour-list point ranges, with the reference's self exclusion
 // (is_self: i == j, fmm.hpp:786, 880).
 //
-// Warp per target leaf.  The leaf's source ranges are gathered into full
-// shared tiles of kChunk sources (x y | z q packed as double2).  Lanes are
-// (target group, source slice): tg targets per pass and 32/tg slices, with tg
-// chosen per leaf so that at most kMaxPass passes cover its targets; every
-// source read from shared memory is applied to the lane's target of every
-// pass (register blocking over passes).  Slices of a target are summed with
-// xor shuffles at the end.
+// Warp per target leaf.  Sources are packed records (x y z q0 | q1 q2, leaf
+// order) and a leaf's near-field ranges are staged into full shared tiles of
+// kChunk sources by asynchronous 16-byte copies, two tiles per warp: the
+// copies of tile c + 1 are in flight while tile c is summed, so the gathers'
+// L2 / DRAM latency hides behind the arithmetic.  The leaf's ranges are read
+// 32 at a time into registers (lane k holds range k) and walked with
+// shuffles.  Lanes are (target group, source slice): tg targets per pass and
+// 32/tg slices, with tg chosen per leaf so that at most kMaxPass passes cover
+// its targets; every source read from shared memory is applied to the lane's
+// target of every pass (register blocking over passes).  Slices of a target
+// are summed with xor shuffles at the end.
 #include "eval_util.cuh"
 
 namespace sfmm {
@@ -17,10 +21,213 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kChunk = 128;
 
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
+// ---------------------------------------------------------------- work items
+// A coarse leaf beside a dense region can hold most of the points in its
+// near field (on 4M Plummer points eight leaves have ~500k near sources each,
+// ten times one warp's share of the whole near field), so one warp per leaf
+// leaves a few warps working long after the rest.  A leaf whose
+// targets x sources exceeds kPartCost is split into parts of consecutive near
+// sources of equal size, each part a work item; a split leaf's parts write
+// rows of partial sums that k_p2p_reduce adds in part order, so the result
+// does not depend on which warp ran which item.  Warps take items from a
+// counter, in leaf order (coarse leaves, the split ones among them, first).
+constexpr int64_t kPartCost = 131072;
+
+__global__ void k_p2p_cost(const int32_t* __restrict__ nr_ptr, const int2* __restrict__ nr,
+                           const int32_t* __restrict__ pbeg, const int32_t* __restrict__ pend,
+                           const int32_t* __restrict__ leaf_node, int64_t n_leaves, int32_t* __restrict__ parts,
+                           int32_t* __restrict__ rows, int32_t* __restrict__ psize, int32_t* __restrict__ nsrc)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t f = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; f < n_leaves; f += stride) {
+        const int g = leaf_node[f];
+        const int nt = pend[g] - pbeg[g];
+        const int r0 = nr_ptr[f], r1 = nr_ptr[f + 1];
+        int64_t ns = 0;
+        for (int r = r0 + lane; r < r1; r += 32) ns += nr[r].y - nr[r].x;
+        for (int o = 16; o; o >>= 1) ns += __shfl_xor_sync(0xffffffffu, ns, o);
+        if (lane == 0) {
+            const int64_t cost = int64_t(nt) * ns;
+            int64_t np = 1, S = ns;
+            if (cost > kPartCost && ns > 1) {
+                np = ns < (cost + kPartCost - 1) / kPartCost ? ns : (cost + kPartCost - 1) / kPartCost;
+                S = (ns + np - 1) / np;
+                np = (ns + S - 1) / S;
+            }
+            parts[f] = static_cast<int>(np);
+            rows[f] = np > 1 ? static_cast<int>(np) * nt : 0;
+            psize[f] = static_cast<int>(S);
+            nsrc[f] = static_cast<int>(ns);
+        }
+    }
+}
+
+__global__ void k_p2p_totals(const int32_t* parts, const int32_t* rows, const int32_t* item_off,
+                             const int32_t* row_off, int64_t n, int32_t* tot)
+{
+    tot[0] = item_off[n - 1] + parts[n - 1];
+    tot[1] = row_off[n - 1] + rows[n - 1];
+}
+
+// Warp per leaf: the items of its parts.  Part k starts at source k * S of
+// the leaf's near field; the range holding it is found from a warp prefix
+// sum over 32 ranges at a time.
+__global__ void k_p2p_items(const int32_t* __restrict__ nr_ptr, const int2* __restrict__ nr,
+                            const int32_t* __restrict__ pbeg, const int32_t* __restrict__ pend,
+                            const int32_t* __restrict__ leaf_node, int64_t n_leaves, const int32_t* __restrict__ parts,
+                            const int32_t* __restrict__ psize, const int32_t* __restrict__ nsrc,
+                            const int32_t* __restrict__ item_off, const int32_t* __restrict__ row_off,
+                            int4* __restrict__ item, int32_t* __restrict__ row)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t f = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; f < n_leaves; f += stride) {
+        const int np = parts[f], off = item_off[f], ns = nsrc[f];
+        const int r0 = nr_ptr[f], r1 = nr_ptr[f + 1];
+        if (np == 1) {
+            if (lane == 0) {
+                item[off] = make_int4(static_cast<int>(f), r0, 0, ns);
+                row[off] = -1;
+            }
+            continue;
+        }
+        const int g = leaf_node[f];
+        const int nt = pend[g] - pbeg[g];
+        const int64_t S = psize[f];
+        const int rb = row_off[f];
+        int64_t base = 0;
+        for (int c0 = r0; c0 < r1; c0 += 32) {
+            const int ri = c0 + lane;
+            const int len = ri < r1 ? nr[ri].y - nr[ri].x : 0;
+            int cum = len;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, cum, o);
+                if (lane >= o) cum += v;
+            }
+            const int64_t lo = base + cum - len, hi = base + cum;
+            for (int64_t k = (lo + S - 1) / S; k < np && k * S < hi; ++k) {
+                item[off + k] = make_int4(static_cast<int>(f), ri, static_cast<int>(k * S - lo),
+                                          static_cast<int>(S < ns - k * S ? S : ns - k * S));
+                row[off + k] = rb + static_cast<int>(k) * nt;
+            }
+            base += __shfl_sync(0xffffffffu, cum, 31);
+        }
+    }
+}
+
+// Sums the parts of every split leaf, in part order, into out2.
+__global__ void k_p2p_reduce(EvalArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t f = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; f < a.n_leaves; f += stride) {
+        const int np = a.p2p_parts[f];
+        if (np <= 1) continue;
+        const int g = a.leaf_node[f];
+        const int t0 = a.pbeg[g], nt = a.pend[g] - t0;
+        const int64_t rb = a.p2p_rowoff[f];
+        for (int e = lane; e < nt * a.K; e += 32) {
+            const int t = e / a.K, o = e - t * a.K;
+            double v = 0;
+            for (int k = 0; k < np; ++k) v += a.p2p_part[(rb + int64_t(k) * nt + t) * a.K + o];
+            a.out2[int64_t(o) * a.n + t0 + t] = v;
+        }
+    }
+}
+
+__device__ __forceinline__ int next_item(int* ctr, int lane)
+{
+    int it = 0;
+    if (lane == 0) it = atomicAdd(ctr, 1);
+    return __shfl_sync(0xffffffffu, it, 0);
+}
+
+// One target's sum of component comp: into out2, or into the item's rows.
+__device__ __forceinline__ void put_near(const EvalArgs& a, int row, int t0, int i, int comp, double v)
+{
+    if (row < 0)
+        a.out2[int64_t(comp) * a.n + i] = v;
+    else
+        a.p2p_part[(int64_t(row) + (i - t0)) * a.K + comp] = v;
+}
+
 template<int QD>
 struct P2PSmem {
-    static constexpr int per_warp = kChunk * (16 + 16 + (QD > 1 ? 16 : 0) + 4);
+    static constexpr int tile = kChunk * (32 + (QD > 1 ? 16 : 0));   // double4 (+ double2) per source
+    static constexpr int per_warp = 2 * tile;
     static constexpr int total = kWarps * per_warp;
+};
+
+// Cursor over a leaf's near ranges [r0, r1): lane k of the warp holds range
+// base + k; every lane walks the same sequence.
+struct RangeWalk {
+    int ri, r1, base, roff, rem;
+    int2 mine;
+
+    // item: (leaf, first range, offset in it, sources); r_end: the leaf's
+    // end of ranges
+    __device__ __forceinline__ void start(const int2* __restrict__ nr, int4 item, int r_end, int lane)
+    {
+        ri = item.y;
+        r1 = r_end;
+        base = item.y;
+        roff = item.z;
+        rem = item.w;
+        mine = ri + lane < r_end ? nr[ri + lane] : make_int2(0, 0);
+    }
+
+    // Issues the copies of the next tile (at most kChunk sources) into t4 / t2;
+    // returns its fill and the one segment that overlaps the target leaf's own
+    // points [t0, t1) (near ranges are disjoint and one of them holds the leaf
+    // itself, so at most one segment of a tile overlaps it).
+    template<int QD>
+    __device__ __forceinline__ int fill_tile(const int2* __restrict__ nr, const double4* __restrict__ src4,
+                                             const double2* __restrict__ src2, double4* t4, double2* t2, int lane,
+                                             int t0, int t1, int& self_s0, int& self_j0, int& self_len)
+    {
+        int fill = 0;
+        self_s0 = 0;
+        self_j0 = 0;
+        self_len = 0;
+        while (rem > 0 && ri < r1 && fill < kChunk) {
+            if (ri - base >= 32) {
+                base = ri;
+                mine = ri + lane < r1 ? nr[ri + lane] : make_int2(0, 0);
+            }
+            const int rx = __shfl_sync(0xffffffffu, mine.x, ri - base);
+            const int ry = __shfl_sync(0xffffffffu, mine.y, ri - base);
+            const int j0 = rx + roff;
+            const int len = min(min(ry - j0, kChunk - fill), rem);
+            const char* g4 = reinterpret_cast<const char*>(src4 + j0);
+            char* d4 = reinterpret_cast<char*>(t4 + fill);
+            for (int c = lane; c < 2 * len; c += 32) cp_async16(d4 + 16 * c, g4 + 16 * c);
+            if (QD > 1)
+                for (int c = lane; c < len; c += 32) cp_async16(t2 + fill + c, src2 + j0 + c);
+            if (j0 < t1 && j0 + len > t0) {
+                self_s0 = fill;
+                self_j0 = j0;
+                self_len = len;
+            }
+            fill += len;
+            roff += len;
+            rem -= len;
+            if (j0 + len == ry) {
+                ++ri;
+                roff = 0;
+            }
+        }
+        cp_async_commit();
+        return fill;
+    }
 };
 
 template<int QD, bool POT, bool FLD, int kMaxPass, int MINB>
@@ -31,18 +238,20 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
     extern __shared__ __align__(16) unsigned char sm[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     unsigned char* mine = sm + w * P2PSmem<QD>::per_warp;
-    double2* sxy = reinterpret_cast<double2*>(mine);
-    double2* szq = sxy + kChunk;
-    double2* sq12 = szq + kChunk;                       // only for QD > 1
-    int* sj = reinterpret_cast<int*>(mine + kChunk * (32 + (QD > 1 ? 16 : 0)));
-    const double* q0 = a.qs;
-    const double* q1 = a.qs + (QD > 1 ? a.n : 0);
-    const double* q2 = a.qs + (QD > 2 ? 2 * a.n : 0);
+    double4* t4[2];
+    double2* t2[2];
+#pragma unroll
+    for (int b = 0; b < 2; ++b) {
+        t4[b] = reinterpret_cast<double4*>(mine + b * P2PSmem<QD>::tile);
+        t2[b] = reinterpret_cast<double2*>(mine + b * P2PSmem<QD>::tile + kChunk * 32);
+    }
 
-    for (int64_t f = blockIdx.x * int64_t(kWarps) + w; f < a.n_leaves; f += int64_t(gridDim.x) * kWarps) {
-        const int g = a.leaf_node[f];
+    for (int it = next_item(a.p2p_ctr, lane); it < a.p2p_items; it = next_item(a.p2p_ctr, lane)) {
+        const int4 item = a.p2p_item[it];
+        const int row = a.p2p_row[it];
+        const int g = a.leaf_node[item.x];
         const int t0 = a.pbeg[g], t1 = a.pend[g];
-        const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
+        const int r1 = a.nr_ptr[item.x + 1];
         for (int tb = t0; tb < t1; tb += kTargetsPerBlock) {
             const int nt = min(kTargetsPerBlock, t1 - tb);
             int tg = 1;
@@ -50,6 +259,10 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
             const int slices = 32 / tg;
             const int passes = (nt + tg - 1) / tg;
             const int ti = lane / slices, s = lane - ti * slices;
+            RangeWalk wk;
+            wk.start(a.nr, item, r1, lane);
+            int cs0, cj0, clen;
+            int fill = wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[0], t2[0], lane, t0, t1, cs0, cj0, clen);
             double xi[kMaxPass], yi[kMaxPass], zi[kMaxPass];
             int ii[kMaxPass];
             double acc[kMaxPass][NO > 0 ? NO : 1];
@@ -58,62 +271,55 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                 const int t = p * tg + ti;
                 const bool on = p < passes && t < nt;
                 ii[p] = on ? tb + t : -1;
-                const int i = on ? tb + t : tb;
-                xi[p] = a.px[i];
-                yi[p] = a.py[i];
-                zi[p] = a.pz[i];
+                const double4 v = a.src4[on ? tb + t : tb];
+                xi[p] = v.x;
+                yi[p] = v.y;
+                zi[p] = v.z;
 #pragma unroll
                 for (int o = 0; o < NO; ++o) acc[p][o] = 0;
             }
-            // stream the leaf's near-field sources through full shared tiles
-            int ri = r0, roff = 0;
-            while (ri < r1) {
-                int fill = 0;
-                while (ri < r1 && fill < kChunk) {
-                    const int2 rg = a.nr[ri];
-                    const int len = min(rg.y - rg.x - roff, kChunk - fill);
-                    for (int k = lane; k < len; k += 32) {
-                        const int j = rg.x + roff + k;
-                        sxy[fill + k] = make_double2(a.px[j], a.py[j]);
-                        szq[fill + k] = make_double2(a.pz[j], q0[j]);
-                        if (QD > 1) sq12[fill + k] = make_double2(q1[j], q2[j]);
-                        sj[fill + k] = j;
-                    }
-                    fill += len;
-                    roff += len;
-                    if (roff == rg.y - rg.x) {
-                        ++ri;
-                        roff = 0;
-                    }
-                }
+            int buf = 0;
+            while (fill > 0) {
+                int ns0, nj0, nlen;
+                const int nfill =
+                    wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[buf ^ 1], t2[buf ^ 1], lane, t0, t1, ns0, nj0, nlen);
+                cp_async_wait_prev();
                 __syncwarp();
+                // slot of the lane's own target in this tile, if it is here
+                int ks[kMaxPass];
+#pragma unroll
+                for (int p = 0; p < kMaxPass; ++p) {
+                    const unsigned d = static_cast<unsigned>(ii[p] - cj0);
+                    ks[p] = ii[p] >= 0 && d < static_cast<unsigned>(clen) ? cs0 + static_cast<int>(d) : -1;
+                }
+                const double4* sx = t4[buf];
+                const double2* sq = t2[buf];
 #pragma unroll 2
                 for (int k = s; k < fill; k += slices) {
-                    const double2 xy = sxy[k], zq = szq[k];
+                    const double4 v = sx[k];
                     double2 qq = make_double2(0, 0);
-                    if (QD > 1) qq = sq12[k];
-                    const int j = sj[k];
+                    if (QD > 1) qq = sq[k];
 #pragma unroll
                     for (int p = 0; p < kMaxPass; ++p) {
                         if (p >= passes) break;
-                        const double dx = xi[p] - xy.x, dy = yi[p] - xy.y, dz = zi[p] - zq.x;
+                        const double dx = xi[p] - v.x, dy = yi[p] - v.y, dz = zi[p] - v.z;
                         const double r2 = fma(dx, dx, fma(dy, dy, dz * dz));
-                        const double ir = j == ii[p] ? 0.0 : rsqrt(r2);
+                        const double ir = k == ks[p] ? 0.0 : rsqrt(r2);
                         int o = 0;
                         if (POT) {
-                            acc[p][o++] = fma(zq.y, ir, acc[p][0]);
+                            acc[p][o++] = fma(v.w, ir, acc[p][0]);
                             if (QD > 1) acc[p][o++] = fma(qq.x, ir, acc[p][1]);
                             if (QD > 2) acc[p][o++] = fma(qq.y, ir, acc[p][2]);
                         }
                         if (FLD) {
                             const double ir3 = ir * ir * ir;
                             if (QD == 1) {
-                                const double cq = zq.y * ir3;
+                                const double cq = v.w * ir3;
                                 acc[p][o] = fma(cq, dx, acc[p][o]);
                                 acc[p][o + 1] = fma(cq, dy, acc[p][o + 1]);
                                 acc[p][o + 2] = fma(cq, dz, acc[p][o + 2]);
                             } else {
-                                const double qa = zq.y, qb = qq.x, qc = qq.y;
+                                const double qa = v.w, qb = qq.x, qc = qq.y;
                                 acc[p][o] = fma((qb * dz - qc * dy), ir3, acc[p][o]);
                                 acc[p][o + 1] = fma((qc * dx - qa * dz), ir3, acc[p][o + 1]);
                                 acc[p][o + 2] = fma((qa * dy - qb * dx), ir3, acc[p][o + 2]);
@@ -122,6 +328,11 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                     }
                 }
                 __syncwarp();
+                buf ^= 1;
+                fill = nfill;
+                cs0 = ns0;
+                cj0 = nj0;
+                clen = nlen;
             }
             // sum the slices of each target (consecutive lanes)
 #pragma unroll
@@ -135,9 +346,9 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                     if (ii[p] < 0) continue;
                     int o = 0;
                     if (POT)
-                        for (int b = 0; b < QD; ++b) a.out2[int64_t(b) * a.n + ii[p]] = acc[p][o++];
+                        for (int b = 0; b < QD; ++b) put_near(a, row, t0, ii[p], b, acc[p][o++]);
                     if (FLD)
-                        for (int c = 0; c < 3; ++c) a.out2[int64_t(a.kf + c) * a.n + ii[p]] = acc[p][o++];
+                        for (int c = 0; c < 3; ++c) put_near(a, row, t0, ii[p], a.kf + c, acc[p][o++]);
                 }
             }
         }
@@ -200,13 +411,15 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
     const double* q1 = a.qs + (QD > 1 ? a.n : 0);
     const double* q2 = a.qs + (QD > 2 ? 2 * a.n : 0);
 
-    for (int64_t f = blockIdx.x * int64_t(kWarps) + w; f < a.n_leaves; f += int64_t(gridDim.x) * kWarps) {
-        const int g = a.leaf_node[f];
+    for (int it = next_item(a.p2p_ctr, lane); it < a.p2p_items; it = next_item(a.p2p_ctr, lane)) {
+        const int4 item = a.p2p_item[it];
+        const int row = a.p2p_row[it];
+        const int g = a.leaf_node[item.x];
         // origin: the leaf's first point (any point near the leaf keeps the
         // FP32 offsets at the leaf's scale)
         const int t0 = a.pbeg[g], t1 = a.pend[g];
         const double c[3] = {a.px[t0], a.py[t0], a.pz[t0]};
-        const int r0 = a.nr_ptr[f], r1 = a.nr_ptr[f + 1];
+        const int r1 = a.nr_ptr[item.x + 1];
         for (int tb = t0; tb < t1; tb += kTargetsPerBlock) {
             const int nt = min(kTargetsPerBlock, t1 - tb);
             int tg = 1;
@@ -230,12 +443,12 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
 #pragma unroll
                 for (int o = 0; o < NO; ++o) acc[p][o] = Sum2{0.f, 0.f};
             }
-            int ri = r0, roff = 0;
-            while (ri < r1) {
+            int ri = item.y, roff = item.z, rem = item.w;
+            while (rem > 0 && ri < r1) {
                 int fill = 0;
-                while (ri < r1 && fill < kChunk) {
+                while (rem > 0 && ri < r1 && fill < kChunk) {
                     const int2 rg = a.nr[ri];
-                    const int len = min(rg.y - rg.x - roff, kChunk - fill);
+                    const int len = min(min(rg.y - rg.x - roff, kChunk - fill), rem);
                     for (int k = lane; k < len; k += 32) {
                         const int j = rg.x + roff + k;
                         const F2 x = split_f(a.px[j] - c[0]), y = split_f(a.py[j] - c[1]), z = split_f(a.pz[j] - c[2]);
@@ -246,6 +459,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
                     }
                     fill += len;
                     roff += len;
+                    rem -= len;
                     if (roff == rg.y - rg.x) {
                         ++ri;
                         roff = 0;
@@ -310,11 +524,21 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
                     for (int off = slices >> 1; off; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
                     if (s == 0 && ii[p] >= 0) {
                         const int comp = POT ? (o < QD ? o : a.kf + (o - QD)) : a.kf + o;
-                        a.out2[int64_t(comp) * a.n + ii[p]] = v;
+                        put_near(a, row, t0, ii[p], comp, v);
                     }
                 }
         }
     }
+}
+
+// Blocks that are resident at once (the warps take items until none is left).
+template<typename K>
+unsigned resident_grid(K kernel, size_t smem, int sms, int64_t items)
+{
+    int nb = 0;
+    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kernel, kWarps * 32, smem));
+    const int64_t need = (items + kWarps - 1) / kWarps;
+    return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>(need, int64_t(std::max(nb, 1)) * sms)));
 }
 
 template<int QD, bool POT, bool FLD, int MP, int MINB>
@@ -322,8 +546,8 @@ void launch_mixed(const EvalArgs& a, int sms, cudaStream_t st)
 {
     const size_t smem = P2PSmemF<QD>::total;
     allow_max_smem(k_p2p_mixed<QD, POT, FLD, MP, MINB>);
-    const int64_t grid = std::min<int64_t>((a.n_leaves + kWarps - 1) / kWarps, int64_t(sms) * 16);
-    k_p2p_mixed<QD, POT, FLD, MP, MINB><<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kWarps * 32, smem, st>>>(a);
+    const unsigned grid = resident_grid(k_p2p_mixed<QD, POT, FLD, MP, MINB>, smem, sms, a.p2p_items);
+    k_p2p_mixed<QD, POT, FLD, MP, MINB><<<grid, kWarps * 32, smem, st>>>(a);
     SFMM_CHECK_LAUNCH();
 }
 
@@ -332,8 +556,8 @@ void launch_fp64(const EvalArgs& a, int sms, cudaStream_t st)
 {
     const size_t smem = P2PSmem<QD>::total;
     allow_max_smem(k_p2p<QD, POT, FLD, MP, MINB>);
-    const int64_t grid = std::min<int64_t>((a.n_leaves + kWarps - 1) / kWarps, int64_t(sms) * 16);
-    k_p2p<QD, POT, FLD, MP, MINB><<<static_cast<unsigned>(std::max<int64_t>(grid, 1)), kWarps * 32, smem, st>>>(a);
+    const unsigned grid = resident_grid(k_p2p<QD, POT, FLD, MP, MINB>, smem, sms, a.p2p_items);
+    k_p2p<QD, POT, FLD, MP, MINB><<<grid, kWarps * 32, smem, st>>>(a);
     SFMM_CHECK_LAUNCH();
 }
 
@@ -353,17 +577,65 @@ void launch(const EvalArgs& a, int sms, cudaStream_t st)
 
 void launch_p2p(const EvalArgs& a, int sms, cudaStream_t st)
 {
+    if (a.p2p_items == 0) return;
+    SFMM_CUDA(cudaMemsetAsync(a.p2p_ctr, 0, sizeof(int), st));
     const int mode = (a.want_pot ? 1 : 0) | (a.want_field ? 2 : 0);
-#define SFMM_P2P(Q)                                              \
-    if (a.qdim == Q) {                                           \
-        if (mode == 1) return launch<Q, true, false>(a, sms, st); \
-        if (mode == 2) return launch<Q, false, true>(a, sms, st); \
-        return launch<Q, true, true>(a, sms, st);                \
+#define SFMM_P2P(Q)                                   \
+    if (a.qdim == Q) {                                \
+        if (mode == 1)                                \
+            launch<Q, true, false>(a, sms, st);       \
+        else if (mode == 2)                           \
+            launch<Q, false, true>(a, sms, st);       \
+        else                                          \
+            launch<Q, true, true>(a, sms, st);        \
     }
     SFMM_P2P(1)
     SFMM_P2P(2)
     SFMM_P2P(3)
 #undef SFMM_P2P
+    if (a.p2p_split) {
+        k_p2p_reduce<<<blocks_for(a.n_leaves * 32, 256, int64_t(sms) * 16), 256, 0, st>>>(a);
+        SFMM_CHECK_LAUNCH();
+    }
+}
+
+void p2p_setup(Plan& pl)
+{
+    Tree& t = *pl.tree;
+    cudaStream_t st = t.ctx->stream;
+    const int64_t nl = t.n_leaves;
+    pl.p2p_items = 0;
+    pl.p2p_rows = 0;
+    pl.p2p_ctr.alloc(1, st);
+    if (nl == 0) return;
+    pl.p2p_parts.alloc(nl, st);
+    pl.p2p_rowoff.alloc(nl, st);
+    DevBuf<int32_t> rows, psize, nsrc, ioff, tot;
+    rows.alloc(nl, st);
+    psize.alloc(nl, st);
+    nsrc.alloc(nl, st);
+    ioff.alloc(nl, st);
+    tot.alloc(2, st);
+    const unsigned grid = blocks_for(nl * 32, 256, int64_t(t.ctx->sm_count) * 16);
+    k_p2p_cost<<<grid, 256, 0, st>>>(t.nr_ptr.ptr, t.nr.ptr, t.pbeg.ptr, t.pend.ptr, t.leaf_node.ptr, nl,
+                                     pl.p2p_parts.ptr, rows.ptr, psize.ptr, nsrc.ptr);
+    SFMM_CHECK_LAUNCH();
+    exclusive_scan_i32(pl.p2p_parts.ptr, ioff.ptr, nl, st);
+    exclusive_scan_i32(rows.ptr, pl.p2p_rowoff.ptr, nl, st);
+    k_p2p_totals<<<1, 1, 0, st>>>(pl.p2p_parts.ptr, rows.ptr, ioff.ptr, pl.p2p_rowoff.ptr, nl, tot.ptr);
+    SFMM_CHECK_LAUNCH();
+    int32_t h[2] = {0, 0};
+    SFMM_CUDA(cudaMemcpyAsync(h, tot.ptr, sizeof h, cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    pl.p2p_items = h[0];
+    pl.p2p_rows = h[1];
+    pl.p2p_item.alloc(size_t(h[0]), st);
+    pl.p2p_row.alloc(size_t(h[0]), st);
+    if (h[1] > 0) pl.p2p_part.alloc(size_t(h[1]) * (pl.qdim + 3), st);
+    k_p2p_items<<<grid, 256, 0, st>>>(t.nr_ptr.ptr, t.nr.ptr, t.pbeg.ptr, t.pend.ptr, t.leaf_node.ptr, nl,
+                                      pl.p2p_parts.ptr, psize.ptr, nsrc.ptr, ioff.ptr, pl.p2p_rowoff.ptr,
+                                      pl.p2p_item.ptr, pl.p2p_row.ptr);
+    SFMM_CHECK_LAUNCH();
 }
 
 }  // namespace sfmm

@@ -108,6 +108,44 @@ def test_medium_against_restatement(ctx, dist, n, p, ppn):
     assert rel_err_per_target(field[tg], ofield[tg], sfl) < TOL
 
 
+def test_leaf_beside_dense_cluster(ctx):
+    """Coarse leaves whose near field holds every point of a dense cluster
+    (targets x sources far above one work item's share): their near field is
+    summed in parts by several warps and reduced in part order.  All targets
+    against the restatement, twice (the parts' order is fixed, so the two
+    evaluations agree bit for bit), and the mixed form against FP64."""
+    rng = np.random.default_rng(5)
+    pos = np.vstack([0.5 + 0.01 * rng.random((30000, 3)), rng.random((300, 3))])
+    n = pos.shape[0]
+    q = W.charges(n, 5)
+    ot = pyoracle.Tree(pos, 20, 64)
+    d = ot.dump()
+    big = 0
+    for l in range(ot.depth + 1):
+        size = {ll: np.diff(d[f"IDXP{ll}"]) for ll in range(ot.depth + 1)}
+        nl = d[f"NLV{l}"].reshape(-1, 2)
+        ptr = d[f"NLP{l}"]
+        for f in range(len(size[l])):
+            ns = sum(int(size[ll][i]) for ll, i in nl[ptr[f]:ptr[f + 1]])
+            big += int(size[l][f]) * ns > 131072
+    assert big > 0
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    plan = sf.Plan(t, 8, 1)
+    pot, field = np.zeros(n), np.zeros((n, 3))
+    plan.evaluate(q, pot, field)
+    opot, ofield = ot.potential_field(8, q)
+    sp, sfl = pyoracle.error_scales(pos, q)
+    assert rel_err_per_target(pot, opot, sp) < TOL
+    assert rel_err_per_target(field, ofield, sfl) < TOL
+    pot2, field2 = np.zeros(n), np.zeros((n, 3))
+    plan.evaluate(q, pot2, field2)
+    assert np.array_equal(pot, pot2) and np.array_equal(field, field2)
+    mpot, mfield = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, 8, 1, precision="mixed").evaluate(q, mpot, mfield)
+    assert rel_l2(mpot, pot) < 1e-6
+    assert rel_l2(mfield, field) < 1e-6
+
+
 def test_large_plummer_against_direct_sum(ctx):
     """Configuration-size check: N = 4M Plummer, p = 10, leaf 64, against the
     FP64 direct sum on seeded sample targets (truncation error only)."""
