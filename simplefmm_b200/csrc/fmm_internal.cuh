@@ -226,7 +226,7 @@ int64_t tree_export(const Tree& t, int level, int what, void* host_out);
 void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets, int64_t nt,
                 double* pot, double* field);
 
-// scan.cu
+// scan.cu: out[0..n] (n + 1 entries; out[n] is the total)
 void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
 void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
 

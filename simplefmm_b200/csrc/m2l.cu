@@ -933,6 +933,70 @@ __host__ __device__ constexpr int tz_job0(int P, int k)
     return s;
 }
 
+// Inverse-rotation jobs, orders j = P+1..0: the two locals of a large order
+// (LA, LB; RT x KC >= 4 fragments) are separate jobs, a small order is one
+// job for both; order P + 1 has only LB.  part: 0 = LA and LB, 1 = LA, 2 = LB.
+__host__ __device__ constexpr bool inv_split(int P, int j) { return j <= P && mma_rt(j) * mma_kc(j) >= 4; }
+__host__ __device__ constexpr int inv_njobs(int P)
+{
+    int s = 0;
+    for (int j = P + 1; j >= 0; --j) s += inv_split(P, j) ? 2 : 1;
+    return s;
+}
+__host__ __device__ constexpr int inv_job_j(int P, int i)
+{
+    for (int j = P + 1; j >= 0; --j) {
+        const int c = inv_split(P, j) ? 2 : 1;
+        if (i < c) return j;
+        i -= c;
+    }
+    return 0;
+}
+__host__ __device__ constexpr int inv_job_part(int P, int i)
+{
+    for (int j = P + 1; j >= 0; --j) {
+        const int c = inv_split(P, j) ? 2 : 1;
+        if (i < c) return c == 2 ? 1 + i : (j <= P ? 0 : 2);
+        i -= c;
+    }
+    return 0;
+}
+// MMA count of job i of a phase (0: rotation jobs (n, rt), n = P..0;
+// 1: translation jobs (k, rt), k = 0..P+1; 2: inverse-rotation jobs)
+__host__ __device__ constexpr int job_cost(int P, int phase, int i)
+{
+    if (phase == 0) {
+        for (int n = P; n >= 0; --n) {
+            if (i < mma_rt(n)) return 2 * mma_kc(n);
+            i -= mma_rt(n);
+        }
+        return 0;
+    }
+    if (phase == 1) {
+        for (int k = 0; k <= P + 1; ++k) {
+            if (i < tz_rt(P, k)) return tz_kc(P, k) > 0 ? 2 * tz_kc(P, k) : 1;
+            i -= tz_rt(P, k);
+        }
+        return 0;
+    }
+    const int j = inv_job_j(P, i);
+    return mma_rt(j) * mma_kc(j) * (inv_job_part(P, i) == 0 ? 4 : 2);
+}
+// Warp of job i: jobs taken in order, each by the least-loaded warp (the
+// orders come largest first, so this is the longest-processing-time rule).
+__host__ __device__ constexpr int job_warp(int P, int NW, int phase, int i)
+{
+    int load[32] = {};
+    int w = 0;
+    for (int k = 0; k <= i; ++k) {
+        w = 0;
+        for (int u = 1; u < NW; ++u)
+            if (load[u] < load[w]) w = u;
+        load[w] += job_cost(P, phase, k);
+    }
+    return w;
+}
+
 // LEAN: no staging buffer for the moments (the phase-in reads them from
 // global memory) and the potential local's buffer shares X's (X is dead after
 // the rotation; one more barrier between accumulation and the next phase-in),
@@ -1128,7 +1192,8 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                 constexpr int KC = mma_kc(n), base = n * (n + 1) / 2;
                 static_for<0, mma_rt(n)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
-                    if ((rot_job0(P, n) + rt) % NW != warp) return;
+                    constexpr int jw = job_warp(P, NW, 0, rot_job0(P, n) + rt);
+                    if (jw != warp) return;
                     const double* fr = rfc + (mma_foff(n) + rt * KC) * 4 * 32;
                     double aP[KC], aQ[KC];
 #pragma unroll
@@ -1165,7 +1230,8 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                 constexpr int KC = tz_kc(P, k), u0 = az_off(P, k);
                 static_for<0, tz_rt(P, k)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
-                    if ((tz_job0(P, k) + rt) % NW != warp) return;
+                    constexpr int jw = job_warp(P, NW, 1, tz_job0(P, k) + rt);
+                    if (jw != warp) return;
                     const double* fz = a.tzfrag + (tz_foff(P, k) + rt * KC) * 32 + lane;
                     double az[KC > 0 ? KC : 1];
 #pragma unroll
@@ -1209,7 +1275,7 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
             // column table of tile b + 2 (its ring slot is free)
             if (tid < NC && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
             __syncthreads();
-            // ---- inverse rotation + phase, in place: one warp per order j (all its rows)
+            // ---- inverse rotation + phase, in place: jobs (order j, local) take all rows of the order
             {
                 int pc0[NS], pc1[NS];
 #pragma unroll
@@ -1217,11 +1283,13 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                     pc0[q] = M.pidx[8 * q + 2 * lc] * (P + 2);
                     pc1[q] = M.pidx[8 * q + 2 * lc + 1] * (P + 2);
                 }
-                static_for<0, P + 2>([&](auto jj) {
-                    constexpr int j = P + 1 - decltype(jj)::value;
-                    if (decltype(jj)::value % NW != warp) return;
+                static_for<0, inv_njobs(P)>([&](auto jj) {
+                    constexpr int job = decltype(jj)::value;
+                    constexpr int j = inv_job_j(P, job), part = inv_job_part(P, job);
+                    constexpr int jw = job_warp(P, NW, 2, job);
+                    if (jw != warp) return;
                     constexpr int KC = mma_kc(j), RT = mma_rt(j), base = j * (j + 1) / 2;
-                    constexpr bool hasA = j <= P;
+                    constexpr bool hasA = j <= P && part != 2, hasB = part != 1;
                     const double* fr = rfc + mma_foff(j) * 4 * 32;
                     double ar[RT][NS][2] = {}, ai[RT][NS][2] = {}, br[RT][NS][2] = {}, bi[RT][NS][2] = {};
 #pragma unroll
@@ -1236,8 +1304,10 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                         for (int kc = 0; kc < KC; ++kc)
 #pragma unroll
                             for (int q = 0; q < NS; ++q) {
-                                mma884(br[rt][q][0], br[rt][q][1], aPB[kc], Bre[bofs1 + q * 8 * LD1 + base + 4 * kc]);
-                                mma884(bi[rt][q][0], bi[rt][q][1], aQB[kc], Bim[bofs1 + q * 8 * LD1 + base + 4 * kc]);
+                                if constexpr (hasB) {
+                                    mma884(br[rt][q][0], br[rt][q][1], aPB[kc], Bre[bofs1 + q * 8 * LD1 + base + 4 * kc]);
+                                    mma884(bi[rt][q][0], bi[rt][q][1], aQB[kc], Bim[bofs1 + q * 8 * LD1 + base + 4 * kc]);
+                                }
                                 if constexpr (hasA) {
                                     mma884(ar[rt][q][0], ar[rt][q][1], aPB[kc], Are[bofs + q * 8 * LD + base + 4 * kc]);
                                     mma884(ai[rt][q][0], ai[rt][q][1], aQB[kc], Aim[bofs + q * 8 * LD + base + 4 * kc]);
@@ -1254,11 +1324,13 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                         for (int q = 0; q < NS; ++q) {
                             const double2 f0 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc0[q] + m);
                             const double2 f1 = __ldg(reinterpret_cast<const double2*>(a.eil) + pc1[q] + m);
-                            const int b0 = e0 + q * 8 * LD1 + t, b1 = e1 + q * 8 * LD1 + t;
-                            Bre[b0] = f0.x * br[rt][q][0] + f0.y * bi[rt][q][0];
-                            Bim[b0] = f0.x * bi[rt][q][0] - f0.y * br[rt][q][0];
-                            Bre[b1] = f1.x * br[rt][q][1] + f1.y * bi[rt][q][1];
-                            Bim[b1] = f1.x * bi[rt][q][1] - f1.y * br[rt][q][1];
+                            if constexpr (hasB) {
+                                const int b0 = e0 + q * 8 * LD1 + t, b1 = e1 + q * 8 * LD1 + t;
+                                Bre[b0] = f0.x * br[rt][q][0] + f0.y * bi[rt][q][0];
+                                Bim[b0] = f0.x * bi[rt][q][0] - f0.y * br[rt][q][0];
+                                Bre[b1] = f1.x * br[rt][q][1] + f1.y * bi[rt][q][1];
+                                Bim[b1] = f1.x * bi[rt][q][1] - f1.y * br[rt][q][1];
+                            }
                             if constexpr (hasA) {
                                 const int a0 = d0 + q * 8 * LD + t, a1 = d1 + q * 8 * LD + t;
                                 Are[a0] = f0.x * ar[rt][q][0] + f0.y * ai[rt][q][0];

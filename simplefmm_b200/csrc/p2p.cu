@@ -71,13 +71,6 @@ __global__ void k_p2p_cost(const int32_t* __restrict__ nr_ptr, const int2* __res
     }
 }
 
-__global__ void k_p2p_totals(const int32_t* parts, const int32_t* rows, const int32_t* item_off,
-                             const int32_t* row_off, int64_t n, int32_t* tot)
-{
-    tot[0] = item_off[n - 1] + parts[n - 1];
-    tot[1] = row_off[n - 1] + rows[n - 1];
-}
-
 // Warp per leaf: the items of its parts.  Part k starts at source k * S of
 // the leaf's near field; the range holding it is found from a warp prefix
 // sum over 32 ranges at a time.
@@ -609,23 +602,21 @@ void p2p_setup(Plan& pl)
     pl.p2p_ctr.alloc(1, st);
     if (nl == 0) return;
     pl.p2p_parts.alloc(nl, st);
-    pl.p2p_rowoff.alloc(nl, st);
-    DevBuf<int32_t> rows, psize, nsrc, ioff, tot;
+    pl.p2p_rowoff.alloc(nl + 1, st);                    // exclusive scans write n + 1 entries
+    DevBuf<int32_t> rows, psize, nsrc, ioff;
     rows.alloc(nl, st);
     psize.alloc(nl, st);
     nsrc.alloc(nl, st);
-    ioff.alloc(nl, st);
-    tot.alloc(2, st);
+    ioff.alloc(nl + 1, st);
     const unsigned grid = blocks_for(nl * 32, 256, int64_t(t.ctx->sm_count) * 16);
     k_p2p_cost<<<grid, 256, 0, st>>>(t.nr_ptr.ptr, t.nr.ptr, t.pbeg.ptr, t.pend.ptr, t.leaf_node.ptr, nl,
                                      pl.p2p_parts.ptr, rows.ptr, psize.ptr, nsrc.ptr);
     SFMM_CHECK_LAUNCH();
     exclusive_scan_i32(pl.p2p_parts.ptr, ioff.ptr, nl, st);
     exclusive_scan_i32(rows.ptr, pl.p2p_rowoff.ptr, nl, st);
-    k_p2p_totals<<<1, 1, 0, st>>>(pl.p2p_parts.ptr, rows.ptr, ioff.ptr, pl.p2p_rowoff.ptr, nl, tot.ptr);
-    SFMM_CHECK_LAUNCH();
-    int32_t h[2] = {0, 0};
-    SFMM_CUDA(cudaMemcpyAsync(h, tot.ptr, sizeof h, cudaMemcpyDeviceToHost, st));
+    int32_t h[2] = {0, 0};                              // items, rows of partial sums
+    SFMM_CUDA(cudaMemcpyAsync(&h[0], ioff.ptr + nl, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaMemcpyAsync(&h[1], pl.p2p_rowoff.ptr + nl, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
     pl.p2p_items = h[0];
     pl.p2p_rows = h[1];

@@ -158,7 +158,7 @@ void shift_setup(Plan& pl)
     const int64_t base = t.lvl_off[2], n = t.lvl_off[t.depth] - base;
     DevBuf<int32_t> flag;
     flag.alloc(n, st);
-    pl.sh_slot.alloc(n, st);
+    pl.sh_slot.alloc(n + 1, st);                        // exclusive scans write n + 1 entries
     pl.sh_list.alloc(std::max<int64_t>(n, 1), st);
     k_has_children<<<grid_for(n, c.sm_count), 256, 0, st>>>(t.nchild.ptr, base, n, flag.ptr);
     SFMM_CHECK_LAUNCH();

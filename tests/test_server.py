@@ -75,6 +75,29 @@ def test_admission_respects_the_memory_budget():
 
 
 @pytest.mark.gpu
+def test_eight_slots_repeat_the_alone_results():
+    """Eight requests at a time on eight streams, five rounds: every result
+    equals the request's evaluation alone (buffers of concurrent requests
+    are disjoint; an allocation overrun shows up here as a mismatch)."""
+    reqs = _requests(200, 10, 200_000)
+    ctx = sf.Context(0)
+    alone = []
+    for pos, q, p in reqs:
+        t = sf.Tree(pos, 20, 64, ctx=ctx)
+        pot, fld = np.zeros(len(q)), np.zeros((len(q), 3))
+        sf.Plan(t, p, 1).evaluate(q, pot, fld)
+        alone.append((pot, fld))
+    for _ in range(5):
+        srv = sf.Server(0, slots=8, memory_budget=8 << 30)
+        ids = [srv.submit(pos, q, p, leaf=64) for pos, q, p in reqs]
+        for rid, (pot_a, fld_a) in zip(ids, alone):
+            pot, fld, _ = srv.wait(rid)
+            np.testing.assert_allclose(pot, pot_a, rtol=0, atol=TOL * np.abs(pot_a).max())
+            np.testing.assert_allclose(fld, fld_a, rtol=0, atol=TOL * np.abs(fld_a).max())
+        srv.close()
+
+
+@pytest.mark.gpu
 def test_oversize_request_is_rejected_and_autotuned_requests_are_correct():
     srv = sf.Server(0, slots=2, memory_budget=256 << 20)
     big = W.points("uniform", 2_000_000, 5)
