@@ -34,6 +34,7 @@ namespace {
 constexpr int kCB = 4;                    // columns per batch
 constexpr int kMaxGroupPairs = 8 * 189;   // <= 8 siblings x n_ilist_max (partition.hpp:149)
 constexpr int kNumClasses = 70;           // fmm.hpp:169
+constexpr int kTf32MinOrder = 11;         // lowest order at which mixed plans use the TF32 M2L
 
 template<int P>
 struct RowCfg {
@@ -1110,19 +1111,17 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
         }
         cp_async_commit();
     };
-    // X = e^{i m phi} M for tile b, column-major
+    // X = e^{i m phi} M for tile b, column-major: a warp per column, lanes
+    // over its coefficients
     auto phase_in = [&](int b) {
         const Meta& M = meta[b % 3];
         const int ncol = M.ncol;
-        const cplx* xr = Xraw;
-        for (int e = tid; e < NC * T; e += NT) {
-            const int c = e / T, t = e - c * T;
-            if (c < ncol) {
-                const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2) + tm[t]);
-                cplx m;
-                if constexpr (LEAN) m = a.M[(int64_t(M.src[c]) * qd + M.bq[c]) * T + t];
-                else m = xr[e];
-                const cplx v = cmul(cplx{ph.x, ph.y}, m);
+        for (int c = warp; c < ncol; c += NW) {
+            const double2* ph = reinterpret_cast<const double2*>(a.eil) + M.pidx[c] * (P + 2);
+            const cplx* src = LEAN ? a.M + (int64_t(M.src[c]) * qd + M.bq[c]) * T : Xraw + c * T;
+            for (int t = lane; t < T; t += 32) {
+                const double2 f = __ldg(ph + tm[t]);
+                const cplx v = cmul(cplx{f.x, f.y}, src[t]);
                 Xre[c * LD + t] = v.re;
                 Xim[c * LD + t] = v.im;
             }
@@ -2022,7 +2021,10 @@ template<int P>
 void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
     if constexpr (P >= 2) {
-        if (a.mixed && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
+        // mixed plans take the TF32 kernel where it is the faster one (p = 12:
+        // 281 ms against 364 ms on 16M uniform points; p = 10: 92 ms against
+        // 81 ms on 4M Plummer points, where the FP64 kernel runs instead)
+        if (a.mixed && P >= kTf32MinOrder && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
         if (try_launch_mma<P, 1, 8, true>(a, g0, g1, sms, st)) return;
         if (try_launch_mma<P, 1, 8, false>(a, g0, g1, sms, st)) return;
     }
