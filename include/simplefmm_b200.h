@@ -155,7 +155,9 @@ int fmm_plan_capture(fmm_plan* plan, const double* Q, double* pot, double* field
 int fmm_plan_replay(fmm_plan* plan);
 
 /* Device time (ms) of each phase of the last evaluation: [0] P2M+M2M,
-   [1] M2L, [2] L2L+L2P, [3] P2P, [4] total; and of the last tree build [5]. */
+   [1] M2L, [2] L2L+L2P, [3] P2P (it runs on a second stream beside the far
+   field, so [0] + [1] + [2] + [3] can exceed [4]), [4] total; and of the last
+   tree build [5]. */
 int fmm_plan_timings(const fmm_plan* plan, double* ms6);
 
 /* Direct O(n * nt) FP64 sums at nt target indices (the reference's own

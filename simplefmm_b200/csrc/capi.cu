@@ -72,6 +72,10 @@ void release_context(fmm_context* ctx)
     cudaStreamSynchronize(ctx->c.stream);
     sfmm::release_blas(ctx->c);
     cudaStreamSynchronize(ctx->c.stream);
+    if (ctx->c.side) {
+        cudaStreamSynchronize(ctx->c.side);
+        cudaStreamDestroy(ctx->c.side);
+    }
     if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
 }
@@ -122,10 +126,12 @@ int fmm_context_create(int device, fmm_context** out)
         SFMM_CUDA(cudaSetDevice(device));
         SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         ctx->c.own_stream = true;
+        SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.side, cudaStreamNonBlocking));
         SFMM_CUDA(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
         (void)sfmm::device_pool(device);
     } catch (...) {
         if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+        if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
         delete ctx;
         throw;
     }
@@ -327,11 +333,15 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
         pl->pl.qdim = qdim;
         pl->pl.precision = precision;
         for (auto& e : pl->pl.ev) SFMM_CUDA(cudaEventCreate(&e));
+        SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.fork, cudaEventDisableTiming));
+        SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.join, cudaEventDisableTiming));
         sfmm::plan_init(pl->pl);
         SFMM_CUDA(cudaStreamSynchronize(tree->t.ctx->stream));
     } catch (...) {
         for (auto& e : pl->pl.ev)
             if (e) cudaEventDestroy(e);
+        if (pl->pl.fork) cudaEventDestroy(pl->pl.fork);
+        if (pl->pl.join) cudaEventDestroy(pl->pl.join);
         delete pl;
         release_tree(tree);
         throw;
@@ -348,6 +358,8 @@ int fmm_plan_destroy(fmm_plan* plan)
     SFMM_CUDA(cudaStreamSynchronize(plan->pl.tree->ctx->stream));
     for (auto& e : plan->pl.ev)
         if (e) cudaEventDestroy(e);
+    if (plan->pl.fork) cudaEventDestroy(plan->pl.fork);
+    if (plan->pl.join) cudaEventDestroy(plan->pl.join);
     if (plan->pl.graph_exec) cudaGraphExecDestroy(plan->pl.graph_exec);
     if (plan->pl.graph) cudaGraphDestroy(plan->pl.graph);
     fmm_tree* owner = plan->owner;

@@ -472,6 +472,19 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
                                                                pl.src4.ptr, pl.src2.ptr);
     SFMM_CHECK_LAUNCH();
     SFMM_CUDA(cudaMemsetAsync(pl.out.ptr, 0, size_t(t.n) * K * sizeof(double), st));
+    // The near field (P2P) depends only on the points and the gathered charges:
+    // it runs on the context's side stream, issued after the M2L so that the
+    // M2L's blocks are dispatched first and the near field fills the M2L's
+    // tail and the downward pass; the stream joins back before the sums.
+    SFMM_CUDA(cudaEventRecord(pl.fork, st));
+    cudaStream_t side = t.ctx->side ? t.ctx->side : st;
+    auto near_field = [&] {
+        SFMM_CUDA(cudaStreamWaitEvent(side, pl.fork, 0));
+        SFMM_CUDA(cudaEventRecord(pl.ev[6], side));
+        launch_p2p(a, sms, side);
+        SFMM_CUDA(cudaEventRecord(pl.ev[7], side));
+        SFMM_CUDA(cudaEventRecord(pl.join, side));
+    };
     const bool far = t.depth >= 2;
     if (far) {
         const int64_t nfar = t.n_leaves - a.far_leaf0;
@@ -495,6 +508,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         }
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
         launch_m2l(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
+        near_field();
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
         const size_t head2 = (32 + 2 * 4 * (2 * kMaxOrder + 1) + 2 * 4 * (2 * kMaxOrder + 3)) * sizeof(double);
         const size_t sm_l2l_w = size_t(qd) * (T + T1) * sizeof(cplx);
@@ -516,10 +530,11 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
         SFMM_CHECK_LAUNCH();
     } else {
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
+        near_field();
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
     }
     SFMM_CUDA(cudaEventRecord(pl.ev[3], st));
-    launch_p2p(a, sms, st);
+    SFMM_CUDA(cudaStreamWaitEvent(st, pl.join, 0));
     SFMM_CUDA(cudaEventRecord(pl.ev[4], st));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
     SFMM_CHECK_LAUNCH();
@@ -537,7 +552,7 @@ void plan_read_timings(Plan& pl, double* ms6)
     ms6[1] = v;
     SFMM_CUDA(cudaEventElapsedTime(&v, pl.ev[2], pl.ev[3]));
     ms6[2] = v;
-    SFMM_CUDA(cudaEventElapsedTime(&v, pl.ev[3], pl.ev[4]));
+    SFMM_CUDA(cudaEventElapsedTime(&v, pl.ev[6], pl.ev[7]));      // near field, on the side stream
     ms6[3] = v;
     SFMM_CUDA(cudaEventElapsedTime(&v, pl.ev[0], pl.ev[5]));
     ms6[4] = v;

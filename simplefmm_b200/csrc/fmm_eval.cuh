@@ -129,7 +129,10 @@ struct Plan {
     DevBuf<int32_t> sh_slot, sh_list;
     std::vector<int32_t> sh_S;
     DevBuf<float2> m32;                       // mixed precision: scaled FP32 source moments
-    cudaEvent_t ev[6] = {};
+    // timing: evaluation start, far field (upward, M2L, downward) ends, end;
+    // ev[6] / ev[7] bracket the near field on the side stream
+    cudaEvent_t ev[8] = {};
+    cudaEvent_t fork = nullptr, join = nullptr;   // side stream: start after the charges, join before the sums
     // one captured evaluation (fmm_plan_capture / fmm_plan_replay)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;

@@ -164,6 +164,9 @@ struct Context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t side = nullptr;          // the library's second stream: the near field runs
+                                          // on it beside the far field (forked from and joined
+                                          // back into `stream` with events)
     int sm_count = 148;
     void* blas = nullptr;                 // cuBLAS handle of the M2M / L2L products (shift.cu)
     void* blas_ws = nullptr;              // its fixed workspace
