@@ -910,6 +910,17 @@ __device__ __forceinline__ void static_for(F&& f)
     }
 }
 
+// Runs f(std::integral_constant<int, W>) for the calling warp's index W, so
+// that a stage's job list is filtered at compile time (each job's code sits
+// in the branch of the one warp that runs it).
+template<int NW, typename F>
+__device__ __forceinline__ void for_warp(int warp, F&& f)
+{
+    static_for<0, NW>([&](auto ww) {
+        if (warp == decltype(ww)::value) f(ww);
+    });
+}
+
 // padded leading dimension of a [col][row] operand buffer: >= rows + 4 (K
 // chunks read up to 3 rows past an order) and = 4 or 12 mod 16 doubles, which
 // makes the B-fragment loads (4 rows x 8 columns) bank-conflict free
@@ -1186,13 +1197,15 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
             // tile b + 1's moments: the staging buffer is free since phase_in(b)
             if (b + 1 < nbat) issue(b + 1);
             // ---- rotation: jobs (n, rt), largest orders first, round robin over warps
+            for_warp<NW>(warp, [&](auto ww) {
+            constexpr int W = decltype(ww)::value;
             static_for<0, P + 1>([&](auto nn) {
                 constexpr int n = P - decltype(nn)::value;
                 constexpr int KC = mma_kc(n), base = n * (n + 1) / 2;
                 static_for<0, mma_rt(n)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
                     constexpr int jw = job_warp(P, NW, 0, rot_job0(P, n) + rt);
-                    if (jw != warp) return;
+                    if (jw != W) return;
                     const double* fr = rfc + (mma_foff(n) + rt * KC) * 4 * 32;
                     double aP[KC], aQ[KC];
 #pragma unroll
@@ -1222,15 +1235,18 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                     }
                 });
             });
+            });
             __syncthreads();
             // ---- z-translation: jobs (k, rt); the same operator for re and im
+            for_warp<NW>(warp, [&](auto ww) {
+            constexpr int W = decltype(ww)::value;
             static_for<0, P + 2>([&](auto kk) {
                 constexpr int k = decltype(kk)::value;
                 constexpr int KC = tz_kc(P, k), u0 = az_off(P, k);
                 static_for<0, tz_rt(P, k)>([&](auto rr) {
                     constexpr int rt = decltype(rr)::value;
                     constexpr int jw = job_warp(P, NW, 1, tz_job0(P, k) + rt);
-                    if (jw != warp) return;
+                    if (jw != W) return;
                     const double* fz = a.tzfrag + (tz_foff(P, k) + rt * KC) * 32 + lane;
                     double az[KC > 0 ? KC : 1];
 #pragma unroll
@@ -1271,6 +1287,7 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                     }
                 });
             });
+            });
             // column table of tile b + 2 (its ring slot is free)
             if (tid < NC && b + 2 < nbat) make_meta(b + 2, tid, meta[(b + 2) % 3], cur);
             __syncthreads();
@@ -1282,11 +1299,13 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                     pc0[q] = M.pidx[8 * q + 2 * lc] * (P + 2);
                     pc1[q] = M.pidx[8 * q + 2 * lc + 1] * (P + 2);
                 }
+                for_warp<NW>(warp, [&](auto ww) {
+                constexpr int W = decltype(ww)::value;
                 static_for<0, inv_njobs(P)>([&](auto jj) {
                     constexpr int job = decltype(jj)::value;
                     constexpr int j = inv_job_j(P, job), part = inv_job_part(P, job);
                     constexpr int jw = job_warp(P, NW, 2, job);
-                    if (jw != warp) return;
+                    if (jw != W) return;
                     constexpr int KC = mma_kc(j), RT = mma_rt(j), base = j * (j + 1) / 2;
                     constexpr bool hasA = j <= P && part != 2, hasB = part != 1;
                     const double* fr = rfc + mma_foff(j) * 4 * 32;
@@ -1339,6 +1358,7 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
                             }
                         }
                     }
+                });
                 });
             }
             cp_async_wait_all();                          // tile b + 1's moments
