@@ -365,6 +365,7 @@ void plan_init(Plan& pl)
     if (pl.precision == FMM_PRECISION_MIXED) pl.m32.alloc(size_t(t.n_nodes) * pl.qdim * pl.T, st);
     shift_setup(pl);
     p2p_setup(pl);
+    pl.m2l_ctr.alloc(1, st);
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     if (pl.precision == FMM_PRECISION_FP64) {
@@ -458,6 +459,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.p2p_rowoff = pl.p2p_rowoff.ptr;
     a.p2p_part = pl.p2p_part.ptr;
     a.p2p_ctr = pl.p2p_ctr.ptr;
+    a.m2l_ctr = pl.m2l_ctr.ptr;
     a.p2p_split = pl.p2p_rows > 0;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;

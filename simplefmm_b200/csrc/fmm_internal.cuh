@@ -55,7 +55,10 @@ inline void allow_max_smem(KernelT k)
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, optin));
+    cudaFuncAttributes fa{};
+    SFMM_CUDA(cudaFuncGetAttributes(&fa, k));                 // static + dynamic <= opt-in limit
+    SFMM_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   optin - static_cast<int>(fa.sharedSizeBytes)));
 }
 
 // ------------------------------------------------------------------ device memory

@@ -1139,7 +1139,17 @@ __global__ void __launch_bounds__(32 * NW, NW <= 8 ? (LEAN ? 4 : 3) : 1) k_m2l_m
         }
     };
 
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+    // blocks take sibling groups from a counter (group costs vary with the
+    // children's interaction lists; the resident blocks stay busy to the end)
+    __shared__ int64_t next_group;
+    auto take = [&]() -> int64_t {
+        if (tid == 0) next_group = g0 + atomicAdd(a.m2l_ctr, 1);
+        __syncthreads();
+        const int64_t g = next_group;
+        __syncthreads();
+        return g;
+    };
+    for (int64_t g = take(); g < g1; g = take()) {
         const int nc = a.nchild[g];
         if (nc == 0) continue;
         const int cb = a.child_beg[g];
@@ -1405,13 +1415,16 @@ bool try_launch_mma(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStre
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > size_t(optin)) return false;
+    cudaFuncAttributes fa{};
+    SFMM_CUDA(cudaFuncGetAttributes(&fa, k_m2l_mma<P, NS, NW, LEAN>));
+    if (smem + fa.sharedSizeBytes > size_t(optin)) return false;
     allow_max_smem(k_m2l_mma<P, NS, NW, LEAN>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_mma<P, NS, NW, LEAN>, 32 * NW, smem));
     if (LEAN && per_sm < 4) return false;
     if (per_sm < 1) return false;
-    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm);
+    SFMM_CUDA(cudaMemsetAsync(a.m2l_ctr, 0, sizeof(int), st));
     k_m2l_mma<P, NS, NW, LEAN><<<static_cast<unsigned>(grid), 32 * NW, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
     return true;
