@@ -1705,7 +1705,16 @@ __global__ void __launch_bounds__(256, 4) k_m2l_tf32(EvalArgs a, int64_t g0, int
         }
     };
 
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
+    // blocks take sibling groups from a counter, as in k_m2l_mma
+    __shared__ int64_t next_group;
+    auto take = [&]() -> int64_t {
+        if (tid == 0) next_group = g0 + atomicAdd(a.m2l_ctr, 1);
+        __syncthreads();
+        const int64_t g = next_group;
+        __syncthreads();
+        return g;
+    };
+    for (int64_t g = take(); g < g1; g = take()) {
         const int nc = a.nchild[g];
         if (nc == 0) continue;
         const int cb = a.child_beg[g];
@@ -1961,7 +1970,9 @@ bool try_launch_tf32(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStr
     int dev = 0, optin = 0;
     SFMM_CUDA(cudaGetDevice(&dev));
     SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > size_t(optin)) return false;
+    cudaFuncAttributes fa{};
+    SFMM_CUDA(cudaFuncGetAttributes(&fa, k_m2l_tf32<P>));
+    if (smem + fa.sharedSizeBytes > size_t(optin)) return false;
     allow_max_smem(k_m2l_tf32<P>);
     int per_sm = 0;
     SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_tf32<P>, 256, smem));
@@ -1971,7 +1982,8 @@ bool try_launch_tf32(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStr
     k_m32<<<static_cast<unsigned>(std::min<int64_t>((n1 - n0) * a.qdim * a.T / 256 + 1, int64_t(sms) * 16)), 256, 0, st>>>(a, n0,
                                                                                                                         n1);
     SFMM_CHECK_LAUNCH();
-    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
+    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm);
+    SFMM_CUDA(cudaMemsetAsync(a.m2l_ctr, 0, sizeof(int), st));
     k_m2l_tf32<P><<<static_cast<unsigned>(grid), 256, smem, st>>>(a, g0, g1);
     SFMM_CHECK_LAUNCH();
     return true;
