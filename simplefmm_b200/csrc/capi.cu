@@ -76,6 +76,10 @@ void release_context(fmm_context* ctx)
         cudaStreamSynchronize(ctx->c.side);
         cudaStreamDestroy(ctx->c.side);
     }
+    if (ctx->c.retired) {
+        cudaStreamSynchronize(ctx->c.retired);
+        cudaStreamDestroy(ctx->c.retired);
+    }
     if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
 }
@@ -152,7 +156,7 @@ int fmm_context_set_stream(fmm_context* ctx, void* stream)
     if (!ctx) return fail(FMM_ERR_INVALID_ARGUMENT, "ctx is NULL");
     bind(ctx->c);
     SFMM_CUDA(cudaStreamSynchronize(ctx->c.stream));
-    if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
+    if (ctx->c.own_stream) ctx->c.retired = ctx->c.stream;   // destroyed with the context
     ctx->c.stream = static_cast<cudaStream_t>(stream);
     ctx->c.own_stream = false;
     API_CATCH

@@ -46,3 +46,33 @@ def test_blocks_of_other_sizes_after_reuse():
         tg = np.random.default_rng(32).choice(n, 500, replace=False)
         dpot, _ = sf.direct(pos, q, tg, ctx=a)
         assert np.linalg.norm(pot[tg] - dpot) / np.linalg.norm(dpot) < 1e-4
+
+
+@pytest.mark.gpu
+def test_work_queued_after_an_evaluation_on_the_caller_stream_sees_the_result():
+    """The near field runs on the context's second stream; it joins back into
+    the caller's stream before the sums, so a kernel the caller queues on its
+    stream right after fmm_evaluate reads the finished result (no host sync)."""
+    import torch
+    n = 200_000
+    pos = W.points("plummer", n, 13)
+    q = W.charges(n, 13)
+    ctx = sf.Context(0)
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    plan = sf.Plan(t, 8, 1)
+    pot_ref, fld_ref = np.zeros(n), np.zeros((n, 3))
+    plan.evaluate(q, pot_ref, fld_ref)
+    s = torch.cuda.Stream()
+    ctx.set_stream(s.cuda_stream)
+    with torch.cuda.stream(s):
+        qd = torch.tensor(q, device="cuda")
+        pot = torch.zeros(n, dtype=torch.float64, device="cuda")
+        fld = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    s.synchronize()
+    plan.evaluate(qd, pot, fld)
+    with torch.cuda.stream(s):
+        copy_pot = pot * 1.0
+        copy_fld = fld * 1.0
+    s.synchronize()
+    assert np.array_equal(copy_pot.cpu().numpy(), pot_ref)
+    assert np.array_equal(copy_fld.cpu().numpy(), fld_ref)
