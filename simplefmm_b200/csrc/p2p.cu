@@ -2,11 +2,13 @@
 // its neighbour-list point ranges, with the reference's self exclusion
 // (is_self: i == j, fmm.hpp:786, 880).
 //
-// Warp per target leaf.  Sources are packed records (x y z q0 | q1 q2, leaf
-// order) and a leaf's near-field ranges are staged into full shared tiles of
+// Warp per work item: a leaf's targets against all of its near field, or,
+// for a leaf with a large near field, against one part of it (work items
+// below).  Sources are packed records (x y z q0 | q1 q2, leaf
+// order) and an item's near-field ranges are staged into full shared tiles of
 // kChunk sources by asynchronous 16-byte copies, two tiles per warp: the
 // copies of tile c + 1 are in flight while tile c is summed, so the gathers'
-// L2 / DRAM latency hides behind the arithmetic.  The leaf's ranges are read
+// L2 / DRAM latency hides behind the arithmetic.  The item's ranges are read
 // 32 at a time into registers (lane k holds range k) and walked with
 // shuffles.  Lanes are (target group, source slice): tg targets per pass and
 // 32/tg slices, with tg chosen per leaf so that at most kMaxPass passes cover
