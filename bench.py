@@ -16,7 +16,8 @@ point.  Metric: points/s = N / (tree build + evaluation time).
 --gpus N runs N independent replicas (one process per GPU, launched by
 torch.distributed.run); value = all points / max-over-ranks time.
 --impl reference times the reference's own CPU implementation (the compiled
-reference headers, run as one shim rank per host core) on a bounded sample.
+reference headers, run as one shim rank per host core) on the same workload:
+one full solve (minutes on the host cores), whatever --steps/--warmup say.
 """
 from __future__ import annotations
 
@@ -41,11 +42,51 @@ SEED = 2024
 
 
 def f_m2l(p: int) -> int:
-    """Algorithmic FLOPs of one M2L pair and component of the reference's
-    rotation scheme: 8 n_rot + 4 T_z + 16 (p+1)^2."""
+    """The reference's operation count of one M2L pair and charge component
+    of its rotation scheme (fmm.hpp:620-688): 8 n_rot + 4 T_z + 16 (p+1)^2.
+    The reference runs it for 4 components (potential + two gradient runs of
+    3); reported as frac_ref_ops only."""
     n_rot = (p + 1) * (2 * p + 1) * (2 * p + 3) // 3
     t_z = sum((p + 1 - abs(k)) ** 2 for k in range(-p, p + 1))
     return 8 * n_rot + 4 * t_z + 16 * (p + 1) ** 2
+
+
+def m2l_useful_flops(p: int) -> int:
+    """FP64 operations the M2L kernel must execute per ilist pair (scalar
+    charges, potential + field), counted on the nonzero operator entries of
+    its formulation: rotation of the order-p multipole (orders n <= p, real
+    (n+1)^2 blocks on the re and im parts), z-translation into the field
+    local (target orders <= p+1, source orders <= p-1) plus the potential
+    local's order-p source column, inverse rotation of both locals (orders
+    <= p and <= p+1), the phase factors in and out (complex products) and the
+    additions into the targets."""
+    T, T1 = (p + 1) * (p + 2) // 2, (p + 2) * (p + 3) // 2
+    rot = 2 * sum((n + 1) ** 2 for n in range(p + 1))
+    tz = 2 * (sum((p + 2 - k) * (p - k) for k in range(p)) + sum(p + 1 - k for k in range(p + 1)))
+    inv = 2 * sum((j + 1) ** 2 for j in range(p + 1)) + 2 * sum((j + 1) ** 2 for j in range(p + 2))
+    return 2 * (rot + tz + inv) + 6 * T + 6 * (T + T1) + 2 * (T + T1)
+
+
+def m2l_mma_flops(p: int) -> int:
+    """FP64 tensor-core operations the M2L kernel (k_m2l_mma) issues per
+    ilist pair: its compile-time MMA schedule for one 8-column tile (8x8x4
+    DMMA, 512 flops each, zero-padded operator fragments) over 8 columns."""
+    rt = lambda n: (n + 8) // 8  # noqa: E731
+    kc = lambda n: (n + 4) // 4  # noqa: E731
+    rot = sum(2 * rt(n) * kc(n) for n in range(p + 1))
+    tz = sum(((p + 2 - k + 7) // 8) * 2 * ((p - k + 3) // 4 if k < p else 0) for k in range(p + 2))
+    inv = sum(rt(j) * kc(j) * 2 * (1 if j == p + 1 else 2) for j in range(p + 2))
+    return (rot + tz + inv) * 512 // 8
+
+
+def measured_peaks() -> tuple[dict, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        try:
+            return json.loads(f.read_text()), "measured (MEASURED_PEAKS.json)"
+        except ValueError:
+            pass
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback (earlier measurement on this pool)"
 
 
 def host_cores() -> int:
@@ -135,63 +176,91 @@ DATA_DESC = {
 }
 
 
-def traffic_per_pair():
-    """DRAM bytes per M2L pair from the committed ncu summary, if present."""
-    f = ROOT / "profiles" / "m2l_fp64_plummer.md"
-    if not f.exists():
-        return None
-    for line in f.read_text().splitlines():
-        if line.startswith("dram_bytes_per_pair:"):
-            return float(line.split(":")[1])
-    return None
-
-
-def cpu_baseline(n_sample: int, p: int, steps: int = 1):
-    """Reference CPU implementation (compiled reference headers) on a bounded
-    sample of the workload, one shim rank per host core."""
+def reference_solve(pos, q, p: int, cores: int):
+    """One solve of the reference's own CPU implementation (the compiled,
+    unmodified reference headers: tree + FMM3D set-up + rinv for the
+    potential, FMM3D<3, grad> set-up + two rinv<true> runs for the field),
+    as `cores` shim ranks (mpirun -n cores).  Returns (seconds, phases)."""
     from oracle import refio
 
+    out = refio.run_reference(pos, q, p=p, max_level=20, max_ppn=LEAF,
+                              flags=refio.FLAG_POT | refio.FLAG_FIELD, ranks=cores, timeout=1800)
+    ph = {k: out[k] for k in ("T_TREE", "T_CTOR1", "T_POT", "T_CTOR3G", "T_FIELD")}
+    return sum(ph.values()), ph
+
+
+def cpu_baseline(dist: str, n_sample: int, p: int, steps: int = 1):
+    """The reference's CPU implementation on a bounded sample of the workload
+    (the first n_sample points of the same seeded distribution), one shim
+    rank per host core; the oracle's restatement on 1 core if the compiled
+    reference is absent."""
+    from oracle import refio
+    from simplefmm_b200 import workloads as W
+
     cores = host_cores()
-    pos = __import__("simplefmm_b200.workloads", fromlist=["x"]).plummer(n_sample, SEED + 1)
-    q = __import__("simplefmm_b200.workloads", fromlist=["x"]).charges(n_sample, SEED + 1)
+    pos = W.points(dist, n_sample, SEED + 1)
+    q = W.charges(n_sample, SEED + 1)
     kind = "reference"
+    vals = []
     if refio.have_reference():
-        vals = []
         for _ in range(steps):
-            out = refio.run_reference(pos, q, p=p, max_level=20, max_ppn=LEAF,
-                                      flags=refio.FLAG_POT | refio.FLAG_FIELD, ranks=cores)
-            t = out["T_TREE"] + out["T_CTOR1"] + out["T_POT"] + out["T_CTOR3G"] + out["T_FIELD"]
+            t, _ = reference_solve(pos, q, p, cores)
             vals.append(n_sample / t)
     else:
         from oracle import pyoracle
         kind, cores = "port", 1
-        vals = []
         for _ in range(steps):
             t0 = time.perf_counter()
             tr = pyoracle.Tree(pos, 20, LEAF)
             tr.potential_field(p, q)
             vals.append(n_sample / (time.perf_counter() - t0))
     return vals, {"unit": "points/s", "cores": cores, "kind": kind,
-                  "sample": f"Plummer N={n_sample} (seed {SEED + 1}), p={p}, leaf {LEAF}, potential + field "
+                  "sample": f"{dist} N={n_sample} (seed {SEED + 1}), p={p}, leaf {LEAF}, potential + field "
                             f"(tree + FMM3D set-up + rinv, field via two rinv<true> runs)"}
 
 
 def run_reference_arm(args):
+    """The reference's own CPU implementation on this arm's workload: the same
+    seeded points and charges, N, p and leaf size, potential + field.  A full
+    solve of the 4M-point workload takes minutes on the host cores, so one
+    solve is timed whatever --steps / --warmup say (steps_run in the line)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    n_sample = args.ref_sample
-    vals, info = cpu_baseline(n_sample, args.p, steps=args.warmup + args.steps)
-    timed = vals[args.warmup:] or vals
-    v = statistics.median(timed)
+    from oracle import refio
+    from simplefmm_b200 import workloads as W
+
+    cores = host_cores()
+    n = args.ref_sample or args.n
+    if not refio.have_reference():
+        print(json.dumps({"impl": "reference", "unavailable": "compiled reference (oracle/_ref/ref_driver) not built"}),
+              flush=True)
+        return
+    pos = W.points(args.dist, n, SEED)
+    q = W.charges(n, SEED)
+    t0 = time.perf_counter()
+    t, ph = reference_solve(pos, q, args.p, cores)
+    wall = time.perf_counter() - t0
+    v = n / t
+    same = n == args.n
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "points/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Plummer sphere, a=1, r<=10; charges U[-1,1])",
-            "config": {"workload": f"plummer_p{args.p}_leaf{LEAF}_fp64_potential+field (bounded CPU sample)",
-                       "n": n_sample, "p": args.p, "leaf": LEAF},
-            "cpu_baseline": dict(info, value=v),
+            "steps": 1, "warmup": 0, "steps_run": 1, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA_DESC.get(args.dist, args.dist),
+            "config": workload_config(args, n, 1),
+            "same_config": same,
+            "note": ("one full solve timed (a solve of this workload takes minutes on the host cores), "
+                     "ignoring --steps/--warmup" if same else f"bounded sample of {n} points"),
+            "reference_phases_s": ph, "wall_s": wall,
+            "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "reference",
+                             "sample": f"the full workload ({n} points), one solve as {cores} shim ranks"},
             "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def workload_config(args, n: int, world: int) -> dict:
+    return {"workload": f"{args.dist}_n{n}_p{args.p}_leaf{LEAF}_{args.precision}_potential+field", "n": n,
+            "p": args.p, "leaf": LEAF, "distribution": args.dist, "precision": args.precision,
+            "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps"}
 
 
 def serve_bench(args):
@@ -292,7 +361,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--p", type=int, default=P_DEFAULT)
     ap.add_argument("--dist", default="plummer")
-    ap.add_argument("--ref-sample", type=int, default=100_000)
+    ap.add_argument("--ref-sample", type=int, default=0,
+                    help="reference arm: points of a bounded sample (0 = the full workload)")
+    ap.add_argument("--cpu-sample", type=int, default=100_000, help="cpu_baseline leg: points of its bounded sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
@@ -389,12 +460,21 @@ def main():
     err_fld = float(np.linalg.norm(fld_h[tg] - dfld) / np.linalg.norm(dfld))
 
     stats = tree.stats()
-    K = 4
-    flops_launch = stats["ilist_pairs"] * K * f_m2l(p)
     m2l_avg = statistics.mean(m2l_ms)
-    achieved = flops_launch / (m2l_avg * 1e-3) / 1e12
+    pairs = stats["ilist_pairs"]
+    useful = pairs * m2l_useful_flops(p)                # per launch
+    achieved = useful / (m2l_avg * 1e-3) / 1e12
     peak = fp64_peak_tflops(torch)
-    tpp = traffic_per_pair()
+    peaks, peaks_src = measured_peaks()
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    T, T1 = (p + 1) * (p + 2) // 2, (p + 2) * (p + 3) // 2
+    # M2L bytes that must cross HBM at least once per launch: every node's
+    # moments read, both locals of every node written, the ilist entries read
+    m2l_bytes = stats["nodes"] * 16 * (T + T + T1) + 8 * pairs
+    build = {}
+    for name, (ms, by) in tree.build_phases().items():
+        gbs = by / (ms * 1e-3) / 1e9 if ms > 0 else None
+        build[name] = {"ms": round(ms, 4), "bytes": int(by), "gbs": gbs, "frac_hbm": gbs / hbm if gbs else None}
 
     e2e = None
     if not args.no_e2e:
@@ -422,7 +502,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        vals, info = cpu_baseline(args.ref_sample, p)
+        vals, info = cpu_baseline(args.dist, args.cpu_sample, p)
         cpu = dict(info, value=statistics.median(vals))
 
     if rank == 0:
@@ -432,19 +512,29 @@ def main():
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
             "data": DATA_DESC.get(args.dist, f"synthetic (seeded {args.dist})"),
-            "config": {"workload": f"{args.dist}_n{n}_p{p}_leaf{LEAF}_{args.precision}_potential+field", "n": n,
-                       "p": p, "leaf": LEAF, "distribution": args.dist, "precision": args.precision,
-                       "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps",
-                       "depth": tree.depth, **stats},
+            "config": workload_config(args, n, world),
+            "tree": {"depth": tree.depth, **stats},
             "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": n_check},
             "phases_ms": {k: round(statistics.mean(ph[k] for ph in phases), 3) for k in phases[0]},
             "step_ms": [round(x, 3) for x in times],
             "tree_ms_per_step": [round(ph["tree_ms"], 3) for ph in phases],
-            "roofline": {"bound": "fp64", "kernel": "k_m2l", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak,
-                         "peak_source": "FP64 DGEMM (torch float64 matmul 8192^3) measured in this run",
-                         "work": f"ilist pairs x 4 components x F(p)={f_m2l(p)} algorithmic FLOPs per launch",
-                         "traffic": (tpp * stats["ilist_pairs"]) if tpp else None},
+            "tree_build_phases": dict(build, peak_hbm_gbs=hbm, peak_source=peaks_src,
+                                      work="algorithmic bytes of each phase (fmm_tree_build_phases) / its device time"),
+            "roofline": {"bound": "tensor", "pipe": "FP64 tensor cores (DMMA 8x8x4)", "kernel": "k_m2l_mma",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_source": "FP64 DGEMM (torch float64 matmul 8192^3, cuBLAS DMMA) measured in this run; "
+                                        "MEASURED_PEAKS.json has no FP64 figure",
+                         "work": f"ilist pairs x {m2l_useful_flops(p)} useful FP64 flops per pair (nonzero operator "
+                                 f"entries of rotate / translate / rotate back, phases, sums), per launch "
+                                 f"{useful:.4g} flops; time = mean CUDA-event M2L phase",
+                         "frac_mma": pairs * m2l_mma_flops(p) / (m2l_avg * 1e-3) / 1e12 / peak,
+                         "mma_flops_per_pair": m2l_mma_flops(p),
+                         "frac_ref_ops": pairs * 4 * f_m2l(p) / (m2l_avg * 1e-3) / 1e12 / peak,
+                         "ref_ops_per_pair": 4 * f_m2l(p),
+                         "traffic": None,
+                         "traffic_model_bytes": m2l_bytes,
+                         "traffic_note": "measured DRAM bytes per launch come from an ncu capture (profiles/), "
+                                         "not from this run"},
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(launches),

@@ -83,7 +83,12 @@ const char* fmm_version(void);
 /* Create a context on `device` with its own stream. */
 int fmm_context_create(int device, fmm_context** out);
 int fmm_context_destroy(fmm_context* ctx);
-/* Use the caller's stream (a cudaStream_t) for all work of this context. */
+/* Use the caller's stream (a cudaStream_t) for all work of this context.
+   The call first waits for the context's current stream.  Device buffers of
+   trees and plans are released in stream order on the stream they were
+   allocated on: a caller stream set earlier must outlive the trees and plans
+   built while it was set (the context's own stream lives as long as the
+   context). */
 int fmm_context_set_stream(fmm_context* ctx, void* stream);
 int fmm_context_synchronize(fmm_context* ctx);
 /* Page-lock host memory so host<->device copies run at full speed. */
@@ -117,6 +122,14 @@ int fmm_tree_export(const fmm_tree* tree, int level, int what, void* host_out);
 /* Total element counts of the device lists: [0] nodes, [1] leaves, [2] ilist
    pairs, [3] near-field point pairs (self excluded), [4] near-field ranges. */
 int fmm_tree_stats(const fmm_tree* tree, int64_t* stats5);
+/* Device time (ms) of the phases of the tree build -- [0] root cube and
+   Morton keys, [1] refinement (the subdivision of partition.hpp:47-104, level
+   by level), [2] leaves and points in leaf order, [3] same-level neighbours,
+   [4] interaction lists, [5] near-field lists -- and, if bytes6 is not NULL,
+   the device-memory bytes each phase must move at least once (its
+   algorithmic traffic), for achieved-bandwidth figures.  No counterpart in
+   the reference (its tree build is timed as one step). */
+int fmm_tree_build_phases(const fmm_tree* tree, double* ms6, double* bytes6);
 
 /* FMM3D<double, qdim, p, Vector, support_gradient>(partitioner, comm):
    fmm.hpp:204-427.  Builds the operator tables for order p (0..16) and
@@ -163,7 +176,9 @@ int fmm_plan_timings(const fmm_plan* plan, double* ms6);
 /* Direct O(n * nt) FP64 sums at nt target indices (the reference's own
    accuracy check, main.cpp:70-111): pot (nt x qdim) = sum_{j != i} Q_j/|R|,
    field (nt x 3) = sum_j q_j R/|R|^3 (qdim 1) or sum_j Q_j x R/|R|^3 (qdim 3).
-   Outputs are overwritten.  Synchronous. */
+   Outputs are overwritten.  Synchronous.  A target index outside [0, n)
+   returns FMM_ERR_INVALID_ARGUMENT (checked before any copy for FMM_HOST,
+   on the device for FMM_DEVICE: nothing out of range is read). */
 int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
                int64_t nt, double* pot, double* field, int where);
 
@@ -177,6 +192,9 @@ int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, 
    call until the process exits; the first call on a device looks up its
    address (set-up), so make that first call before any stream capture.
    Limit: nt <= 174762 targets per call (FMM_ERR_OVER_BUDGET above it).
+   The call cannot wait for the GPU, so a target index outside [0, n) is not
+   reported by the status: nothing out of range is read and that target's
+   outputs are NaN.
    Every call shares the array: calls that overlap on the GPU (other streams,
    other host threads) race and corrupt each other's results. */
 int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets,
@@ -186,7 +204,7 @@ int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q, int qdim, 
    problem per call).  Solves of different N, p and precision are submitted
    as they arrive and run concurrently on one device: `slots` workers, each
    with its own stream, admit queued requests in arrival order as a slot and
-   `memory_budget` bytes of (estimated) device memory become free, so the
+   `memory_budget` bytes of estimated device memory become free, so the
    kernels of admitted requests overlap.  A request keeps its host pointers
    (xyz, Q, pot, field) until fmm_server_wait returns; pot / field are
    accumulated as by fmm_evaluate.  max_particles_per_node = 0 lets the
@@ -205,6 +223,15 @@ int fmm_server_wait(fmm_server* server, int64_t id, double* latency_ms);
    latency ms, [4] most requests running at once, [5] most budgeted bytes in
    use at once, [6] budget bytes, [7] requests queued now. */
 int fmm_server_stats(fmm_server* server, double* stats8);
+/* Measured device memory: [0] peak of the bytes allocated at once by the
+   running requests (every device allocation of their tree, plan and
+   evaluation, metered on the worker threads; the workers return freed blocks
+   to the pool rather than to the library's block cache), [1] budget bytes,
+   [2] largest ratio of a completed request's measured peak to the estimate
+   that admission used for it.  Shared operator tables (one copy per device,
+   p and precision, built by the first request that needs them) count toward
+   that request. */
+int fmm_server_memory(fmm_server* server, double* out3);
 
 /* Number of kernels this library has launched in this process. */
 int fmm_launch_count(int64_t* count);

@@ -98,7 +98,7 @@ struct Job {
 
 // per-p evaluation entry points (one translation unit per p, see Makefile)
 #define DECL(P) void run_p##P(const Job&, const Part&, Out&, int rank);
-DECL(2) DECL(3) DECL(4) DECL(5) DECL(6) DECL(7) DECL(8) DECL(9) DECL(10) DECL(11) DECL(12)
+DECL(2) DECL(3) DECL(4) DECL(5) DECL(6) DECL(7) DECL(8) DECL(9) DECL(10) DECL(11) DECL(12) DECL(13) DECL(16)
 #undef DECL
 
 template<int p>
@@ -335,7 +335,8 @@ int main(int argc, char** argv)
     if (!(job.flags & 32)) {
         switch (job.p) {
 #define CASE(P) case P: run_p##P(job, part, out, rank); break;
-            CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) CASE(11) CASE(12)
+            CASE(2) CASE(3) CASE(4) CASE(5) CASE(6) CASE(7) CASE(8) CASE(9) CASE(10) CASE(11) CASE(12) CASE(13)
+            CASE(16)
 #undef CASE
         default:
             if (rank == 0) std::fprintf(stderr, "unsupported p=%d\n", job.p);

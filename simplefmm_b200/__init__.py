@@ -69,6 +69,7 @@ def load_library():
         "fmm_tree_export_size": ([vp, i32, i32, C.POINTER(i64)], i32),
         "fmm_tree_export": ([vp, i32, i32, vp], i32),
         "fmm_tree_stats": ([vp, C.POINTER(i64)], i32),
+        "fmm_tree_build_phases": ([vp, C.POINTER(dbl), C.POINTER(dbl)], i32),
         "fmm_plan_create": ([vp, i32, i32, i32, C.POINTER(vp)], i32),
         "fmm_plan_destroy": ([vp], i32),
         "fmm_rinv": ([vp, vp, vp, i32, i32], i32),
@@ -83,6 +84,7 @@ def load_library():
         "fmm_server_poll": ([vp, i64, C.POINTER(i32)], i32),
         "fmm_server_wait": ([vp, i64, C.POINTER(dbl)], i32),
         "fmm_server_stats": ([vp, C.POINTER(dbl)], i32),
+        "fmm_server_memory": ([vp, C.POINTER(dbl)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -192,6 +194,15 @@ class Tree:
         s = (C.c_int64 * 5)()
         _check(load_library().fmm_tree_stats(self._h, s))
         return dict(nodes=s[0], leaves=s[1], ilist_pairs=s[2], near_pairs=s[3], near_ranges=s[4])
+
+    PHASES = ("keys", "refine", "leaves_points", "colleagues", "ilist", "near_lists")
+
+    def build_phases(self) -> dict:
+        """Device ms and algorithmic bytes of each tree-build phase:
+        {phase: (ms, bytes)} (fmm_tree_build_phases)."""
+        ms, by = (C.c_double * 6)(), (C.c_double * 6)()
+        _check(load_library().fmm_tree_build_phases(self._h, ms, by))
+        return {k: (ms[i], by[i]) for i, k in enumerate(self.PHASES)}
 
     def export(self, level: int, what) -> np.ndarray:
         w = EXPORT[what] if isinstance(what, str) else int(what)
@@ -386,6 +397,12 @@ class Server:
         _check(load_library().fmm_server_stats(self._h, s))
         return dict(completed=int(s[0]), p50_ms=s[1], p99_ms=s[2], mean_ms=s[3], peak_running=int(s[4]),
                     peak_bytes=int(s[5]), budget_bytes=int(s[6]), queued=int(s[7]))
+
+    def memory(self) -> dict:
+        """Measured device memory of the running requests (fmm_server_memory)."""
+        s = (C.c_double * 3)()
+        _check(load_library().fmm_server_memory(self._h, s))
+        return dict(peak_measured_bytes=int(s[0]), budget_bytes=int(s[1]), worst_measured_over_estimate=s[2])
 
     def close(self):
         if getattr(self, "_h", None):

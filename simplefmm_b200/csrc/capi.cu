@@ -318,6 +318,18 @@ int fmm_tree_stats(const fmm_tree* tree, int64_t* s)
     return FMM_OK;
 }
 
+int fmm_tree_build_phases(const fmm_tree* tree, double* ms6, double* bytes6)
+{
+    API_TRY
+    if (!tree || !ms6) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    for (int k = 0; k < 6; ++k) ms6[k] = tree->t.phase_ms[k];
+    if (bytes6) {
+        bind(*tree->t.ctx);
+        sfmm::tree_phase_bytes(tree->t, bytes6);
+    }
+    API_CATCH
+}
+
 int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** out)
 {
     API_TRY
@@ -341,6 +353,7 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
         SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.join, cudaEventDisableTiming));
         sfmm::plan_init(pl->pl);
         SFMM_CUDA(cudaStreamSynchronize(tree->t.ctx->stream));
+        sfmm::check_scan_error();
     } catch (...) {
         for (auto& e : pl->pl.ev)
             if (e) cudaEventDestroy(e);
@@ -479,13 +492,24 @@ int fmm_direct(fmm_context* ctx, const double* xyz, int64_t n, const double* Q, 
     if (qdim < 1 || qdim > 3) return fail(FMM_ERR_UNSUPPORTED, "qdim must be 1, 2 or 3");
     if (field && qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs qdim 1 or 3");
     if (n <= 0 || nt < 0) return fail(FMM_ERR_INVALID_ARGUMENT, "bad sizes");
+    if (where != FMM_HOST && where != FMM_DEVICE) return fail(FMM_ERR_INVALID_ARGUMENT, "where must be FMM_HOST or FMM_DEVICE");
     bind(ctx->c);
     cudaStream_t st = ctx->c.stream;
     if (where == FMM_DEVICE) {
-        sfmm::direct_sum(ctx->c, xyz, n, Q, qdim, targets, nt, pot, field);
+        // the targets are device memory: the kernels skip an index outside
+        // [0, n) and flag it; the flag is read back after the sums
+        sfmm::DevBuf<int> bad;
+        bad.alloc(1, st);
+        SFMM_CUDA(cudaMemsetAsync(bad.ptr, 0, sizeof(int), st));
+        sfmm::direct_sum(ctx->c, xyz, n, Q, qdim, targets, nt, pot, field, bad.ptr);
+        int h_bad = 0;
+        SFMM_CUDA(cudaMemcpyAsync(&h_bad, bad.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
         SFMM_CUDA(cudaStreamSynchronize(st));
+        if (h_bad) return fail(FMM_ERR_INVALID_ARGUMENT, "target index out of range [0, n)");
         return FMM_OK;
     }
+    for (int64_t t = 0; t < nt; ++t)
+        if (targets[t] < 0 || targets[t] >= n) return fail(FMM_ERR_INVALID_ARGUMENT, "target index out of range [0, n)");
     sfmm::DevBuf<double> dx, dq, dp, df;
     sfmm::DevBuf<int64_t> dt;
     dx.alloc(size_t(3) * n, st);

@@ -20,8 +20,10 @@ __global__ void __launch_bounds__(kThreads) k_direct(const double* __restrict__ 
 {
     __shared__ double s[kThreads][6];
     const int64_t t = blockIdx.x * int64_t(kThreads) + threadIdx.x;
-    const bool on = t < nt;
-    const int64_t i = on ? targets[t] : 0;
+    const int64_t ti = t < nt ? targets[t] : -1;
+    // a target index outside [0, n) reads nothing; k_direct_sum reports it
+    const bool on = ti >= 0 && ti < n;
+    const int64_t i = on ? ti : 0;
     const double xi = on ? xyz[3 * i] : 0, yi = on ? xyz[3 * i + 1] : 0, zi = on ? xyz[3 * i + 2] : 0;
     double pa[3] = {0, 0, 0}, fa[3] = {0, 0, 0};
     // sources [jb, je) of this block's chunk (blockIdx.y)
@@ -62,12 +64,24 @@ __global__ void __launch_bounds__(kThreads) k_direct(const double* __restrict__ 
     for (int c = 0; c < 3; ++c) o[3 + c] = fa[c];
 }
 
-// Sum the chunks' partial sums in chunk order (deterministic).
+// Sum the chunks' partial sums in chunk order (deterministic).  A target
+// index outside [0, n) gets NaN outputs and sets *bad (when given).
 __global__ void k_direct_sum(const double* __restrict__ part, int64_t nt, int nchunk, int qdim,
-                             double* __restrict__ pot, double* __restrict__ field)
+                             const int64_t* __restrict__ targets, int64_t n, double* __restrict__ pot,
+                             double* __restrict__ field, int* __restrict__ bad)
 {
     const int64_t t = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
     if (t >= nt) return;
+    const int64_t ti = targets[t];
+    if (ti < 0 || ti >= n) {
+        const double nan = __longlong_as_double(0x7ff8000000000000LL);
+        if (pot)
+            for (int b = 0; b < qdim; ++b) pot[t * qdim + b] = nan;
+        if (field)
+            for (int c = 0; c < 3; ++c) field[t * 3 + c] = nan;
+        if (bad) atomicOr(bad, 1);
+        return;
+    }
     double acc[6] = {0, 0, 0, 0, 0, 0};
     for (int c = 0; c < nchunk; ++c)
         for (int k = 0; k < 6; ++k) acc[k] += part[(c * nt + t) * 6 + k];
@@ -80,7 +94,7 @@ __global__ void k_direct_sum(const double* __restrict__ part, int64_t nt, int nc
 }  // namespace
 
 void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets, int64_t nt,
-                double* pot, double* field)
+                double* pot, double* field, int* bad)
 {
     if (nt <= 0) return;
     // split the sources into chunks so that small target sets still fill the device
@@ -94,8 +108,8 @@ void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int q
     k_direct<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(nchunk)), kThreads, 0, c.stream>>>(
         xyz, n, Q, qdim, targets, nt, chunk, part.ptr);
     SFMM_CHECK_LAUNCH();
-    k_direct_sum<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, c.stream>>>(part.ptr, nt, static_cast<int>(nchunk),
-                                                                               qdim, pot, field);
+    k_direct_sum<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, c.stream>>>(
+        part.ptr, nt, static_cast<int>(nchunk), qdim, targets, n, pot, field, bad);
     SFMM_CHECK_LAUNCH();
 }
 
@@ -174,8 +188,9 @@ extern "C" int fmm_direct_noalloc(const double* xyz, int64_t n, const double* Q,
         k_direct<<<dim3(static_cast<unsigned>(gx), static_cast<unsigned>(nchunk)), kThreads, 0, st>>>(
             xyz, n, Q, qdim, targets, nt, chunk, d.scratch);
         SFMM_CHECK_LAUNCH();
-        k_direct_sum<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, st>>>(d.scratch, nt, static_cast<int>(nchunk),
-                                                                            qdim, pot, field);
+        // a target index outside [0, n) is not read: its outputs become NaN
+        k_direct_sum<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, st>>>(
+            d.scratch, nt, static_cast<int>(nchunk), qdim, targets, n, pot, field, nullptr);
         SFMM_CHECK_LAUNCH();
         return FMM_OK;
     } catch (const sfmm::Error& e) {

@@ -14,6 +14,7 @@
 // source-gradient moments (fmm.hpp:234-253, 549-551).
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -366,6 +367,9 @@ void plan_init(Plan& pl)
     shift_setup(pl);
     p2p_setup(pl);
     pl.m2l_ctr.alloc(1, st);
+    // test switch: the row-owner M2L kernel instead of the tensor-core ones
+    const char* mk = std::getenv("SFMM_M2L_KERNEL");
+    pl.m2l_force_rows = mk && std::strcmp(mk, "rows") == 0;
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     if (pl.precision == FMM_PRECISION_FP64) {
@@ -460,6 +464,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.p2p_part = pl.p2p_part.ptr;
     a.p2p_ctr = pl.p2p_ctr.ptr;
     a.m2l_ctr = pl.m2l_ctr.ptr;
+    a.m2l_force_rows = pl.m2l_force_rows;
     a.p2p_split = pl.p2p_rows > 0;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;

@@ -83,6 +83,7 @@ struct EvalArgs {
     double* p2p_part;
     int* p2p_ctr;
     int* m2l_ctr;                         // FP64 M2L: the counter blocks take sibling groups from
+    int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
     int p2p_split;                        // some leaf has more than one part
     double* out;                         // far field per component, sorted order
     double* out2;                        // near field per component, sorted order
@@ -121,6 +122,7 @@ struct Plan {
     DevBuf<int4> p2p_item;
     DevBuf<int32_t> p2p_row, p2p_parts, p2p_rowoff, p2p_ctr;
     DevBuf<int32_t> m2l_ctr;                  // M2L group counter (m2l.cu)
+    bool m2l_force_rows = false;              // SFMM_M2L_KERNEL=rows at plan creation
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers

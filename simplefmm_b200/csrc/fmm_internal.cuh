@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include "alloc_meter.h"
+#include "csr_limits.h"
 #include "fmm_ops.cuh"
 #include "simplefmm_b200.h"
 
@@ -79,6 +81,8 @@ cudaMemPool_t device_pool(int device);
 // allocation fails, before the allocation is retried.
 void* device_alloc(size_t bytes, int device, cudaStream_t s);        // throws FMM_ERR_OUT_OF_MEMORY
 void device_free(void* p, size_t bytes, int device, cudaStream_t s) noexcept;
+
+
 
 template<typename T>
 struct DevBuf {
@@ -219,6 +223,9 @@ struct Tree {
     int64_t near_pairs = 0;
 
     float build_ms = 0;
+    // device time of the build's phases: keys, refinement, leaves and points,
+    // colleagues, interaction lists, near-field lists
+    float phase_ms[6] = {};
 };
 
 struct Plan;
@@ -229,14 +236,29 @@ struct Plan;
 void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg,
                 const double* corner3 = nullptr, double width = 0.0);
 int64_t tree_export(const Tree& t, int level, int what, void* host_out);
+void tree_phase_bytes(const Tree& t, double* bytes6);
 
-// direct.cu
+// direct.cu: a target index outside [0, n) is not read; its outputs are NaN
+// and *bad (a device int, may be NULL) is set to 1
 void direct_sum(Context& c, const double* xyz, int64_t n, const double* Q, int qdim, const int64_t* targets, int64_t nt,
-                double* pot, double* field);
+                double* pot, double* field, int* bad = nullptr);
 
-// scan.cu: out[0..n] (n + 1 entries; out[n] is the total)
-void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s);
-void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s);
+// scan.cu: out[0..n] (n + 1 entries; out[n] is the total) of non-negative
+// counts, one launch.  total64 (a device int64, may be NULL) receives the
+// total in 64 bits, so that an int32 scan that overflowed can be refused.
+void exclusive_scan_i32(const int32_t* in, int32_t* out, int64_t n, cudaStream_t s, int64_t* total64 = nullptr);
+void exclusive_scan_i64(const int64_t* in, int64_t* out, int64_t n, cudaStream_t s, int64_t* total64 = nullptr);
+// Throws if a scan's bounded wait gave up since the last call (a scan's
+// result is then wrong); call after synchronizing the scans' stream.
+void check_scan_error();
+
+// A CSR list whose row pointers are int32 must have at most 2^31 - 1
+// entries; the total is summed in 64 bits and checked before the list is
+// allocated (csr_limits.h).
+inline void require_i32_total(int64_t total, const char* what)
+{
+    if (!csr_total_fits(total)) throw Error(FMM_ERR_UNSUPPORTED, csr_overflow_message(what, total));
+}
 
 inline unsigned blocks_for(int64_t n, int threads, int64_t cap = 1 << 20)
 {

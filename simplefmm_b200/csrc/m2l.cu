@@ -2,6 +2,11 @@
 // local (order p) and the field local (order p + 1, source orders <= p - 1)
 // produced from one rotation and one z-translation per pair.
 //
+// Kernels: k_m2l_mma (FP64 tensor cores, below) is the path for p >= 2;
+// k_m2l_tf32 the mixed-precision one for p >= 11; k_m2l_rows (this header)
+// runs p < 2 and any plan whose DMMA kernel does not fit the device, and a
+// plan created with SFMM_M2L_KERNEL=rows in the environment (a test switch).
+//
 // Work decomposition.  One block per sibling group: the children of one node
 // (<= 8 targets at level l >= 2).  Their interaction lists are contiguous and
 // share most sources.  The group's pairs are stably sorted by rotation class
@@ -352,61 +357,6 @@ void launch_rows_fallback(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cu
     SFMM_CHECK_LAUNCH();
 }
 
-// ------------------------------------------------------------------ role-pipelined kernel (p <= 12)
-// The same row-ownership arithmetic as k_m2l_rows, with the four operators
-// given to four disjoint thread groups (roles) so each thread keeps only one
-// operator row in registers, and pipelined over batches: in every step
-//   C  phases batch s (its source moments were copied into shared memory
-//      asynchronously during step s-1), starts the copy of batch s+1,
-//      computes batch s+2's column table, z-translates batch s-2
-//      (W -> LzA, LzB);
-//   B  rotates batch s-1 (X -> W);
-//   DA rotates back the potential local of batch s-3 (LzA -> accA);
-//   DB rotates back the field local of batch s-3 (LzB -> accB);
-// with one block barrier per step and double-buffered batch vectors.  C's
-// rows are ordered by azimuth k so the translation loop length p+1-k is
-// uniform across a warp.  Roles branch once at kernel entry; the barriers are
-// the non-aligned barrier.sync so different roles may arrive from different
-// code.
-
-struct Meta {
-    int cls, ncol, dsq, pad;
-    int src[8], bq[8], sb[8], pidx[8];
-};
-
-template<int P, int CB>
-struct RoleCfg {
-    static constexpr int T = (P + 1) * (P + 2) / 2;
-    static constexpr int T1 = (P + 2) * (P + 3) / 2;
-    static constexpr int NB = (T + 31) / 32 * 32;
-    static constexpr int NC = (T1 + 31) / 32 * 32;
-    static constexpr int OB = 0, OC = NB, ODA = NB + NC, ODB = 2 * NB + NC;
-    static constexpr int NT = 2 * NB + 2 * NC;
-};
-
-// Shared-memory layout of one block (byte offsets; all but accB are
-// compile-time constants so buffer addresses are immediate offsets).
-template<int P, int CB>
-struct RoleLayout {
-    static constexpr int T = (P + 1) * (P + 2) / 2;
-    static constexpr int T1 = (P + 2) * (P + 3) / 2;
-    static constexpr int ent_src = 0;
-    static constexpr int ent_code = al16(ent_src + 4 * kMaxGroupPairs);
-    static constexpr int sorted = al16(ent_code + 4 * kMaxGroupPairs);
-    static constexpr int cls = al16(sorted + 2 * kMaxGroupPairs);
-    static constexpr int cls_cnt = al16(cls + kMaxGroupPairs);
-    static constexpr int cls_off = al16(cls_cnt + 4 * 72);
-    static constexpr int bat_off = al16(cls_off + 4 * 72);
-    static constexpr int meta = al16(bat_off + 4 * 72);
-    static constexpr int Xraw = al16(meta + int(sizeof(Meta)) * 8);   // thread-private staging of source moments
-    static constexpr int X = al16(Xraw + 16 * 2 * CB * T);            // X, W, LzA, LzB are contiguous (zeroed together)
-    static constexpr int W = al16(X + 16 * 2 * CB * T);
-    static constexpr int LzA = al16(W + 16 * 2 * CB * T);
-    static constexpr int LzB = al16(LzA + 16 * 2 * CB * T);
-    static constexpr int accA = al16(LzB + 16 * 2 * CB * T1);
-    __host__ __device__ static constexpr int accB(int qd) { return al16(accA + 16 * 8 * qd * T); }
-    __host__ __device__ static constexpr int total(int qd) { return al16(accB(qd) + 16 * 8 * qd * T1); }
-};
 
 __device__ __forceinline__ void block_barrier() { asm volatile("barrier.sync 0;" ::: "memory"); }
 
@@ -424,422 +374,6 @@ __device__ __forceinline__ void cp_async8(void* smem, const void* gmem)
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
-
-template<int P, int CB>
-struct RoleShared {
-    using L = RoleLayout<P, CB>;
-    int accB_off;
-    __device__ static unsigned char* base()
-    {
-        extern __shared__ __align__(16) unsigned char sm_roles[];
-        return sm_roles;
-    }
-    __device__ int* ent_src() const { return reinterpret_cast<int*>(base() + L::ent_src); }
-    __device__ int* ent_code() const { return reinterpret_cast<int*>(base() + L::ent_code); }
-    __device__ short* sorted() const { return reinterpret_cast<short*>(base() + L::sorted); }
-    __device__ unsigned char* cls() const { return base() + L::cls; }
-    __device__ int* cls_cnt() const { return reinterpret_cast<int*>(base() + L::cls_cnt); }
-    __device__ int* cls_off() const { return reinterpret_cast<int*>(base() + L::cls_off); }
-    __device__ int* bat_off() const { return reinterpret_cast<int*>(base() + L::bat_off); }
-    __device__ Meta* meta() const { return reinterpret_cast<Meta*>(base() + L::meta); }
-    __device__ cplx* Xraw() const { return reinterpret_cast<cplx*>(base() + L::Xraw); }
-    __device__ cplx* X() const { return reinterpret_cast<cplx*>(base() + L::X); }
-    __device__ cplx* W() const { return reinterpret_cast<cplx*>(base() + L::W); }
-    __device__ cplx* LzA() const { return reinterpret_cast<cplx*>(base() + L::LzA); }
-    __device__ cplx* LzB() const { return reinterpret_cast<cplx*>(base() + L::LzB); }
-    __device__ cplx* accA() const { return reinterpret_cast<cplx*>(base() + L::accA); }
-    __device__ cplx* accB() const { return reinterpret_cast<cplx*>(base() + accB_off); }
-};
-
-// Column table of batch b (thread k < CB of the calling group fills column k).
-// c is the class of an earlier batch (batches ascend by class) and is
-// advanced to batch b's class.  Columns past ncol point at node 0 / slot 0;
-// their arithmetic runs on stale (finite) buffer contents and is discarded.
-template<int P, int CB>
-__device__ void compute_meta(const RoleShared<P, CB>& S, int b, int k, int qd, Meta& M, int& c)
-{
-    while (S.bat_off()[c + 1] <= b) ++c;
-    const int col0 = (b - S.bat_off()[c]) * CB;
-    const int ncol = min(CB, S.cls_cnt()[c] * qd - col0);
-    if (k < ncol) {
-        const int col = col0 + k;
-        const int pair = col / qd;
-        const int e = S.sorted()[S.cls_off()[c] + pair];
-        const int code = S.ent_code()[e];
-        const int di = (code & 7) - 3, dj = ((code >> 3) & 7) - 3, dk = ((code >> 6) & 7) - 3;
-        const int bq = col - pair * qd;
-        M.src[k] = S.ent_src()[e];
-        M.bq[k] = bq;
-        M.sb[k] = ((code >> 9) & 7) * qd + bq;
-        M.pidx[k] = 7 * (dj + 3) + (di + 3);
-        if (k == 0) {
-            M.cls = c;
-            M.ncol = ncol;
-            M.dsq = di * di + dj * dj + dk * dk;
-        }
-    } else if (k < CB) {
-        M.src[k] = 0;
-        M.bq[k] = 0;
-        M.sb[k] = 0;
-        M.pidx[k] = 24;
-    }
-}
-
-// Group set-up shared by all roles: gather, class sort, batch table, batch
-// 0's column table, zeroed accumulators.  Returns the batch count.
-template<int P, int CB>
-__device__ int group_prologue(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g, int tid)
-{
-    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
-    const int qd = a.qdim;
-    const int nc = a.nchild[g];
-    const int cb = a.child_beg[g];
-    const int e0 = a.il_ptr[cb];
-    const int E = a.il_ptr[cb + nc] - e0;
-    for (int s = 0; s < nc; ++s) {
-        const int q0 = a.il_ptr[cb + s] - e0, q1 = a.il_ptr[cb + s + 1] - e0;
-        for (int e = q0 + tid; e < q1; e += NT) {
-            const int code = a.il_code[e0 + e];
-            S.ent_src()[e] = a.il_src[e0 + e];
-            S.ent_code()[e] = code | (s << 9);
-            S.cls()[e] = static_cast<unsigned char>(rot_class((code & 7) - 3, ((code >> 3) & 7) - 3, ((code >> 6) & 7) - 3));
-        }
-    }
-    for (int t = tid; t < 8 * qd * T; t += NT) S.accA()[t] = cplx{0, 0};
-    for (int t = tid; t < 8 * qd * T1; t += NT) S.accB()[t] = cplx{0, 0};
-    block_barrier();
-    for (int cl = tid; cl < kNumClasses; cl += NT) {
-        int cnt = 0;
-        for (int e = 0; e < E; ++e) cnt += S.cls()[e] == cl;
-        S.cls_cnt()[cl] = cnt;
-    }
-    block_barrier();
-    if (tid == 0) {
-        int s = 0, k = 0;
-        for (int c = 0; c < kNumClasses; ++c) {
-            S.cls_off()[c] = s;
-            S.bat_off()[c] = k;
-            s += S.cls_cnt()[c];
-            k += (S.cls_cnt()[c] * qd + CB - 1) / CB;
-        }
-        S.cls_off()[kNumClasses] = s;
-        S.bat_off()[kNumClasses] = k;
-    }
-    block_barrier();
-    for (int cl = tid; cl < kNumClasses; cl += NT) {
-        int pos = S.cls_off()[cl];
-        for (int e = 0; e < E; ++e)
-            if (S.cls()[e] == cl) S.sorted()[pos++] = static_cast<short>(e);
-    }
-    block_barrier();
-    if (tid < CB) {
-        int c = 0;
-        if (S.bat_off()[kNumClasses] > 0) compute_meta<P, CB>(S, 0, tid, qd, S.meta()[0], c);
-        if (S.bat_off()[kNumClasses] > 1) compute_meta<P, CB>(S, 1, tid, qd, S.meta()[1], c);
-    }
-    block_barrier();
-    return S.bat_off()[kNumClasses];
-}
-
-template<int P, int CB>
-__device__ void group_epilogue(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g, int tid)
-{
-    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1, NT = RoleCfg<P, CB>::NT;
-    const int qd = a.qdim;
-    const int nc = a.nchild[g];
-    const int cb = a.child_beg[g];
-    if (a.want_pot)
-        for (int e = tid; e < nc * qd * T; e += NT) a.LA[int64_t(cb) * qd * T + e] = S.accA()[e];
-    if (a.want_field)
-        for (int e = tid; e < nc * qd * T1; e += NT) a.LB[int64_t(cb) * qd * T1 + e] = S.accB()[e];
-    block_barrier();
-}
-
-// C: column table, load + phase, z-translation.  Translation rows are
-// ordered by azimuth k (row ci -> (j, k)); operator entries past a row's
-// length are zero, so the loop runs to the warp's longest row without
-// per-lane tests, reading in-range (clamped) source coefficients.
-template<int P, int CB>
-__device__ void role_C(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid)
-{
-    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
-    const int ci = tid - RoleCfg<P, CB>::OC;
-    const int qd = a.qdim;
-    int k = 0, rem = ci;
-    while (k <= P + 1 && rem >= P + 2 - k) {
-        rem -= P + 2 - k;
-        ++k;
-    }
-    const bool on = ci < T1;
-    const int j = on ? k + rem : 0;
-    if (!on) k = 0;
-    const int r = tri(j, k);
-    const int kc = k <= P ? k : P;                    // clamped azimuth for source reads
-    int kmin = on ? k : P + 1;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) kmin = min(kmin, __shfl_xor_sync(0xffffffffu, kmin, o));
-    // translation row: sources n' = k + i, i < p - k in tz[], the n' = p term in tzl
-    double tz[P], tzl;
-    {
-        const int wd = P + 1 - k;
-        const double* row = a.tzx + a.tzx_off[k] + (j - k) * (wd > 0 ? wd : 0);
-#pragma unroll
-        for (int i = 0; i < P; ++i) tz[i] = (on && i < wd - 1) ? __ldg(row + i) : 0.0;
-        tzl = (on && wd > 0) ? __ldg(row + wd - 1) : 0.0;
-    }
-    // load role: coefficient xt = ci of every column (T <= NC)
-    const bool ld = ci < T;
-    int xm = 0;
-    if (ld) {
-        int xn;
-        tri_nm(ci, xn, xm);
-    }
-    // batch b's source coefficients -> Xraw[b & 1], issued a step ahead of use
-    auto issue = [&](int b) {
-        const Meta& M = S.meta()[b & 7];
-        const int ncol = M.ncol;
-        cplx* xr = S.Xraw() + (b & 1) * CB * T + ci;
-#pragma unroll
-        for (int cc = 0; cc < CB; ++cc)
-            if (cc < ncol) cp_async16(xr + cc * T, a.M + (int64_t(M.src[cc]) * qd + M.bq[cc]) * T + ci);
-        cp_async_commit();
-    };
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
-        if (a.nchild[g] == 0) continue;
-        const int lt = level_of(a, g) + 1;
-        const int nbat = group_prologue<P, CB>(a, S, g, tid);
-        int cmeta = 0;
-        if (ld && nbat > 0) issue(0);
-        for (int s = 0; s < nbat + 3; ++s) {
-            if (s < nbat && ld) {
-                cp_async_wait_all();
-                const Meta& M = S.meta()[s & 7];
-                const int ncol = M.ncol;
-                const cplx* xr = S.Xraw() + (s & 1) * CB * T + ci;
-                cplx* X = S.X() + (s & 1) * CB * T + ci;
-#pragma unroll
-                for (int cc = 0; cc < CB; ++cc)
-                    if (cc < ncol) {
-                        const double2 ph = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + xm);
-                        X[cc * T] = cmul(cplx{ph.x, ph.y}, xr[cc * T]);
-                    }
-                if (s + 1 < nbat) issue(s + 1);
-            }
-            if (s + 2 < nbat && ci < CB) compute_meta<P, CB>(S, s + 2, ci, qd, S.meta()[(s + 2) & 7], cmeta);
-            if (s >= 2 && s - 2 < nbat) {
-                const Meta& M = S.meta()[(s - 2) & 7];
-                const cplx* W = S.W() + (s & 1) * CB * T;          // (s - 2) & 1 == s & 1
-                cplx* LzA = S.LzA() + (s & 1) * CB * T;
-                cplx* LzB = S.LzB() + (s & 1) * CB * T1;
-                const double sc = a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + j];
-                double bre[CB], bim[CB];
-#pragma unroll
-                for (int cc = 0; cc < CB; ++cc) bre[cc] = bim[cc] = 0;
-#pragma unroll
-                for (int i = 0; i < P; ++i) {
-                    if (i >= P - kmin) break;
-                    const int np = min(k + i, P);
-                    const cplx* y = W + np * (np + 1) / 2 + kc;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc) {
-                        const cplx w = y[cc * T];
-                        bre[cc] = fma(tz[i], w.re, bre[cc]);
-                        bim[cc] = fma(tz[i], w.im, bim[cc]);
-                    }
-                }
-                if (on) {
-                    // field local: sources of order <= p - 1; potential local adds order p
-                    const cplx* yl = W + P * (P + 1) / 2 + kc;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc) {
-                        LzB[cc * T1 + r] = cplx{bre[cc] * sc, bim[cc] * sc};
-                        if (j <= P) {
-                            const cplx w = yl[cc * T];
-                            LzA[cc * T + r] = cplx{fma(tzl, w.re, bre[cc]) * sc, fma(tzl, w.im, bim[cc]) * sc};
-                        }
-                    }
-                }
-            }
-            block_barrier();
-        }
-        group_epilogue<P, CB>(a, S, g, tid);
-    }
-}
-
-// B: forward rotation, order n row m (operator entries past n are zero).
-template<int P, int CB>
-__device__ void role_B(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid)
-{
-    constexpr int T = RoleCfg<P, CB>::T;
-    const int bi = tid - RoleCfg<P, CB>::OB;
-    const bool on = bi < T;
-    int n = 0, m = 0;
-    if (on) tri_nm(bi, n, m);
-    const int base = n * (n + 1) / 2;
-    int nmax = on ? n : 0;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-    double Pr[P + 1], Qr[P + 1];
-#pragma unroll
-    for (int b = 0; b <= P; ++b) Pr[b] = Qr[b] = 0.0;
-    int cur = -1;
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
-        if (a.nchild[g] == 0) continue;
-        const int lt = level_of(a, g) + 1;
-        const int nbat = group_prologue<P, CB>(a, S, g, tid);
-        for (int s = 0; s < nbat + 3; ++s) {
-            if (s >= 1 && s - 1 < nbat) {
-                const Meta& M = S.meta()[(s - 1) & 7];
-                if (M.cls != cur) {
-                    cur = M.cls;
-                    if (on) {
-                        const double* Pp = a.rot + int64_t(cur) * a.rot_len + a.rot_off[n] + m * (n + 1);
-                        const double* Qp = Pp + (n + 1) * (n + 1);
-#pragma unroll
-                        for (int b = 0; b <= P; ++b) {
-                            Pr[b] = b <= n ? __ldg(Pp + b) : 0.0;
-                            Qr[b] = b <= n ? __ldg(Qp + b) : 0.0;
-                        }
-                    }
-                }
-                const cplx* X = S.X() + ((s - 1) & 1) * CB * T + base;
-                cplx* W = S.W() + ((s - 1) & 1) * CB * T;
-                double re[CB], im[CB];
-#pragma unroll
-                for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
-#pragma unroll
-                for (int b = 0; b <= P; ++b) {
-                    if (b > nmax) break;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc) {
-                        const cplx x = X[cc * T + b];
-                        re[cc] = fma(Pr[b], x.re, re[cc]);
-                        im[cc] = fma(Qr[b], x.im, im[cc]);
-                    }
-                }
-                if (on) {
-                    const double sc = n ? a.ipow[(int64_t(lt) * 28 + M.dsq) * a.ipow_w + n - 1] : 1.0;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc) W[cc * T + bi] = cplx{re[cc] * sc, im[cc] * sc};
-                }
-            }
-            block_barrier();
-        }
-        group_epilogue<P, CB>(a, S, g, tid);
-    }
-}
-
-// D: inverse rotation of one local (LA: order <= P, ORDER1 = false; LB:
-// order <= P + 1, ORDER1 = true) and phase, accumulated into the group's
-// targets in column order (deterministic).
-template<int P, int CB, bool ORDER1>
-__device__ void role_D(const EvalArgs& a, const RoleShared<P, CB>& S, int64_t g0, int64_t g1, int tid, int off)
-{
-    constexpr int T = RoleCfg<P, CB>::T, T1 = RoleCfg<P, CB>::T1;
-    constexpr int TO = ORDER1 ? T1 : T;               // rows of this local
-    constexpr int NMAX = ORDER1 ? P + 1 : P;
-    const int di = tid - off;
-    const bool wanted = ORDER1 ? a.want_field : a.want_pot;
-    const bool on = di < TO && wanted;
-    int n = 0, m = 0;
-    if (di < TO) tri_nm(di, n, m);
-    const int base = n * (n + 1) / 2;
-    int nmax = on ? n : 0;
-#pragma unroll
-    for (int o = 16; o; o >>= 1) nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-    double PB[NMAX + 1], QB[NMAX + 1];
-#pragma unroll
-    for (int b = 0; b <= NMAX; ++b) PB[b] = QB[b] = 0.0;
-    int cur = -1;
-    for (int64_t g = g0 + blockIdx.x; g < g1; g += gridDim.x) {
-        if (a.nchild[g] == 0) continue;
-        const int nbat = group_prologue<P, CB>(a, S, g, tid);
-        for (int s = 0; s < nbat + 3; ++s) {
-            if (wanted && s >= 3) {
-                const Meta& M = S.meta()[(s - 3) & 7];
-                const int ncol = M.ncol;
-                if (M.cls != cur) {
-                    cur = M.cls;
-                    if (on) {
-                        const int wd = (n + 1) * (n + 1);
-                        const double* PBp = a.rot + int64_t(cur) * a.rot_len + a.rot_off[n] + 2 * wd + m * (n + 1);
-                        const double* QBp = PBp + wd;
-#pragma unroll
-                        for (int b = 0; b <= NMAX; ++b) {
-                            PB[b] = b <= n ? __ldg(PBp + b) : 0.0;
-                            QB[b] = b <= n ? __ldg(QBp + b) : 0.0;
-                        }
-                    }
-                }
-                const cplx* Lz = (ORDER1 ? S.LzB() + ((s - 3) & 1) * CB * T1 : S.LzA() + ((s - 3) & 1) * CB * T) + base;
-                double re[CB], im[CB];
-#pragma unroll
-                for (int cc = 0; cc < CB; ++cc) re[cc] = im[cc] = 0;
-#pragma unroll
-                for (int b = 0; b <= NMAX; ++b) {
-                    if (b > nmax) break;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc) {
-                        const cplx z = Lz[cc * TO + b];
-                        re[cc] = fma(PB[b], z.re, re[cc]);
-                        im[cc] = fma(QB[b], z.im, im[cc]);
-                    }
-                }
-                if (on) {
-                    cplx* acc = (ORDER1 ? S.accB() : S.accA()) + di;
-#pragma unroll
-                    for (int cc = 0; cc < CB; ++cc)
-                        if (cc < ncol) {
-                            const double2 e = __ldg(reinterpret_cast<const double2*>(a.eil) + M.pidx[cc] * (P + 2) + m);
-                            const cplx v = cmul(cplx{e.x, -e.y}, cplx{re[cc], im[cc]});
-                            cplx& d = acc[M.sb[cc] * TO];
-                            d.re += v.re;
-                            d.im += v.im;
-                        }
-                }
-            }
-            block_barrier();
-        }
-        group_epilogue<P, CB>(a, S, g, tid);
-    }
-}
-
-template<int P, int CB, int MINB>
-__global__ void __launch_bounds__(RoleCfg<P, CB>::NT, MINB) k_m2l_roles(EvalArgs a, int64_t g0, int64_t g1)
-{
-    using C = RoleCfg<P, CB>;
-    using L = RoleLayout<P, CB>;
-    RoleShared<P, CB> S;
-    S.accB_off = L::accB(a.qdim);
-    const int tid = threadIdx.x;
-    // batch buffers start at zero: columns past a batch's count are computed
-    // on whatever the buffers hold, which must be finite
-    for (int t = tid; t < (L::accA - L::X) / 16; t += C::NT) S.X()[t] = cplx{0, 0};
-    block_barrier();
-    if (tid < C::OC) role_B<P, CB>(a, S, g0, g1, tid);
-    else if (tid < C::ODA) role_C<P, CB>(a, S, g0, g1, tid);
-    else if (tid < C::ODB) role_D<P, CB, false>(a, S, g0, g1, tid, C::ODA);
-    else role_D<P, CB, true>(a, S, g0, g1, tid, C::ODB);
-}
-
-template<int P, int CB, int MINB>
-bool try_launch_roles(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
-{
-    using C = RoleCfg<P, CB>;
-    const size_t smem = RoleLayout<P, CB>::total(a.qdim);
-    int dev = 0, optin = 0;
-    SFMM_CUDA(cudaGetDevice(&dev));
-    SFMM_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    if (smem > size_t(optin)) return false;
-    allow_max_smem(k_m2l_roles<P, CB, MINB>);
-    int per_sm = 0;
-    SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_m2l_roles<P, CB, MINB>, C::NT, smem));
-    if (per_sm < 1) return false;
-    const int64_t grid = std::min<int64_t>(std::max<int64_t>(g1 - g0, 1), int64_t(sms) * per_sm * 4);
-    k_m2l_roles<P, CB, MINB><<<static_cast<unsigned>(grid), C::NT, smem, st>>>(a, g0, g1);
-    SFMM_CHECK_LAUNCH();
-    return true;
-}
 
 // ------------------------------------------------------------------ FP64 tensor-core kernel
 // The same rotate / translate / rotate-back arithmetic as matrix products on
@@ -2065,6 +1599,10 @@ __global__ void k_frag_tz32(const double* __restrict__ tzx, const int* __restric
 template<int P>
 void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st)
 {
+    if (a.m2l_force_rows) {
+        launch_rows_fallback<P>(a, g0, g1, sms, st);
+        return;
+    }
     if constexpr (P >= 2) {
         // mixed plans take the TF32 kernel where it is the faster one (p = 12:
         // 281 ms against 364 ms on 16M uniform points; p = 10: 92 ms against
@@ -2072,16 +1610,6 @@ void launch_m2l_p(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream
         if (a.mixed && P >= kTf32MinOrder && try_launch_tf32<P>(a, g0, g1, sms, st)) return;
         if (try_launch_mma<P, 1, 8, true>(a, g0, g1, sms, st)) return;
         if (try_launch_mma<P, 1, 8, false>(a, g0, g1, sms, st)) return;
-    }
-    if constexpr (P >= 2 && P <= 12) {
-        // two blocks per SM of 4-column batches measured fastest up to p = 10
-        // (4M-point Plummer, p = 10: 122 ms against 144 ms for one block of
-        // 8-column batches); higher orders keep one block of 8 columns
-        if constexpr (P <= 10) {
-            if (try_launch_roles<P, 4, 2>(a, g0, g1, sms, st)) return;
-        }
-        if (try_launch_roles<P, 8, 1>(a, g0, g1, sms, st)) return;
-        if (try_launch_roles<P, 4, 1>(a, g0, g1, sms, st)) return;
     }
     launch_rows_fallback<P>(a, g0, g1, sms, st);
 }

@@ -32,6 +32,22 @@ namespace {
 
 constexpr size_t kCacheMin = size_t(4) << 20;
 
+thread_local AllocMeter* tl_meter_request = nullptr;
+thread_local AllocMeter* tl_meter_server = nullptr;
+thread_local bool tl_cache_on = true;
+
+void meter_add(size_t bytes)
+{
+    if (tl_meter_request) tl_meter_request->add(int64_t(bytes));
+    if (tl_meter_server) tl_meter_server->add(int64_t(bytes));
+}
+
+void meter_sub(size_t bytes) noexcept
+{
+    if (tl_meter_request) tl_meter_request->sub(int64_t(bytes));
+    if (tl_meter_server) tl_meter_server->sub(int64_t(bytes));
+}
+
 struct Cached {
     void* p;
     cudaEvent_t released;                  // recorded on the releasing stream
@@ -77,10 +93,27 @@ struct DeviceScope {
 
 }  // namespace
 
+void set_thread_alloc_meters(AllocMeter* request, AllocMeter* server) noexcept
+{
+    tl_meter_request = request;
+    tl_meter_server = server;
+}
+
+void set_thread_block_cache(bool on) noexcept { tl_cache_on = on; }
+
 void* device_alloc(size_t bytes, int device, cudaStream_t s)
 {
     SFMM_REQUIRE(device >= 0 && device < 64, FMM_ERR_INVALID_ARGUMENT, "device index out of range");
     BlockCache& c = block_cache(device);
+    meter_add(bytes);
+    struct Undo {
+        size_t b;
+        bool armed = true;
+        ~Undo()
+        {
+            if (armed) meter_sub(b);
+        }
+    } undo{bytes};
     if (bytes >= kCacheMin) {
         std::lock_guard<std::mutex> lk(c.mu);
         auto it = c.blocks.find(bytes);
@@ -90,6 +123,7 @@ void* device_alloc(size_t bytes, int device, cudaStream_t s)
             SFMM_CUDA(cudaEventDestroy(it->second.released));
             c.bytes -= bytes;
             c.blocks.erase(it);
+            undo.armed = false;
             return p;
         }
     }
@@ -108,13 +142,15 @@ void* device_alloc(size_t bytes, int device, cudaStream_t s)
         }
     }
     SFMM_CUDA(e);
+    undo.armed = false;
     return p;
 }
 
 void device_free(void* p, size_t bytes, int device, cudaStream_t s) noexcept
 {
     if (!p) return;
-    if (bytes >= kCacheMin && device >= 0 && device < 64) {
+    meter_sub(bytes);
+    if (tl_cache_on && bytes >= kCacheMin && device >= 0 && device < 64) {
         DeviceScope scope(device);
         BlockCache& c = block_cache(device);
         cudaEvent_t ev = nullptr;

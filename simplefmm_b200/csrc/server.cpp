@@ -11,10 +11,19 @@
 // fits is admitted.  A request larger than the whole budget is rejected at
 // submission (FMM_ERR_OVER_BUDGET).
 //
+// Memory: admission sums per-request estimates (estimate_bytes) against the
+// budget.  Every device allocation a request makes is metered on its worker
+// thread (its own peak, and the server's live total over running requests),
+// and a server's workers bypass the library's block cache, so freed blocks go
+// back to the pool: fmm_server_memory reports the measured peak of the
+// running requests' device memory beside the budget, and the largest ratio
+// of a request's measured peak to its estimate.
+//
 // Leaf size: a request may name max_particles_per_node, or pass 0 to let the
-// server's autotuner choose: per (p, precision, log2 N) bucket it times each
-// candidate leaf size once (points per second of the whole solve) and then
-// uses the fastest.
+// server's autotuner choose: per (p, precision, log2 N) bucket it tries each
+// candidate leaf size twice, timing the solve's own tree build and
+// evaluation on the device (CUDA events on its stream, after the operator
+// tables exist), keeps each candidate's best rate, and then uses the fastest.
 //
 // Latency is measured from submission to completion (queueing included);
 // fmm_server_stats reports its p50 / p99 over completed requests.
@@ -33,6 +42,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "alloc_meter.h"
 #include "simplefmm_b200.h"
 
 namespace sfmm {
@@ -51,7 +61,8 @@ struct Request {
     int qdim = 1, p = 0, precision = 0, leaf = 0;
     double* pot = nullptr;
     double* field = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;                 // estimated device memory (admission)
+    int64_t measured = 0;             // measured peak of its device allocations
     bool tuned = false;               // leaf size chosen by the autotuner
     Clock::time_point t_submit, t_done;
     int status = FMM_OK;
@@ -74,11 +85,13 @@ size_t estimate_bytes(int64_t n, int p, int qdim, int leaf)
     return static_cast<size_t>(per_point * double(n) + per_node * nodes + (64 << 20));
 }
 
+constexpr int kTrialsPerCandidate = 2;
+
 struct Autotuner {
     std::mutex mu;
     struct Bucket {
         double best_rate[3] = {0, 0, 0};
-        int tried = 0;
+        int tried = 0;                // trials handed out, candidate tried % 3
     };
     std::map<std::tuple<int, int, int>, Bucket> buckets;
 
@@ -86,22 +99,26 @@ struct Autotuner {
     {
         return {r.p, r.precision, static_cast<int>(std::log2(double(std::max<int64_t>(r.n, 1))))};
     }
+    // Called once a request has been accepted (after the budget check), so a
+    // rejected request takes no trial.
     int choose(const Request& r)
     {
         std::lock_guard<std::mutex> lk(mu);
         Bucket& b = buckets[key(r)];
-        if (b.tried < 3) return kLeafCandidates[b.tried++];
+        if (b.tried < 3 * kTrialsPerCandidate) return kLeafCandidates[b.tried++ % 3];
         int best = 1;
         for (int i = 0; i < 3; ++i)
             if (b.best_rate[i] > b.best_rate[best]) best = i;
         return kLeafCandidates[best];
     }
-    void report(const Request& r, double seconds)
+    // device_ms: the request's tree build + evaluation on its stream
+    void report(const Request& r, double device_ms)
     {
+        if (!(device_ms > 0)) return;
         std::lock_guard<std::mutex> lk(mu);
         Bucket& b = buckets[key(r)];
         for (int i = 0; i < 3; ++i)
-            if (kLeafCandidates[i] == r.leaf) b.best_rate[i] = std::max(b.best_rate[i], double(r.n) / seconds);
+            if (kLeafCandidates[i] == r.leaf) b.best_rate[i] = std::max(b.best_rate[i], double(r.n) / device_ms);
     }
 };
 
@@ -118,6 +135,8 @@ struct fmm_server {
     std::unordered_map<int64_t, std::shared_ptr<Request>> all;
     size_t in_use = 0, peak_in_use = 0;
     int running = 0, peak_running = 0;
+    sfmm::AllocMeter meter;               // measured device bytes of the running requests
+    double worst_ratio = 0;               // largest measured / estimated over completed requests
     int64_t next_id = 1;
     bool stopping = false;
     std::vector<double> latencies_ms;
@@ -131,21 +150,26 @@ void fmm_server::run(fmm_context* c, Request& r)
 {
     fmm_tree* tree = nullptr;
     fmm_plan* plan = nullptr;
-    const auto t0 = Clock::now();
+    sfmm::AllocMeter own;
+    sfmm::set_thread_alloc_meters(&own, &meter);
     int rc = fmm_tree_build(c, r.xyz, r.n, FMM_HOST, 20, r.leaf, 2, 0.0, &tree);
     if (rc == FMM_OK) rc = fmm_plan_create(tree, r.p, r.qdim, r.precision, &plan);
     if (rc == FMM_OK) rc = fmm_evaluate(plan, r.Q, r.pot, r.field, FMM_HOST);
     if (rc != FMM_OK) r.error = fmm_last_error();
+    double ms6[6] = {0, 0, 0, 0, 0, 0};
+    if (rc == FMM_OK && r.tuned && fmm_plan_timings(plan, ms6) != FMM_OK) ms6[4] = ms6[5] = 0;
     if (plan) fmm_plan_destroy(plan);
     if (tree) fmm_tree_destroy(tree);
+    sfmm::set_thread_alloc_meters(nullptr, nullptr);
+    r.measured = own.peak.load();
     r.status = rc;
-    if (rc == FMM_OK && r.tuned)
-        tuner.report(r, std::chrono::duration<double>(Clock::now() - t0).count());
+    if (rc == FMM_OK && r.tuned) tuner.report(r, ms6[4] + ms6[5]);
 }
 
 void fmm_server::worker(int slot)
 {
     fmm_context* c = ctx[slot];
+    sfmm::set_thread_block_cache(false);
     for (;;) {
         std::shared_ptr<Request> r;
         {
@@ -169,6 +193,7 @@ void fmm_server::worker(int slot)
             r->done = true;
             in_use -= r->bytes;
             --running;
+            if (r->bytes) worst_ratio = std::max(worst_ratio, double(r->measured) / double(r->bytes));
             if (r->status == FMM_OK)
                 latencies_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
         }
@@ -232,10 +257,13 @@ int fmm_server_submit(fmm_server* s, const double* xyz, int64_t n, const double*
     r->pot = pot;
     r->field = field;
     r->tuned = max_particles_per_node == 0;
-    r->leaf = r->tuned ? s->tuner.choose(*r) : max_particles_per_node;
+    // the budget check takes the smallest candidate leaf (the largest
+    // estimate) for an autotuned request, before it takes a trial
+    r->leaf = r->tuned ? kLeafCandidates[0] : max_particles_per_node;
     r->bytes = estimate_bytes(n, p, qdim, r->leaf);
     if (r->bytes > s->budget)
         return sfmm::record_failure(FMM_ERR_OVER_BUDGET, "request's estimated device memory exceeds the server budget");
+    if (r->tuned) r->leaf = s->tuner.choose(*r);
     {
         std::lock_guard<std::mutex> lk(s->mu);
         if (s->stopping) return sfmm::record_failure(FMM_ERR_INVALID_ARGUMENT, "server is stopping");
@@ -297,6 +325,16 @@ int fmm_server_stats(fmm_server* s, double* stats8)
     stats8[5] = double(s->peak_in_use);
     stats8[6] = double(s->budget);
     stats8[7] = double(s->queue.size());
+    return FMM_OK;
+}
+
+int fmm_server_memory(fmm_server* s, double* out3)
+{
+    if (!s || !out3) return sfmm::record_failure(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    out3[0] = double(s->meter.peak.load());
+    out3[1] = double(s->budget);
+    out3[2] = s->worst_ratio;
     return FMM_OK;
 }
 

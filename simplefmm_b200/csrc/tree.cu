@@ -549,9 +549,18 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     t.vertical_axis = vertical_axis;
     t.phideg = phideg;
 
-    cudaEvent_t e0, e1;
-    SFMM_CUDA(cudaEventCreate(&e0));
-    SFMM_CUDA(cudaEventCreate(&e1));
+    // events at the phase boundaries: start, keys, refinement, leaves and
+    // points, colleagues, interaction lists, near-field lists (the end)
+    struct Events {
+        cudaEvent_t e[7] = {};
+        ~Events()
+        {
+            for (auto& x : e)
+                if (x) cudaEventDestroy(x);
+        }
+    } ev;
+    for (auto& x : ev.e) SFMM_CUDA(cudaEventCreate(&x));
+    cudaEvent_t e0 = ev.e[0], e1 = ev.e[6];
     SFMM_CUDA(cudaEventRecord(e0, st));
 
     // --- box (box.hpp:84-107)
@@ -592,6 +601,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     t.order.alloc(n, st);
     k_keys<<<blocks_for(n, 256, 8192), 256, 0, st>>>(xyz, n, t.d_box.ptr, keyA.ptr, ordA.ptr);
     SFMM_CHECK_LAUNCH();
+    SFMM_CUDA(cudaEventRecord(ev.e[1], st));
     t.box = read_one(t.d_box.ptr, st);
     SFMM_REQUIRE(t.box.status == FMM_OK, FMM_ERR_DEGENERATE_INPUT,
                  "all points share the vertical coordinate: the reference's box loop would never end");
@@ -685,6 +695,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     }
     t.depth = level;
     t.n_nodes = total;
+    SFMM_CUDA(cudaEventRecord(ev.e[2], st));
 
     // --- leaves (per level in key order: the reference's _i_leaf)
     {
@@ -722,6 +733,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         t.far_z = t.pts.ptr + t.box.Z * n;
     }
 
+    SFMM_CUDA(cudaEventRecord(ev.e[3], st));
+
     // --- colleagues, level by level
     t.colleague.alloc(27 * total, st);
     for (int l = 0; l <= t.depth; ++l) {
@@ -730,6 +743,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
                                                           t.nchild.ptr, t.colleague.ptr);
         SFMM_CHECK_LAUNCH();
     }
+
+    SFMM_CUDA(cudaEventRecord(ev.e[4], st));
 
     // --- interaction lists (levels >= 2)
     {
@@ -743,8 +758,11 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
             SFMM_CHECK_LAUNCH();
         }
         t.il_ptr.alloc(total + 1, st);
-        exclusive_scan_i32(icnt.ptr, t.il_ptr.ptr, total, st);
-        t.il_nnz = read_one(t.il_ptr.ptr + total, st);
+        DevBuf<int64_t> tot;
+        tot.alloc(1, st);
+        exclusive_scan_i32(icnt.ptr, t.il_ptr.ptr, total, st, tot.ptr);
+        t.il_nnz = read_one(tot.ptr, st);
+        require_i32_total(t.il_nnz, "the interaction list");
         t.il_src.alloc(std::max<int64_t>(t.il_nnz, 1), st);
         t.il_code.alloc(std::max<int64_t>(t.il_nnz, 1), st);
         for (int l = 2; l <= t.depth; ++l) {
@@ -755,6 +773,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
             SFMM_CHECK_LAUNCH();
         }
     }
+
+    SFMM_CUDA(cudaEventRecord(ev.e[5], st));
 
     // --- near-field ranges per leaf
     {
@@ -768,8 +788,11 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
                                                            t.pend.ptr, t.colleague.ptr, ncnt.ptr, nullptr, pairs.ptr);
         SFMM_CHECK_LAUNCH();
         t.nr_ptr.alloc(L + 1, st);
-        exclusive_scan_i32(ncnt.ptr, t.nr_ptr.ptr, L, st);
-        t.nr_nnz = read_one(t.nr_ptr.ptr + L, st);
+        DevBuf<int64_t> tot;
+        tot.alloc(1, st);
+        exclusive_scan_i32(ncnt.ptr, t.nr_ptr.ptr, L, st, tot.ptr);
+        t.nr_nnz = read_one(tot.ptr, st);
+        require_i32_total(t.nr_nnz, "the near-field range list");
         t.near_pairs = static_cast<int64_t>(read_one(pairs.ptr, st));
         t.nr.alloc(std::max<int64_t>(t.nr_nnz, 1), st);
         k_near<true><<<blocks_for(L, 128), 128, 0, st>>>(L, t.leaf_node.ptr, t.parent.ptr, t.nchild.ptr, t.pbeg.ptr,
@@ -779,9 +802,41 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
 
     SFMM_CUDA(cudaEventRecord(e1, st));
     SFMM_CUDA(cudaEventSynchronize(e1));
+    check_scan_error();
     SFMM_CUDA(cudaEventElapsedTime(&t.build_ms, e0, e1));
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    for (int k = 0; k < 6; ++k) SFMM_CUDA(cudaEventElapsedTime(&t.phase_ms[k], ev.e[k], ev.e[k + 1]));
+}
+
+// Algorithmic device-memory bytes of each build phase (what the phase's
+// kernels must read and write at least once), for the achieved-bandwidth
+// figures beside phase_ms:
+//   keys        min/max read 24 B and key kernel read 24 B + write 12 B per point
+//   refinement  per level, each point of a splitting node: the histogram reads
+//               its 8 B key, the scatter reads and writes key + index (24 B);
+//               the final order is written once (4 B per point)
+//   leaves      points gathered into leaf order: read 24 B + 4 B index, write 24 B
+//               (twice when the frame is rotated); leaf ids 16 B per node
+//   colleagues  27 int32 per node written, parent/child fields read (12 B)
+//   ilist       both passes read the 27 colleagues and 16 B of node fields per
+//               node; the entries (src, code) are written once, 8 B each
+//   near lists  both passes read the 27 colleagues per leaf's node; the ranges
+//               are written once (int2), the row pointers once
+void tree_phase_bytes(const Tree& t, double* bytes6)
+{
+    cudaStream_t st = t.ctx->stream;
+    const auto nch = to_host(t.nchild.ptr, t.n_nodes, st);
+    const auto pb = to_host(t.pbeg.ptr, t.n_nodes, st);
+    const auto pe = to_host(t.pend.ptr, t.n_nodes, st);
+    double active = 0;                           // sum over levels of points in splitting nodes
+    for (int64_t g = 0; g < t.n_nodes; ++g)
+        if (nch[g] > 0) active += double(pe[g] - pb[g]);
+    const double n = double(t.n), nodes = double(t.n_nodes), L = double(t.n_leaves);
+    bytes6[0] = 60.0 * n;
+    bytes6[1] = 32.0 * active + 4.0 * n;
+    bytes6[2] = (t.box.rotated ? 76.0 : 52.0) * n + 16.0 * nodes;
+    bytes6[3] = (27.0 * 4 + 12.0) * nodes;
+    bytes6[4] = 2 * (27.0 * 4 + 16.0) * nodes + 8.0 * double(t.il_nnz) + 4.0 * nodes;
+    bytes6[5] = 2 * 27.0 * 4 * L + 8.0 * double(t.nr_nnz) + 4.0 * L;
 }
 
 // ------------------------------------------------------------------ exports

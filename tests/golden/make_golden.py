@@ -36,6 +36,8 @@ CASES = {
     "axis0_n3000_p6": ("plummer", 3000, 19, 6, 20, 32, 0, 0.0, T | POT, "uniform", 1),
     "phi30_n3000_p6": ("uniform", 3000, 20, 6, 20, 32, 2, 30.0, T | POT, "uniform", 1),
     "uniform_n3000_p12": ("uniform", 3000, 21, 12, 20, 64, 2, 0.0, POT | FIELD, "uniform", 1),
+    "uniform_n3000_p13": ("uniform", 3000, 25, 13, 20, 64, 2, 0.0, POT | FIELD, "uniform", 1),
+    "plummer_n3000_p16_ppn32": ("plummer", 3000, 26, 16, 20, 32, 2, 0.0, T | POT | FIELD, "uniform", 1),
     "box_n3000_p6": ("uniform", 3000, 22, 6, 20, 64, 2, 0.0, T | POT | FIELD | refio.FLAG_BOX, "uniform", 1),
     "exclude_n3000_p6": ("plummer", 3000, 23, 6, 20, 32, 2, 0.0, POT | FIELD | refio.FLAG_EXCLUDE, "uniform", 1),
     "exclude_far_n3000_p6": ("plummer", 3000, 24, 6, 20, 32, 2, 0.0, POT | FIELD | refio.FLAG_EXCLUDE_FAR,

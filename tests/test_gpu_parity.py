@@ -254,3 +254,45 @@ def test_captured_evaluation_replays_like_evaluate():
         plan.evaluate(q, pot, fld)
         np.testing.assert_array_equal(pot_d.cpu().numpy(), pot)
         np.testing.assert_array_equal(fld_d.cpu().numpy(), fld)
+
+
+@pytest.mark.parametrize("name", ["uniform_n3000_p6", "gauss2_n4000_p8", "uniform_n3000_p12", "uniform_n3000_p13",
+                                  "vector_n2000_p8_ppn128"])
+def test_row_owner_m2l_matches_reference(monkeypatch, ctx, name):
+    """The row-owner M2L kernel (k_m2l_rows: runs p < 2 and plans whose
+    tensor-core kernel does not fit) forced by its test switch: the same
+    reference results as the default kernels."""
+    monkeypatch.setenv("SFMM_M2L_KERNEL", "rows")
+    g = load_golden(name)
+    t = golden_tree(sf, g, ctx)
+    plan = sf.Plan(t, g["p"], g["qdim"])
+    monkeypatch.delenv("SFMM_M2L_KERNEL")
+    sp, sf_ = pyoracle.error_scales(g["pos"], g["q"])
+    n = g["n"]
+    if g["qdim"] == 1:
+        pot, field = np.zeros(n), np.zeros((n, 3))
+        plan.evaluate(g["q"], pot, field)
+        assert rel_err_per_target(pot, g["POT"], sp) < TOL
+        assert rel_err_per_target(field, g["FIELD"], sf_) < TOL
+    else:
+        vp, bi = np.zeros((n, 3)), np.zeros((n, 3))
+        plan.rinv(g["q"], vp)
+        plan.rinv(g["q"], bi, gradient=True)
+        assert rel_err_per_target(vp, g["VECPOT"], sp) < TOL
+        assert rel_err_per_target(bi, g["BIOT"], sf_) < TOL
+
+
+@pytest.mark.parametrize("p", [0, 1])
+def test_lowest_orders_against_restatement(ctx, p):
+    """p = 0 and 1 (the row-owner M2L kernel's own orders) against the CPU
+    restatement, all targets."""
+    n = 20000
+    pos, q = W.points("plummer", n, 77), W.charges(n, 77)
+    t = sf.Tree(pos, 20, 32, ctx=ctx)
+    pot, field = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, p, 1).evaluate(q, pot, field)
+    ot = pyoracle.Tree(pos, 20, 32)
+    opot, ofield = ot.potential_field(p, q)
+    sp, sfl = pyoracle.error_scales(pos, q)
+    assert rel_err_per_target(pot, opot, sp) < TOL
+    assert rel_err_per_target(field, ofield, sfl) < TOL

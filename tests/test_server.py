@@ -69,8 +69,13 @@ def test_admission_respects_the_memory_budget():
         pot, fld, _ = srv.wait(rid)
         assert np.isfinite(pot).all() and np.isfinite(fld).all()
     st = srv.stats()
-    assert st["peak_bytes"] <= budget
+    assert st["peak_bytes"] <= budget              # the estimates admitted at once
     assert st["completed"] == len(reqs)
+    mem = srv.memory()
+    # every request's measured device allocations stayed below its estimate,
+    # and what the running requests held at once stayed below the budget
+    assert 0 < mem["worst_measured_over_estimate"] <= 1.0
+    assert 0 < mem["peak_measured_bytes"] <= budget
     srv.close()
 
 
