@@ -234,9 +234,9 @@ SFMM_HD cplx derive_component(const CompSpec& cs, const cplx* M, int T, int k, i
 SFMM_HD void unpack_term(int code, int* power, int* q, int* in, bool* conj_in)
 {
     *power = code & 31;
-    *q = ((code >> 5) & 63) - 16;
-    *in = (code >> 11) & 511;
-    *conj_in = (code >> 20) & 1;
+    *q = ((code >> 5) & 127) - 32;
+    *in = (code >> 12) & 511;
+    *conj_in = (code >> 21) & 1;
 }
 
 // One output coefficient of M2M (child -> parent, fmm.hpp:558-576) or L2L

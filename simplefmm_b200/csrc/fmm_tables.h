@@ -8,11 +8,17 @@ namespace sfmm {
 constexpr int kMaxP = 16;
 constexpr int kRotClasses = 70;          // fmm.hpp:169
 
-// M2M / L2L term code: power of rho (5 bits), phase index q + 16 (6 bits),
-// input coefficient index (9 bits), conjugate-input flag (1 bit).
+// M2M / L2L term code: power of rho (5 bits, 0..31), phase index q + 32
+// (7 bits, |q| <= 32), input coefficient index (9 bits, < 512), conjugate-input
+// flag (1 bit).  The L2L of the field local runs at order p + 1 <= 17, where
+// q = m - k reaches -17: the phase field must hold it without a sign.
+inline constexpr bool term_fits(int power, int q, int in)
+{
+    return power >= 0 && power < 32 && q >= -32 && q < 96 && in >= 0 && in < 512;
+}
 inline constexpr int pack_term(int power, int q, int in, bool conj_in)
 {
-    return power | ((q + 16) << 5) | (in << 11) | (conj_in ? 1 << 20 : 0);
+    return power | ((q + 32) << 5) | (in << 12) | (conj_in ? 1 << 21 : 0);
 }
 
 struct HostTables {

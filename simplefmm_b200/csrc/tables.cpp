@@ -19,6 +19,7 @@
 #include <algorithm>
 #include <cmath>
 #include <complex>
+#include <stdexcept>
 #include <vector>
 
 #include "fmm_tables.h"
@@ -182,6 +183,7 @@ HostTables make_tables(int p)
                     const int q = -m;
                     const int km = k - m;
                     const int in = tri(j - n, std::abs(km));
+                    if (!term_fits(n, q, in)) throw std::length_error("M2M term outside its code's fields");
                     t.m2m_code.push_back(pack_term(n, q, in, km < 0));
                     t.m2m_g.push_back(g);
                 }
@@ -199,6 +201,7 @@ HostTables make_tables(int p)
                                      Znear[tri(n - j, std::abs(m - k))];
                     const int q = m - k;
                     const int in = tri(n, std::abs(m));
+                    if (!term_fits(n - j, q, in)) throw std::length_error("L2L term outside its code's fields");
                     t.l2l_code.push_back(pack_term(n - j, q, in, m < 0));
                     t.l2l_g.push_back(g);
                 }

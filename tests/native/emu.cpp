@@ -421,3 +421,25 @@ extern "C" int emu_fmm(int depth, const int64_t* nnode, const int64_t* nleaf, vo
             }
     return 0;
 }
+
+// Decodes every M2M / L2L term code of order p and counts the codes whose
+// fields fall outside what an order-p shift can hold (|phase index| <= p,
+// rho power <= p, input coefficient < T(p)): a field too narrow for its
+// value shows up here, where on the device it would index past the arrays.
+extern "C" int emu_check_term_codes(int p)
+{
+    const HostTables tb = make_tables(p);
+    const int T = (p + 1) * (p + 2) / 2;
+    int bad = 0;
+    auto check = [&](const std::vector<int>& codes) {
+        for (int c : codes) {
+            int pw, q, in;
+            bool cj;
+            unpack_term(c, &pw, &q, &in, &cj);
+            if (q < -p || q > p || pw < 0 || pw > p || in < 0 || in >= T) ++bad;
+        }
+    };
+    check(tb.m2m_code);
+    check(tb.l2l_code);
+    return bad;
+}

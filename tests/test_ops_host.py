@@ -110,3 +110,23 @@ def test_emulated_p12(emu, split):
     sp, sf = pyoracle.error_scales(g["pos"], g["q"])
     assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
     assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
+
+
+@pytest.mark.parametrize("name,p", [("uniform_n3000_p13", 13), ("plummer_n3000_p16_ppn32", 16)])
+def test_emulated_highest_orders(emu, name, p):
+    """p = 13 and the largest order the library takes, 16: the field local's
+    L2L runs at order 17, whose term codes need the widest phase field."""
+    g = load_golden(name)
+    t = pyoracle.Tree(g["pos"], g["max_level"], g["max_ppn"])
+    pot, field = run_emu(emu, t.dump(), g["pos"], g["q"], p)
+    sp, sf = pyoracle.error_scales(g["pos"], g["q"])
+    assert rel_err_per_target(pot, g["POT"], sp) < 1e-12
+    assert rel_err_per_target(field, g["FIELD"], sf) < 1e-12
+
+
+def test_shift_term_codes_hold_every_order(emu):
+    """M2M / L2L term codes decode to in-range fields for every order the
+    library runs them at: 0..16, and 17 for the field local's L2L at p = 16."""
+    emu.emu_check_term_codes.restype = C.c_int
+    for p in range(0, 18):
+        assert emu.emu_check_term_codes(p) == 0, p
