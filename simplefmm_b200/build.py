@@ -69,7 +69,7 @@ def build(verbose: bool = False, extra_flags=None) -> Path:
     objs = [BUILD / (s.stem + ".o") for s in _sources()]
     if jobs or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
         run([nvcc()] + ARCH + ["-shared", "-o", str(LIB)] + [str(o) for o in objs] +
-            ["-lcudart", "-lcublas", "-Xlinker", "-rpath=" + str(cuda_lib())])
+            ["-lcudart", "-Xlinker", "-rpath=" + str(cuda_lib())])
     return LIB
 
 

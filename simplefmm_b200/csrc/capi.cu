@@ -70,8 +70,6 @@ void release_context(fmm_context* ctx)
     if (!ctx || --ctx->refs > 0) return;
     cudaSetDevice(ctx->c.device);
     cudaStreamSynchronize(ctx->c.stream);
-    sfmm::release_blas(ctx->c);
-    cudaStreamSynchronize(ctx->c.stream);
     if (ctx->c.side) {
         cudaStreamSynchronize(ctx->c.side);
         cudaStreamDestroy(ctx->c.side);

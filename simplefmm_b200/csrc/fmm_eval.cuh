@@ -129,7 +129,7 @@ struct Plan {
     // M2M / L2L as matrix products (shift.cu): per children level the octant
     // maps, compact slots of the parents that have children, scratch rows
     bool shift_on = false;
-    DevBuf<double> sh_ops, sh_x, sh_y;
+    DevBuf<double> sh_ops;
     DevBuf<int32_t> sh_slot, sh_list;
     std::vector<int32_t> sh_S;
     DevBuf<float2> m32;                       // mixed precision: scaled FP32 source moments
@@ -148,7 +148,6 @@ void plan_init(Plan& pl);
 void shift_setup(Plan& pl);
 void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st);
 void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st);
-void release_blas(Context& c) noexcept;
 // p2p.cu: near-field work items of the plan's tree (leaves with a large near
 // field split into parts), built at plan creation
 void p2p_setup(Plan& pl);

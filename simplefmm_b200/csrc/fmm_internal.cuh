@@ -177,8 +177,6 @@ struct Context {
                                           // on it beside the far field (forked from and joined
                                           // back into `stream` with events)
     int sm_count = 148;
-    void* blas = nullptr;                 // cuBLAS handle of the M2M / L2L products (shift.cu)
-    void* blas_ws = nullptr;              // its fixed workspace
 };
 
 // Device-resident octree: nodes of all levels concatenated level by level

@@ -1,25 +1,32 @@
-// M2M and L2L (fmm.hpp:558-590, 714-745) as FP64 matrix products on the
-// tensor cores.
+// M2M and L2L (fmm.hpp:558-590, 714-745) as FP64 tensor-core products, one
+// fused kernel per level.
 //
 // A shift between a box and one of its children is a fixed real-linear map
 // on the box's coefficient row (the m >= 0 triangle stored as re, im pairs:
 // R = 2T doubles) that depends only on the child's octant and on the level
 // (through rho = sqrt(3/4) w / 2^l).  Per children level the maps are built
 // once per plan by applying the direct term sums of fmm_ops.cuh
-// (shift_output, the same code as k_m2m / k_l2l) to unit vectors:
-//   L2L  OpL (8R x R): rows oct * R + i, so one product gives all eight
-//        children's shifts of a parent's local;
-//   M2M  OpM (R x 8R): columns oct * R + i, applied to a parent's eight
-//        children stacked (absent children are zero columns).
-// Only parents with children take part: their compact slots come from a
-// scan at set-up.  Per level, a gather kernel stacks the rows, one cuBLAS
-// DGEMM (FP64 tensor cores) applies the map to every slot, and a scatter
-// kernel adds the result to the children (L2L) or writes the parents (M2M).
+// (shift_output, the code of the warp-per-node kernels k_m2m / k_l2l) to
+// unit vectors, and stored in MMA fragment order:
+//   M2M  OpM (R x 8R): a parent's row is OpM times its eight children's rows
+//        stacked in octant order (absent children are zero);
+//   L2L  OpL (8R x R): rows oct * R + i, one product gives all eight
+//        children's shifts of a parent's local.
+// Only parents with children take part (compact slots from a scan at
+// set-up).  A block takes 32 (M2M) or 64 (L2L) columns (parent slot x charge
+// component); K chunks that hold only zero operator entries (the maps are
+// triangular in the expansion order) are skipped:
+//   k_m2m_mma  for each octant, stages the 32 children's moments in shared
+//              memory (the B operand) and accumulates OpM's octant block on the
+//              FP64 tensor cores (mma.sync m8n8k4, operator fragments read
+//              from L2 once per 4 column tiles); then writes the parents.
+//   k_l2l_mma  stages the 64 parents' locals, and for each 8-row tile of OpL
+//              adds the product into the child of that row's octant (each
+//              child coefficient has one writer: no atomics, deterministic).
 // The sums differ from the direct ones in rounding order only (FP64, about
-// 1e-16 relative per term).
+// 1e-16 relative per term).  Evaluations allocate nothing here, so they can
+// be captured as CUDA graphs.
 #include "eval_util.cuh"
-
-#include <cublas_v2.h>
 
 #include <algorithm>
 #include <cmath>
@@ -28,21 +35,38 @@
 namespace sfmm {
 namespace {
 
-#define SFMM_BLAS(call)                                                                              \
-    do {                                                                                             \
-        const cublasStatus_t s_ = (call);                                                            \
-        if (s_ != CUBLAS_STATUS_SUCCESS)                                                             \
-            throw Error(FMM_ERR_CUDA, std::string("cuBLAS error ") + std::to_string(int(s_)) + " in " #call); \
-    } while (0)
+constexpr int kShiftCols = 32;            // M2M columns per block: four 8-column MMA tiles
+constexpr int kL2LTiles = 8;              // L2L: eight 8-column MMA tiles (64 columns) per block
+constexpr int kShiftWarps = 8;
 
-constexpr size_t kBlasWorkspace = size_t(32) << 20;
+__host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
 
-// Column k (input re / im part of coefficient k / 2) of the octant maps of one level.
+// padded leading dimension of a [col][k] operand buffer (>= k + 4, = 4 or
+// 12 mod 16 doubles: the B-fragment loads are bank-conflict free)
+__host__ __device__ constexpr int shift_ld(int k)
+{
+    int ld = k + 4;
+    while (ld % 16 != 4 && ld % 16 != 12) ++ld;
+    return ld;
+}
+
+__device__ __forceinline__ void mma884(double& d0, double& d1, double a, double b)
+{
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// Column k (input re / im part of coefficient k / 2) of the octant maps of
+// one level, written in fragment order (lane l of fragment (rt, kc) holds
+// A[8 rt + l / 4][4 kc + l % 4]):
+//   M2M  fragment ((oct * RT + rt) * KC + kc), RT = ceil(R / 8), KC = ceil(R / 4)
+//   L2L  fragment (rt * KC + kc), rt over the 8R rows oct * R + i
 template<bool kM2M>
 __global__ void k_shift_ops(const int* __restrict__ ptr, const int* __restrict__ code, const double* __restrict__ g,
                             const cplx* __restrict__ phase, int pp, double rho, double* __restrict__ op)
 {
-    const int Tn = (pp + 1) * (pp + 2) / 2, R = 2 * Tn;
+    const int Tn = (pp + 1) * (pp + 2) / 2, R = 2 * Tn, RT = cdiv(R, 8), KC = cdiv(R, 4);
     const int oct = blockIdx.x / R, k = blockIdx.x - oct * R, in = k >> 1, part = k & 1;
     extern __shared__ double sm[];
     double* rpow = sm;                                      // pp + 1 <= 32
@@ -53,11 +77,15 @@ __global__ void k_shift_ops(const int* __restrict__ ptr, const int* __restrict__
         for (int q = 1; q <= pp; ++q) rpow[q] = rpow[q - 1] * rho;
     }
     __syncthreads();
+    const int kc = k >> 2, lc = k & 3;
     for (int o = threadIdx.x; o < Tn; o += blockDim.x) {
         const cplx v = shift_output<kM2M>(o, ptr, code, g, X, oct, rpow, phase + (oct & 3) * (2 * pp + 1), pp);
-        const int64_t idx = kM2M ? int64_t(oct * R + k) * R + 2 * o : int64_t(k) * 8 * R + oct * R + 2 * o;
-        op[idx] = v.re;
-        op[idx + 1] = v.im;
+        for (int h = 0; h < 2; ++h) {
+            const int row = kM2M ? 2 * o + h : oct * R + 2 * o + h;
+            const int rt = row >> 3, lr = row & 7;
+            const int64_t f = kM2M ? (int64_t(oct) * RT + rt) * KC + kc : int64_t(rt) * KC + kc;
+            op[f * 32 + lr * 4 + lc] = h ? v.im : v.re;
+        }
     }
 }
 
@@ -80,70 +108,182 @@ __global__ void k_slots(const int32_t* __restrict__ flag, const int32_t* __restr
         }
 }
 
-// M2M: children of level lc stacked under their parent's slot
-__global__ void k_m2m_gather(const double* __restrict__ M, const uint64_t* __restrict__ key, const int32_t* __restrict__ parent,
-                             const int32_t* __restrict__ slot, int64_t base, int32_t slot0, int64_t c0, int64_t nc, int qd,
-                             int R, double* __restrict__ X)
+// Order of coefficient index t of the m >= 0 triangle, and the number of
+// coefficients of orders < j.
+__device__ __forceinline__ int tri_order(int t)
 {
-    const int64_t per = int64_t(qd) * R, total = nc * per;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t c = c0 + i / per;
-        const int e = static_cast<int>(i % per), b = e / R, r = e - b * R;
-        const int s = slot[parent[c] - base] - slot0, oct = static_cast<int>(key[c] & 7);
-        X[(int64_t(s) * qd + b) * 8 * R + oct * R + r] = M[c * per + e];
+    int n, m;
+    tri_nm(t, n, m);
+    return n;
+}
+__host__ __device__ constexpr int tri_count(int j) { return j * (j + 1) / 2; }
+
+// The shift maps are triangular in the expansion order: an M2M output of
+// order j takes inputs of orders <= j, an L2L output of order j inputs of
+// orders >= j.  K chunks that hold only zero operator entries are skipped
+// (a zero product adds nothing, so the sums are unchanged).
+__device__ __forceinline__ int m2m_kc_end(int rt, int R)
+{
+    const int r = min(8 * rt + 7, R - 1);                  // the tile's last (highest-order) row
+    return min(cdiv(2 * tri_count(tri_order(r >> 1) + 1), 4), cdiv(R, 4));
+}
+__device__ __forceinline__ int l2l_kc_begin(int rt, int R)
+{
+    int jmin = 1 << 20;
+    for (int q = 0; q < 8; ++q) {
+        const int i = (8 * rt + q) % R;                    // coefficient row within its octant block
+        jmin = min(jmin, tri_order(i >> 1));
+    }
+    return (2 * tri_count(jmin)) / 4;
+}
+
+// The block's columns (slot x component) and each slot's child per octant.
+struct ShiftTile {
+    int node[kShiftCols];                 // parent node of column c (-1 past the end)
+    int b[kShiftCols];                    // charge component of column c
+    int kid[kShiftCols][8];               // child node of column c's parent per octant (-1 absent)
+};
+
+// Columns [(blockIdx.x * per + h) * 32, + 32): part h of the block's per x 32 columns.
+__device__ void shift_tile(ShiftTile& t, const int32_t* __restrict__ list, int32_t slot0, int64_t ncols, int qd,
+                           const int32_t* __restrict__ child_beg, const int32_t* __restrict__ nchild,
+                           const uint64_t* __restrict__ key, int per = 1, int h = 0)
+{
+    const int64_t c0 = (int64_t(blockIdx.x) * per + h) * kShiftCols;
+    for (int c = threadIdx.x; c < kShiftCols; c += blockDim.x) {
+        const int64_t col = c0 + c;
+        for (int o = 0; o < 8; ++o) t.kid[c][o] = -1;
+        if (col < ncols) {
+            const int64_t s = col / qd;
+            const int g = list[slot0 + s];
+            t.node[c] = g;
+            t.b[c] = static_cast<int>(col - s * qd);
+            const int cb = child_beg[g], nc = nchild[g];
+            for (int k = cb; k < cb + nc; ++k) t.kid[c][key[k] & 7] = k;
+        } else {
+            t.node[c] = -1;
+            t.b[c] = 0;
+        }
     }
 }
 
-// rows of the n slots -> nodes list[slot0 + s] (add = false) or from them (gather)
-__global__ void k_slot_rows(double* __restrict__ node_rows, const int32_t* __restrict__ list, int32_t slot0, int64_t n, int qd,
-                            int R, double* __restrict__ slot_rows, bool to_nodes)
+// M2M into the parents of one level: columns [blockIdx.x * 32, + 32) of the
+// ncols = slots x qd columns; op = that level's OpM fragments.
+__global__ void __launch_bounds__(32 * kShiftWarps) k_m2m_mma(const double* __restrict__ op, int R,
+                                                              const int32_t* __restrict__ list, int32_t slot0,
+                                                              int64_t ncols, int qd, const int32_t* __restrict__ child_beg,
+                                                              const int32_t* __restrict__ nchild,
+                                                              const uint64_t* __restrict__ key, double* __restrict__ M)
 {
-    const int64_t per = int64_t(qd) * R, total = n * per;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t s = i / per, e = i - s * per;
-        const int64_t g = list[slot0 + s];
-        if (to_nodes) node_rows[g * per + e] = slot_rows[i];
-        else slot_rows[i] = node_rows[g * per + e];
+    constexpr int kMaxRowTiles = 5;       // R / 8 / warps: R <= 306 (p <= 16)
+    __shared__ ShiftTile tile;
+    extern __shared__ double Bs[];        // [32 cols][LD]
+    const int RT = cdiv(R, 8), KC = cdiv(R, 4), LD = shift_ld(4 * KC);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lr = lane >> 2, lc = lane & 3;
+    shift_tile(tile, list, slot0, ncols, qd, child_beg, nchild, key);
+    double acc[kMaxRowTiles][4][2];
+#pragma unroll
+    for (int j = 0; j < kMaxRowTiles; ++j)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[j][q][0] = acc[j][q][1] = 0.0;
+    for (int oct = 0; oct < 8; ++oct) {
+        __syncthreads();                  // the tile is set / the previous octant's operands are consumed
+        for (int e = threadIdx.x; e < kShiftCols * LD; e += blockDim.x) {
+            const int c = e / LD, k = e - c * LD;
+            const int kid = tile.kid[c][oct];
+            Bs[e] = (k < R && kid >= 0) ? M[(int64_t(kid) * qd + tile.b[c]) * R + k] : 0.0;
+        }
+        __syncthreads();
+        const double* fo = op + int64_t(oct) * RT * KC * 32 + lane;
+#pragma unroll
+        for (int j = 0; j < kMaxRowTiles; ++j) {
+            const int rt = warp + kShiftWarps * j;
+            if (rt >= RT) break;
+            const double* fr = fo + int64_t(rt) * KC * 32;
+            const int kce = m2m_kc_end(rt, R);
+            for (int kc = 0; kc < kce; ++kc) {
+                const double a = __ldg(fr + kc * 32);
+#pragma unroll
+                for (int q = 0; q < 4; ++q)
+                    mma884(acc[j][q][0], acc[j][q][1], a, Bs[(q * 8 + lr) * LD + 4 * kc + lc]);
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < kMaxRowTiles; ++j) {
+        const int rt = warp + kShiftWarps * j;
+        if (rt >= RT) break;
+        const int r = 8 * rt + lr;
+        if (r >= R) continue;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = q * 8 + 2 * lc + h;
+                if (tile.node[c] >= 0) M[(int64_t(tile.node[c]) * qd + tile.b[c]) * R + r] = acc[j][q][h];
+            }
     }
 }
 
-// L2L: each child of level lc adds its octant's block of its parent's product
-__global__ void k_l2l_scatter(double* __restrict__ L, const uint64_t* __restrict__ key, const int32_t* __restrict__ parent,
-                              const int32_t* __restrict__ slot, int64_t base, int32_t slot0, int64_t c0, int64_t nc, int qd,
-                              int R, const double* __restrict__ Y)
+// L2L into the children of one level; blockIdx.y = 0: potential local
+// (LA, R = 2T), 1: field local (LB, R = 2 T1).
+struct L2LSide {
+    const double* op;
+    int R;
+    double* L;
+};
+
+template<int NQ>                          // NQ 8-column MMA tiles: 8 NQ columns per block
+__global__ void __launch_bounds__(32 * kShiftWarps) k_l2l_mma(L2LSide sa, L2LSide sb, const int32_t* __restrict__ list,
+                                                              int32_t slot0, int64_t ncols, int qd,
+                                                              const int32_t* __restrict__ child_beg,
+                                                              const int32_t* __restrict__ nchild,
+                                                              const uint64_t* __restrict__ key)
 {
-    const int64_t per = int64_t(qd) * R, total = nc * per;
-    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
-        const int64_t c = c0 + i / per;
-        const int e = static_cast<int>(i % per), b = e / R, r = e - b * R;
-        const int s = slot[parent[c] - base] - slot0, oct = static_cast<int>(key[c] & 7);
-        L[c * per + e] += Y[(int64_t(s) * qd + b) * 8 * R + oct * R + r];
+    constexpr int NC = 8 * NQ;
+    const L2LSide sd = blockIdx.y ? sb : sa;
+    if (!sd.L) return;
+    __shared__ ShiftTile tile[NQ / 4];
+    extern __shared__ double Bs[];        // [NC cols][LD]
+    const int R = sd.R, RT8 = R, KC = cdiv(R, 4), LD = shift_ld(4 * KC);   // 8R rows: R row tiles
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lr = lane >> 2, lc = lane & 3;
+    for (int h = 0; h < NQ / 4; ++h) shift_tile(tile[h], list, slot0, ncols, qd, child_beg, nchild, key, NQ / 4, h);
+    __syncthreads();
+    for (int e = threadIdx.x; e < NC * LD; e += blockDim.x) {
+        const int c = e / LD, k = e - c * LD;
+        const int g = tile[c / kShiftCols].node[c % kShiftCols];
+        Bs[e] = (k < R && g >= 0) ? sd.L[(int64_t(g) * qd + tile[c / kShiftCols].b[c % kShiftCols]) * R + k] : 0.0;
+    }
+    __syncthreads();
+    for (int rt = warp; rt < RT8; rt += kShiftWarps) {
+        double acc[NQ][2] = {};
+        const double* fr = sd.op + int64_t(rt) * KC * 32 + lane;
+        for (int kc = l2l_kc_begin(rt, R); kc < KC; ++kc) {
+            const double a = __ldg(fr + kc * 32);
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) mma884(acc[q][0], acc[q][1], a, Bs[(q * 8 + lr) * LD + 4 * kc + lc]);
+        }
+        const int row = 8 * rt + lr, oct = row / R, i = row - oct * R;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int c = q * 8 + 2 * lc + h;
+                const ShiftTile& t = tile[c / kShiftCols];
+                const int cc = c % kShiftCols;
+                const int kid = t.node[cc] >= 0 ? t.kid[cc][oct] : -1;
+                if (kid >= 0) sd.L[(int64_t(kid) * qd + t.b[cc]) * R + i] += acc[q][h];
+            }
     }
 }
 
 unsigned grid_for(int64_t n, int sms) { return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(sms) * 16))); }
 
-cublasHandle_t blas(Context& c)
-{
-    if (!c.blas) {
-        cublasHandle_t h = nullptr;
-        SFMM_BLAS(cublasCreate(&h));
-        c.blas = h;
-        c.blas_ws = device_alloc(kBlasWorkspace, c.device, c.stream);
-        SFMM_BLAS(cublasSetWorkspace(h, c.blas_ws, kBlasWorkspace));
-    }
-    return static_cast<cublasHandle_t>(c.blas);
-}
+// fragment counts of one level's maps
+int64_t m2m_frags(int R) { return int64_t(8) * cdiv(R, 8) * cdiv(R, 4); }
+int64_t l2l_frags(int R) { return int64_t(R) * cdiv(R, 4); }
 
 }  // namespace
-
-void release_blas(Context& c) noexcept
-{
-    if (c.blas) cublasDestroy(static_cast<cublasHandle_t>(c.blas));
-    if (c.blas_ws) device_free(c.blas_ws, kBlasWorkspace, c.device, c.stream);
-    c.blas = nullptr;
-    c.blas_ws = nullptr;
-}
 
 void shift_setup(Plan& pl)
 {
@@ -152,8 +292,7 @@ void shift_setup(Plan& pl)
     if (t.depth < 3) return;
     Context& c = *t.ctx;
     cudaStream_t st = c.stream;
-    blas(c);
-    const int p = pl.p, qd = pl.qdim, RA = 2 * pl.T, RB = 2 * pl.T1;
+    const int p = pl.p, RA = 2 * pl.T, RB = 2 * pl.T1;
     // parents of levels 2 .. depth - 1 with children: compact slots
     const int64_t base = t.lvl_off[2], n = t.lvl_off[t.depth] - base;
     DevBuf<int32_t> flag;
@@ -173,10 +312,11 @@ void shift_setup(Plan& pl)
     pl.sh_S.assign(t.depth + 1, 0);
     SFMM_CUDA(cudaMemcpyAsync(pl.sh_S.data(), S.ptr, (t.depth + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
-    // operators per children level 3 .. depth: OpM (RA x 8RA), OpLA (8RA x RA), OpLB (8RB x RB)
-    const int64_t per_level = 8LL * RA * RA * 2 + 8LL * RB * RB;
+    // maps per children level 3 .. depth, fragment order: OpM (RA x 8RA),
+    // OpLA (8RA x RA), OpLB (8RB x RB); zero padding rows / columns
+    const int64_t per_level = (m2m_frags(RA) + l2l_frags(RA) + l2l_frags(RB)) * 32;
     pl.sh_ops.alloc(size_t(per_level) * (t.depth - 2), st);
-    int64_t max_slots = 0;
+    SFMM_CUDA(cudaMemsetAsync(pl.sh_ops.ptr, 0, size_t(per_level) * (t.depth - 2) * sizeof(double), st));
     for (int l = 3; l <= t.depth; ++l) {
         double* op = pl.sh_ops.ptr + per_level * (l - 3);
         const double rho = std::sqrt(0.75) * t.box.width / double(1 << l);
@@ -186,69 +326,54 @@ void shift_setup(Plan& pl)
         SFMM_CHECK_LAUNCH();
         k_shift_ops<false><<<8 * RA, 128, shm, st>>>(pl.tab->l2l_ptr.ptr, pl.tab->l2l_code.ptr, pl.tab->l2l_g.ptr,
                                                      reinterpret_cast<const cplx*>(pl.tab->eparent.ptr), p, rho,
-                                                     op + 8LL * RA * RA);
+                                                     op + m2m_frags(RA) * 32);
         SFMM_CHECK_LAUNCH();
         k_shift_ops<false><<<8 * RB, 128, shm, st>>>(pl.tab->l2l1_ptr.ptr, pl.tab->l2l1_code.ptr, pl.tab->l2l1_g.ptr,
                                                      reinterpret_cast<const cplx*>(pl.tab->eparent1.ptr), p + 1, rho,
-                                                     op + 16LL * RA * RA);
+                                                     op + (m2m_frags(RA) + l2l_frags(RA)) * 32);
         SFMM_CHECK_LAUNCH();
-        max_slots = std::max<int64_t>(max_slots, pl.sh_S[l] - pl.sh_S[l - 1]);
     }
-    pl.sh_x.alloc(size_t(std::max<int64_t>(max_slots, 1)) * qd * 8 * RB, st);
-    pl.sh_y.alloc(size_t(std::max<int64_t>(max_slots, 1)) * qd * 8 * RB, st);
+    const size_t smem = size_t(8 * kL2LTiles) * shift_ld(4 * cdiv(RB, 4)) * sizeof(double);
+    SFMM_REQUIRE(smem + 2 * sizeof(ShiftTile) <= 227 * 1024, FMM_ERR_UNSUPPORTED, "shift operands exceed shared memory");
+    allow_max_smem(k_m2m_mma);
+    allow_max_smem(k_l2l_mma<kL2LTiles>);
     pl.shift_on = true;
 }
 
 void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st)
 {
     Tree& t = *pl.tree;
-    const int qd = pl.qdim, R = 2 * pl.T, sms = t.ctx->sm_count;
+    const int qd = pl.qdim, R = 2 * pl.T;
     const int32_t slot0 = pl.sh_S[lp];
     const int64_t n = pl.sh_S[lp + 1] - slot0;
     if (n <= 0) return;
     const int lc = lp + 1;
-    const int64_t c0 = t.lvl_off[lc], nc = t.lvl_off[lc + 1] - c0, base = t.lvl_off[2];
-    const double* op = pl.sh_ops.ptr + (8LL * R * R * 2 + 8LL * (2 * pl.T1) * (2 * pl.T1)) * (lc - 3);
-    SFMM_CUDA(cudaMemsetAsync(pl.sh_x.ptr, 0, size_t(n) * qd * 8 * R * sizeof(double), st));
-    k_m2m_gather<<<grid_for(nc * qd * R, sms), 256, 0, st>>>(reinterpret_cast<const double*>(a.M), a.key, a.parent,
-                                                            pl.sh_slot.ptr, base, slot0, c0, nc, qd, R, pl.sh_x.ptr);
-    SFMM_CHECK_LAUNCH();
-    cublasHandle_t h = blas(*t.ctx);
-    SFMM_BLAS(cublasSetStream(h, st));
-    const double one = 1.0, zero = 0.0;
-    SFMM_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, R, static_cast<int>(n * qd), 8 * R, &one, op, R, pl.sh_x.ptr, 8 * R,
-                          &zero, pl.sh_y.ptr, R));
-    k_slot_rows<<<grid_for(n * qd * R, sms), 256, 0, st>>>(reinterpret_cast<double*>(a.M), pl.sh_list.ptr, slot0, n, qd, R,
-                                                          pl.sh_y.ptr, true);
+    const int64_t per_level = (m2m_frags(R) + l2l_frags(R) + l2l_frags(2 * pl.T1)) * 32;
+    const double* op = pl.sh_ops.ptr + per_level * (lc - 3);
+    const int64_t ncols = n * qd;
+    const size_t smem = size_t(kShiftCols) * shift_ld(4 * cdiv(R, 4)) * sizeof(double);
+    k_m2m_mma<<<static_cast<unsigned>((ncols + kShiftCols - 1) / kShiftCols), 32 * kShiftWarps, smem, st>>>(
+        op, R, pl.sh_list.ptr, slot0, ncols, qd, t.child_beg.ptr, t.nchild.ptr, t.key.ptr, reinterpret_cast<double*>(a.M));
     SFMM_CHECK_LAUNCH();
 }
 
 void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st)
 {
     Tree& t = *pl.tree;
-    const int qd = pl.qdim, RA = 2 * pl.T, RB = 2 * pl.T1, sms = t.ctx->sm_count;
+    const int qd = pl.qdim, RA = 2 * pl.T, RB = 2 * pl.T1;
     const int32_t slot0 = pl.sh_S[lc - 1];
     const int64_t n = pl.sh_S[lc] - slot0;
     if (n <= 0) return;
-    const int64_t c0 = t.lvl_off[lc], nc = t.lvl_off[lc + 1] - c0, base = t.lvl_off[2];
-    const double* op = pl.sh_ops.ptr + (8LL * RA * RA * 2 + 8LL * RB * RB) * (lc - 3);
-    cublasHandle_t h = blas(*t.ctx);
-    SFMM_BLAS(cublasSetStream(h, st));
-    const double one = 1.0, zero = 0.0;
-    for (int which = 0; which < 2; ++which) {
-        if (which == 0 && !a.want_pot) continue;
-        if (which == 1 && !a.want_field) continue;
-        const int R = which ? RB : RA;
-        double* L = reinterpret_cast<double*>(which ? a.LB : a.LA);
-        const double* opl = which ? op + 16LL * RA * RA : op + 8LL * RA * RA;
-        k_slot_rows<<<grid_for(n * qd * R, sms), 256, 0, st>>>(L, pl.sh_list.ptr, slot0, n, qd, R, pl.sh_x.ptr, false);
-        SFMM_CHECK_LAUNCH();
-        SFMM_BLAS(cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, 8 * R, static_cast<int>(n * qd), R, &one, opl, 8 * R, pl.sh_x.ptr, R,
-                              &zero, pl.sh_y.ptr, 8 * R));
-        k_l2l_scatter<<<grid_for(nc * qd * R, sms), 256, 0, st>>>(L, a.key, a.parent, pl.sh_slot.ptr, base, slot0, c0, nc, qd, R,
-                                                                 pl.sh_y.ptr);
-        SFMM_CHECK_LAUNCH();
-    }
+    const int64_t per_level = (m2m_frags(RA) + l2l_frags(RA) + l2l_frags(RB)) * 32;
+    const double* op = pl.sh_ops.ptr + per_level * (lc - 3);
+    const L2LSide sa{op + m2m_frags(RA) * 32, RA, a.want_pot ? reinterpret_cast<double*>(a.LA) : nullptr};
+    const L2LSide sb{op + (m2m_frags(RA) + l2l_frags(RA)) * 32, RB, a.want_field ? reinterpret_cast<double*>(a.LB) : nullptr};
+    const int64_t ncols = n * qd;
+    constexpr int NC = 8 * kL2LTiles;
+    const size_t smem = size_t(NC) * shift_ld(4 * cdiv(RB, 4)) * sizeof(double);
+    k_l2l_mma<kL2LTiles><<<dim3(static_cast<unsigned>((ncols + NC - 1) / NC), 2), 32 * kShiftWarps, smem, st>>>(
+        sa, sb, pl.sh_list.ptr, slot0, ncols, qd, t.child_beg.ptr, t.nchild.ptr, t.key.ptr);
+    SFMM_CHECK_LAUNCH();
 }
 
 }  // namespace sfmm
