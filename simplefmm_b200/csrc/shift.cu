@@ -37,6 +37,8 @@ namespace {
 
 constexpr int kShiftCols = 32;            // M2M columns per block: four 8-column MMA tiles
 constexpr int kL2LTiles = 8;              // L2L: eight 8-column MMA tiles (64 columns) per block
+constexpr int kL2LRowGroups = 8;          // L2L: the 8R output rows split over 8 blocks
+constexpr int kM2MRowGroups = 4;          // M2M: the R output rows split over 4 blocks
 constexpr int kShiftWarps = 8;
 
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
@@ -179,6 +181,8 @@ __global__ void __launch_bounds__(32 * kShiftWarps) k_m2m_mma(const double* __re
     __shared__ ShiftTile tile;
     extern __shared__ double Bs[];        // [32 cols][LD]
     const int RT = cdiv(R, 8), KC = cdiv(R, 4), LD = shift_ld(4 * KC);
+    // this block's share of the R output rows: row tiles [rt0, rt1)
+    const int per = cdiv(RT, gridDim.y), rt0 = blockIdx.y * per, rt1 = min(RT, rt0 + per);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, lr = lane >> 2, lc = lane & 3;
     shift_tile(tile, list, slot0, ncols, qd, child_beg, nchild, key);
     double acc[kMaxRowTiles][4][2];
@@ -197,22 +201,32 @@ __global__ void __launch_bounds__(32 * kShiftWarps) k_m2m_mma(const double* __re
         const double* fo = op + int64_t(oct) * RT * KC * 32 + lane;
 #pragma unroll
         for (int j = 0; j < kMaxRowTiles; ++j) {
-            const int rt = warp + kShiftWarps * j;
-            if (rt >= RT) break;
+            const int rt = rt0 + warp + kShiftWarps * j;
+            if (rt >= rt1) break;
             const double* fr = fo + int64_t(rt) * KC * 32;
             const int kce = m2m_kc_end(rt, R);
-            for (int kc = 0; kc < kce; ++kc) {
-                const double a = __ldg(fr + kc * 32);
+            // operator fragments four K chunks ahead of their products
+            double a4[4];
 #pragma unroll
-                for (int q = 0; q < 4; ++q)
-                    mma884(acc[j][q][0], acc[j][q][1], a, Bs[(q * 8 + lr) * LD + 4 * kc + lc]);
+            for (int u = 0; u < 4; ++u) a4[u] = u < kce ? __ldg(fr + u * 32) : 0.0;
+            for (int kc = 0; kc < kce; kc += 4) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const double a = a4[u];
+                    a4[u] = kc + 4 + u < kce ? __ldg(fr + (kc + 4 + u) * 32) : 0.0;
+                    if (kc + u < kce) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q)
+                            mma884(acc[j][q][0], acc[j][q][1], a, Bs[(q * 8 + lr) * LD + 4 * (kc + u) + lc]);
+                    }
+                }
             }
         }
     }
 #pragma unroll
     for (int j = 0; j < kMaxRowTiles; ++j) {
-        const int rt = warp + kShiftWarps * j;
-        if (rt >= RT) break;
+        const int rt = rt0 + warp + kShiftWarps * j;
+        if (rt >= rt1) break;
         const int r = 8 * rt + lr;
         if (r >= R) continue;
 #pragma unroll
@@ -255,13 +269,27 @@ __global__ void __launch_bounds__(32 * kShiftWarps) k_l2l_mma(L2LSide sa, L2LSid
         Bs[e] = (k < R && g >= 0) ? sd.L[(int64_t(g) * qd + tile[c / kShiftCols].b[c % kShiftCols]) * R + k] : 0.0;
     }
     __syncthreads();
-    for (int rt = warp; rt < RT8; rt += kShiftWarps) {
+    // this block's share of the 8R output rows: row tiles [rt0, rt1)
+    const int per = cdiv(RT8, gridDim.z), rt0 = blockIdx.z * per, rt1 = min(RT8, rt0 + per);
+    for (int rt = rt0 + warp; rt < rt1; rt += kShiftWarps) {
         double acc[NQ][2] = {};
         const double* fr = sd.op + int64_t(rt) * KC * 32 + lane;
-        for (int kc = l2l_kc_begin(rt, R); kc < KC; ++kc) {
-            const double a = __ldg(fr + kc * 32);
+        const int kcb = l2l_kc_begin(rt, R);
+        // operator fragments four K chunks ahead of their products
+        double a4[4];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) mma884(acc[q][0], acc[q][1], a, Bs[(q * 8 + lr) * LD + 4 * kc + lc]);
+        for (int u = 0; u < 4; ++u) a4[u] = kcb + u < KC ? __ldg(fr + (kcb + u) * 32) : 0.0;
+        for (int kc = kcb; kc < KC; kc += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const double a = a4[u];
+                a4[u] = kc + 4 + u < KC ? __ldg(fr + (kc + 4 + u) * 32) : 0.0;
+                if (kc + u < KC) {
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q)
+                        mma884(acc[q][0], acc[q][1], a, Bs[(q * 8 + lr) * LD + 4 * (kc + u) + lc]);
+                }
+            }
         }
         const int row = 8 * rt + lr, oct = row / R, i = row - oct * R;
 #pragma unroll
@@ -352,7 +380,8 @@ void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st)
     const double* op = pl.sh_ops.ptr + per_level * (lc - 3);
     const int64_t ncols = n * qd;
     const size_t smem = size_t(kShiftCols) * shift_ld(4 * cdiv(R, 4)) * sizeof(double);
-    k_m2m_mma<<<static_cast<unsigned>((ncols + kShiftCols - 1) / kShiftCols), 32 * kShiftWarps, smem, st>>>(
+    k_m2m_mma<<<dim3(static_cast<unsigned>((ncols + kShiftCols - 1) / kShiftCols), kM2MRowGroups), 32 * kShiftWarps, smem,
+                st>>>(
         op, R, pl.sh_list.ptr, slot0, ncols, qd, t.child_beg.ptr, t.nchild.ptr, t.key.ptr, reinterpret_cast<double*>(a.M));
     SFMM_CHECK_LAUNCH();
 }
@@ -371,7 +400,7 @@ void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st)
     const int64_t ncols = n * qd;
     constexpr int NC = 8 * kL2LTiles;
     const size_t smem = size_t(NC) * shift_ld(4 * cdiv(RB, 4)) * sizeof(double);
-    k_l2l_mma<kL2LTiles><<<dim3(static_cast<unsigned>((ncols + NC - 1) / NC), 2), 32 * kShiftWarps, smem, st>>>(
+    k_l2l_mma<kL2LTiles><<<dim3(static_cast<unsigned>((ncols + NC - 1) / NC), 2, kL2LRowGroups), 32 * kShiftWarps, smem, st>>>(
         sa, sb, pl.sh_list.ptr, slot0, ncols, qd, t.child_beg.ptr, t.nchild.ptr, t.key.ptr);
     SFMM_CHECK_LAUNCH();
 }
