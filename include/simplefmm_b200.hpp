@@ -171,6 +171,10 @@ public:
         fmm_plan* pl = nullptr;
         check(fmm_plan_create(partitioner.handle(), p, static_cast<int>(N), precision, &pl));
         plan_.reset(pl);
+#ifdef FMM_M2L_DIRECT
+        // the reference's build option for the dense M2L (fmm.hpp:700-712)
+        check(fmm_plan_set_m2l(plan_.get(), FMM_M2L_DIRECT));
+#endif
     }
 
     // fmm.hpp:204, 398-408: self_generator(i) names the sources whose

@@ -31,7 +31,11 @@ FLAG_EXCLUDE = 128       # self_generator {i, i+s1, i+s2} with the matching is_s
 FLAG_EXCLUDE_FAR = 256   # the same generator, default is_self (only non-neighbours removed)
 
 
-def ref_binary(native: bool = False) -> Path:
+def ref_binary(native: bool = False, direct: bool = False) -> Path:
+    """The compiled reference: portable, -march=native, or -march=native with
+    the reference's dense-M2L build option (-DFMM_M2L_DIRECT)."""
+    if direct:
+        return REF_DIR / "ref_driver_direct"
     return REF_DIR / ("ref_driver_native" if native else "ref_driver")
 
 
@@ -84,9 +88,9 @@ def read_output(path) -> dict:
 
 
 def run_reference(pos, q, p, max_level=20, max_ppn=64, vertical_axis=2, phideg=0.0,
-                  flags=FLAG_POT, ranks=1, native=False, timeout=3600, box=None, strides=None) -> dict:
+                  flags=FLAG_POT, ranks=1, native=False, timeout=3600, box=None, strides=None, direct=False) -> dict:
     """Run the compiled reference on (pos, q) and return its parsed output."""
-    binary = ref_binary(native)
+    binary = ref_binary(native, direct)
     if not binary.exists():
         raise FileNotFoundError(f"{binary} is not built (make -C oracle ref)")
     with tempfile.TemporaryDirectory() as td:

@@ -62,6 +62,7 @@ def load_library():
         "fmm_tree_destroy": ([vp], i32),
         "fmm_tree_build_box": ([vp, vp, i64, i32, C.POINTER(dbl), dbl, i32, i32, i32, dbl, C.POINTER(vp)], i32),
         "fmm_plan_set_exclusions": ([vp, vp, vp, i32, i32], i32),
+        "fmm_plan_set_m2l": ([vp, i32], i32),
         "fmm_plan_capture": ([vp, vp, vp, vp], i32),
         "fmm_plan_replay": ([vp], i32),
         "fmm_tree_depth": ([vp, C.POINTER(i32)], i32),
@@ -259,6 +260,12 @@ class Plan:
         h = C.c_void_p()
         _check(load_library().fmm_plan_create(tree._h, p, qdim, PRECISION[precision], C.byref(h)))
         self._h = h
+
+    def set_m2l(self, method: str):
+        """M2L formulation: "rotation" (default) or "direct", the reference's
+        FMM_M2L_DIRECT option (fmm_plan_set_m2l)."""
+        _check(load_library().fmm_plan_set_m2l(self._h, {"rotation": 0, "direct": 1}[method]))
+        return self
 
     def evaluate(self, Q, pot=None, field=None):
         """pot += potential, field += field (either may be None).  numpy arrays

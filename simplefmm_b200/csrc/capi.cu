@@ -265,6 +265,15 @@ int fmm_plan_set_exclusions(fmm_plan* plan, const int64_t* row_ptr, const int32_
     API_CATCH
 }
 
+int fmm_plan_set_m2l(fmm_plan* plan, int method)
+{
+    API_TRY
+    if (!plan) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL plan");
+    bind(*plan->pl.tree->ctx);
+    sfmm::plan_set_m2l(plan->pl, method);
+    API_CATCH
+}
+
 int fmm_tree_destroy(fmm_tree* tree)
 {
     API_TRY

@@ -341,6 +341,38 @@ static std::shared_ptr<PlanTables> tables_on_device(int device, int p, bool mixe
     return t;
 }
 
+static std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int p, cudaStream_t st)
+{
+    static std::mutex mu;
+    static auto* cache = new std::map<std::pair<int, int>, std::shared_ptr<DirectDevTables>>();   // kept until exit
+    std::lock_guard<std::mutex> lk(mu);
+    auto& slot = (*cache)[std::make_pair(device, p)];
+    if (slot) return slot;
+    const DirectTables h = make_direct_tables(p);
+    auto t = std::make_shared<DirectDevTables>();
+    upload(t->coef, h.coef, st);
+    upload(t->zil, h.zil, st);
+    upload(t->eil2, h.eil2, st);
+    t->ncoef = h.ncoef;
+    t->nz = h.nz;
+    t->ne = h.ne;
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    slot = t;
+    return t;
+}
+
+void plan_set_m2l(Plan& pl, int method)
+{
+    SFMM_REQUIRE(method == FMM_M2L_ROTATION || method == FMM_M2L_DIRECT, FMM_ERR_INVALID_ARGUMENT,
+                 "method must be FMM_M2L_ROTATION or FMM_M2L_DIRECT");
+    if (method == FMM_M2L_DIRECT) {
+        SFMM_REQUIRE(pl.precision == FMM_PRECISION_FP64, FMM_ERR_UNSUPPORTED, "the direct M2L is FP64 only");
+        SFMM_REQUIRE(pl.T + pl.T1 <= 512, FMM_ERR_UNSUPPORTED, "the direct M2L takes p <= 20");
+        if (!pl.dtab) pl.dtab = direct_tables_on_device(pl.tree->ctx->device, pl.p, pl.tree->ctx->stream);
+    }
+    pl.m2l_method = method;
+}
+
 void plan_init(Plan& pl)
 {
     Tree& t = *pl.tree;
@@ -465,6 +497,15 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.p2p_ctr = pl.p2p_ctr.ptr;
     a.m2l_ctr = pl.m2l_ctr.ptr;
     a.m2l_force_rows = pl.m2l_force_rows;
+    a.m2l_direct = pl.m2l_method == FMM_M2L_DIRECT;
+    if (a.m2l_direct) {
+        a.dcoef = pl.dtab->coef.ptr;
+        a.dncoef = pl.dtab->ncoef;
+        a.dzil = pl.dtab->zil.ptr;
+        a.dnz = pl.dtab->nz;
+        a.deil2 = reinterpret_cast<const cplx*>(pl.dtab->eil2.ptr);
+        a.dne = pl.dtab->ne;
+    }
     a.p2p_split = pl.p2p_rows > 0;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;
@@ -514,7 +555,8 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
             SFMM_CHECK_LAUNCH();
         }
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
-        launch_m2l(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
+        if (a.m2l_direct) launch_m2l_direct(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
+        else launch_m2l(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
         near_field();
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
         const size_t head2 = (32 + 2 * 4 * (2 * kMaxOrder + 1) + 2 * 4 * (2 * kMaxOrder + 3)) * sizeof(double);

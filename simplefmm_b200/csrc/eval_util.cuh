@@ -40,6 +40,8 @@ static __device__ __forceinline__ void tri_nm(int t, int& n, int& m)
 
 // M2L over all sibling groups (children of nodes in [g0, g1)), m2l.cu.
 void launch_m2l(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st);
+// The same with the direct (dense) formulation, m2l_direct.cu.
+void launch_m2l_direct(const EvalArgs& a, int64_t g0, int64_t g1, int sms, cudaStream_t st);
 
 // Near field of every leaf into a.out2, p2p.cu.
 void launch_p2p(const EvalArgs& a, int sms, cudaStream_t st);

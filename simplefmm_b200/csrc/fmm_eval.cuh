@@ -84,6 +84,15 @@ struct EvalArgs {
     int* p2p_ctr;
     int* m2l_ctr;                         // FP64 M2L: the counter blocks take sibling groups from
     int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
+    // direct M2L (m2l_direct.cu, FMM_M2L_DIRECT): dense coefficient table,
+    // Z of the interaction-list angles, phases; row lengths
+    int m2l_direct;
+    const double* dcoef;
+    int dncoef;
+    const double* dzil;
+    int dnz;
+    const cplx* deil2;
+    int dne;
     int p2p_split;                        // some leaf has more than one part
     double* out;                         // far field per component, sorted order
     double* out2;                        // near field per component, sorted order
@@ -100,6 +109,12 @@ struct PlanTables {
     int rfrag_nf = 0;
     DevBuf<float> rf32, tz32, tzl32;
     int rf32_nf = 0, tz32_nf = 0;
+};
+
+// Direct-M2L tables of one order on one device (shared like PlanTables).
+struct DirectDevTables {
+    DevBuf<double> coef, zil, eil2;
+    int ncoef = 0, nz = 0, ne = 0;
 };
 
 struct Plan {
@@ -123,6 +138,8 @@ struct Plan {
     DevBuf<int32_t> p2p_row, p2p_parts, p2p_rowoff, p2p_ctr;
     DevBuf<int32_t> m2l_ctr;                  // M2L group counter (m2l.cu)
     bool m2l_force_rows = false;              // SFMM_M2L_KERNEL=rows at plan creation
+    int m2l_method = FMM_M2L_ROTATION;        // fmm_plan_set_m2l
+    std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_DIRECT
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
@@ -155,6 +172,9 @@ void p2p_setup(Plan& pl);
 // FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
 void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);
 void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
+// Selects the M2L formulation (FMM_M2L_ROTATION / FMM_M2L_DIRECT); the
+// direct one's tables are built on first use per (device, p).
+void plan_set_m2l(Plan& pl, int method);
 void plan_read_timings(Plan& pl, double* ms6);
 // Exclusions (exclude.cu): ptr / cols are device arrays (n + 1, ptr[n]).
 void plan_set_exclusions(Plan& pl, const int64_t* ptr, const int32_t* cols, int near_too);

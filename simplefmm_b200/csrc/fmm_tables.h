@@ -42,4 +42,19 @@ struct HostTables {
 
 HostTables make_tables(int p);
 
+// Tables of the direct (dense) M2L, the reference's M2Lc_direct
+// (fmm.hpp:317-337, 592-618), for target orders j <= p + 1 (the field local)
+// and source orders n <= p:
+//   coef  [tri(j, k)][n (n + 1) + m]  (-1)^(fkm(k - m, k) + n) A(n,m) A(j,k) / A(j+n, m-k)
+//         (the dk >= 0 form; dk < 0 multiplies by (-1)^((j+n) - (m-k)))
+//   zil   [16 |dk| + 4 |dj| + |di|][tri(n, m)]  Z(n, m, acos(|dk| / |d|)), n <= 2p + 1
+//   eil2  [7 (dj + 3) + (di + 3)][q + 2p + 1]  e^{i q atan2(dj, di)}, |q| <= 2p + 1 (re, im)
+struct DirectTables {
+    int p = 0;
+    int ncoef = 0, nz = 0, ne = 0;       // row lengths of coef / zil / eil2
+    std::vector<double> coef, zil, eil2;
+};
+
+DirectTables make_direct_tables(int p);
+
 }  // namespace sfmm

@@ -417,7 +417,7 @@ __host__ __device__ constexpr int az_off(int P, int k) { return k * (P + 1) - k 
 
 __device__ __forceinline__ void mma884(double& d0, double& d1, double a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }

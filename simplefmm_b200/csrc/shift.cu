@@ -37,8 +37,8 @@ namespace {
 
 constexpr int kShiftCols = 32;            // M2M columns per block: four 8-column MMA tiles
 constexpr int kL2LTiles = 8;              // L2L: eight 8-column MMA tiles (64 columns) per block
-constexpr int kL2LRowGroups = 8;          // L2L: the 8R output rows split over 8 blocks
-constexpr int kM2MRowGroups = 4;          // M2M: the R output rows split over 4 blocks
+constexpr int kL2LRowGroups = 4;          // L2L: the 8R output rows split over 4 blocks
+constexpr int kM2MRowGroups = 2;          // M2M: the R output rows split over 2 blocks
 constexpr int kShiftWarps = 8;
 
 __host__ __device__ constexpr int cdiv(int a, int b) { return (a + b - 1) / b; }
@@ -54,7 +54,7 @@ __host__ __device__ constexpr int shift_ld(int k)
 
 __device__ __forceinline__ void mma884(double& d0, double& d1, double a, double b)
 {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+    asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
                  : "+d"(d0), "+d"(d1)
                  : "d"(a), "d"(b));
 }

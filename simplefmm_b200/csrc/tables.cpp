@@ -210,4 +210,47 @@ HostTables make_tables(int p)
     return t;
 }
 
+DirectTables make_direct_tables(int p)
+{
+    DirectTables d;
+    d.p = p;
+    const int jmax = p + 1, nzmax = 2 * p + 1;
+    std::vector<double> A((2 * nzmax + 2) * (2 * nzmax + 3) / 2);
+    for (int n = 0; n <= 2 * nzmax; ++n)
+        for (int m = 0; m <= n; ++m) A[tri(n, m)] = Afun(n, m);
+    auto a = [&](int n, int m) { return A[tri(n, std::abs(m))]; };
+    d.ncoef = (p + 1) * (p + 1);
+    const int T1 = (jmax + 1) * (jmax + 2) / 2;
+    d.coef.assign(size_t(T1) * d.ncoef, 0.0);
+    for (int j = 0; j <= jmax; ++j)
+        for (int k = 0; k <= j; ++k)
+            for (int n = 0; n <= p; ++n)
+                for (int m = -n; m <= n; ++m)
+                    d.coef[size_t(tri(j, k)) * d.ncoef + n * (n + 1) + m] =
+                        sgn_pow(fkm(k - m, k) + n) * a(n, m) * a(j, k) / a(j + n, m - k);
+    d.nz = (nzmax + 1) * (nzmax + 2) / 2;
+    d.zil.assign(size_t(64) * d.nz, 0.0);
+    for (int k = 0; k < 4; ++k)
+        for (int j = 0; j < 4; ++j)
+            for (int i = 0; i < 4; ++i) {
+                if (i + j + k < 2) continue;
+                const double th = std::acos(k / std::sqrt(double(i * i + j * j + k * k)));
+                for (int n = 0; n <= nzmax; ++n)
+                    for (int m = 0; m <= n; ++m) d.zil[size_t(16 * k + 4 * j + i) * d.nz + tri(n, m)] = Zfun(n, m, th);
+            }
+    d.ne = 2 * nzmax + 1;
+    d.eil2.assign(size_t(49) * d.ne * 2, 0.0);
+    for (int dj = -3; dj <= 3; ++dj)
+        for (int di = -3; di <= 3; ++di) {
+            const double ph = std::atan2(double(dj), double(di));
+            for (int q = -nzmax; q <= nzmax; ++q) {
+                const std::complex<double> e = std::polar(1.0, q * ph);
+                const size_t o = (size_t(7 * (dj + 3) + (di + 3)) * d.ne + (q + nzmax)) * 2;
+                d.eil2[o] = e.real();
+                d.eil2[o + 1] = e.imag();
+            }
+        }
+    return d;
+}
+
 }  // namespace sfmm

@@ -44,6 +44,11 @@ CASES = {
                              "uniform", 1),
 }
 
+# cases run by the reference built with its dense-M2L option (-DFMM_M2L_DIRECT)
+DIRECT = {"direct_plummer_n4000_p8": ("plummer", 4000, 27, 8, 20, 32, 2, 0.0, POT | FIELD, "uniform", 1),
+          "direct_vector_n2000_p6": ("uniform", 2000, 28, 6, 20, 64, 2, 0.0, VEC | BIOT, "uniform", 3)}
+CASES.update(DIRECT)
+
 # explicit root cube (corner, width) and exclusion strides of the cases above
 BOXES = {"box_n3000_p6": ((-0.25, -0.5, -0.125), 2.0)}
 STRIDES = {"exclude_n3000_p6": (1, 1777), "exclude_far_n3000_p6": (1, 1777)}
@@ -54,7 +59,8 @@ def make_case(name, spec):
     pos = W.points(dist, n, seed)
     q = W.charges(n, seed, qkind, qdim)
     out = refio.run_reference(pos, q, p=p, max_level=max_level, max_ppn=ppn, vertical_axis=va,
-                              phideg=phideg, flags=flags, native=True, box=BOXES.get(name), strides=STRIDES.get(name))
+                              phideg=phideg, flags=flags, native=True, box=BOXES.get(name), strides=STRIDES.get(name),
+                              direct=name in DIRECT)
     arrays = {k: v for k, v in out.items() if not k.startswith("T_")}
     if name in BOXES:
         arrays["box_corner"] = np.array(BOXES[name][0])
@@ -62,6 +68,8 @@ def make_case(name, spec):
     if name in STRIDES:
         arrays["strides"] = np.array(STRIDES[name])
     meta = np.array([n, seed, p, max_level, ppn, va, flags, qdim], dtype=np.int64)
+    if name in DIRECT:
+        arrays["m2l_direct"] = np.array([1])
     np.savez_compressed(HERE / f"{name}.npz", pos=pos, q=q, meta=meta, phideg=np.array([phideg]),
                         dist=np.array([dist]), **arrays)
 

@@ -42,6 +42,8 @@ def test_results_match_reference(ctx, name):
     g = load_golden(name)
     t = golden_tree(sf, g, ctx)
     plan = sf.Plan(t, g["p"], g["qdim"])
+    if "m2l_direct" in g:                # the reference built with -DFMM_M2L_DIRECT: the same option here
+        plan.set_m2l("direct")
     ex = golden_exclusions(g)
     if ex is not None:
         plan.set_exclusions(*ex)
@@ -296,3 +298,48 @@ def test_lowest_orders_against_restatement(ctx, p):
     sp, sfl = pyoracle.error_scales(pos, q)
     assert rel_err_per_target(pot, opot, sp) < TOL
     assert rel_err_per_target(field, ofield, sfl) < TOL
+
+
+@pytest.mark.parametrize("name", ["uniform_n3000_p6", "plummer_n6000_p5_ppn32", "gauss2_n4000_p8", "uniform_n3000_p12",
+                                  "vector_n2000_p8_ppn128", "exclude_n3000_p6", "plummer_n3000_p16_ppn32",
+                                  "direct_plummer_n4000_p8", "direct_vector_n2000_p6"])
+def test_direct_m2l_matches_reference(ctx, name):
+    """The reference's FMM_M2L_DIRECT formulation (M2Lc_direct, fmm.hpp:592-618):
+    the dense M2L reproduces the reference's results to the same 1e-12."""
+    g = load_golden(name)
+    t = golden_tree(sf, g, ctx)
+    plan = sf.Plan(t, g["p"], g["qdim"]).set_m2l("direct")
+    ex = golden_exclusions(g)
+    if ex is not None:
+        plan.set_exclusions(*ex)
+    sp, sf_ = pyoracle.error_scales(g["pos"], g["q"])
+    n = g["n"]
+    if g["qdim"] == 1:
+        pot = np.zeros(n)
+        field = np.zeros((n, 3)) if "FIELD" in g else None
+        plan.evaluate(g["q"], pot, field)
+        assert rel_err_per_target(pot, g["POT"], sp) < TOL
+        if field is not None:
+            assert rel_err_per_target(field, g["FIELD"], sf_) < TOL
+    else:
+        vp, bi = np.zeros((n, 3)), np.zeros((n, 3))
+        plan.rinv(g["q"], vp)
+        plan.rinv(g["q"], bi, gradient=True)
+        assert rel_err_per_target(vp, g["VECPOT"], sp) < TOL
+        assert rel_err_per_target(bi, g["BIOT"], sf_) < TOL
+
+
+def test_direct_m2l_equals_rotation_on_a_medium_case(ctx):
+    """The two M2L formulations on 40,000 Plummer points, p = 10: equal to
+    1e-12 per target (they differ in rounding order only)."""
+    n = 40_000
+    pos, q = W.points("plummer", n, 202), W.charges(n, 202)
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    pot_r, fld_r = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, 10, 1).evaluate(q, pot_r, fld_r)
+    pot_d, fld_d = np.zeros(n), np.zeros((n, 3))
+    sf.Plan(t, 10, 1).set_m2l("direct").evaluate(q, pot_d, fld_d)
+    tg = np.arange(0, n, 41)
+    sp, sfl = pyoracle.error_scales(pos, q, tg)
+    assert rel_err_per_target(pot_d[tg], pot_r[tg], sp) < TOL
+    assert rel_err_per_target(fld_d[tg], fld_r[tg], sfl) < TOL
