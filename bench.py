@@ -14,7 +14,9 @@ point.  Metric: points/s = N / (tree build + evaluation time).
          outputs) and the device->host copy of potential and field are inside
          the timed region.
 --gpus N runs N independent replicas (one process per GPU, launched by
-torch.distributed.run); value = all points / max-over-ranks time.
+torch.distributed.run); value = all points / max-over-ranks time.  With
+--shard, the N ranks split one solve instead (strong scaling; the moments,
+locals and outputs are summed with NCCL all-reduces between the stages).
 --impl reference times the reference's own CPU implementation (the compiled
 reference headers, run as one shim rank per host core) on a bounded sample of
 the same workload: the first 1M of its points.
@@ -267,9 +269,10 @@ def run_reference_arm(args):
 
 
 def workload_config(args, n: int, world: int) -> dict:
+    par = f"shard x{world} (one solve, NCCL all-reduce)" if getattr(args, "shard", False) and world > 1 else f"replicas x{world}"
     return {"workload": f"{args.dist}_n{n}_p{args.p}_leaf{LEAF}_{args.precision}_potential+field", "n": n,
             "p": args.p, "leaf": LEAF, "distribution": args.dist, "precision": args.precision,
-            "parallelism": f"replicas x{world}", "l2": "flushed (256 MiB write) between timed steps"}
+            "parallelism": par, "l2": "flushed (256 MiB write) between timed steps"}
 
 
 def serve_bench(args):
@@ -377,6 +380,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark instead of the solve benchmark")
+    ap.add_argument("--shard", action="store_true",
+                    help="with --gpus N > 1: one solve split over the N ranks (fmm_plan_set_shard, NCCL all-reduce of "
+                         "moments, locals and outputs; strong scaling) instead of N independent replicas")
     ap.add_argument("--requests", type=int, default=2000)
     ap.add_argument("--rate", type=float, default=100.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--slots", type=int, default=4)
@@ -416,6 +422,7 @@ def main():
     torch.cuda.synchronize()
 
     live = []
+    sharded = args.shard and world > 1
 
     def step():
         # one evaluation as a time-stepping caller runs it: release the
@@ -426,7 +433,13 @@ def main():
         fld_d.zero_()
         tree = sf.Tree(pos_d, 20, LEAF, ctx=ctx)
         plan = sf.Plan(tree, p, 1, precision=args.precision)
-        plan.evaluate(q_d, pot_d, fld_d)
+        if sharded:
+            plan.set_shard(rank, world)
+            plan.evaluate_sharded(q_d, pot_d, fld_d, allreduce=dist.all_reduce)
+            dist.all_reduce(pot_d)
+            dist.all_reduce(fld_d)
+        else:
+            plan.evaluate(q_d, pot_d, fld_d)
         live.extend([plan, tree])
         return tree, plan
 
@@ -458,7 +471,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
         dist.barrier()
-    value = n * world * args.steps / (total_ms * 1e-3)
+    value = n * (1 if sharded else world) * args.steps / (total_ms * 1e-3)
 
     # accuracy of the last step against the FP64 direct sum on seeded targets
     n_check = min(n, 10_000)
@@ -487,25 +500,57 @@ def main():
 
     e2e = None
     if not args.no_e2e:
+        # the same step through the public API with pinned host arrays: the
+        # host->device copies of the inputs (and of the accumulated outputs)
+        # and the device->host copy of the outputs are inside the timed region
         pin = lambda a: torch.from_numpy(a).pin_memory().numpy()  # noqa: E731
         pos_p, q_p = pin(pos_h), pin(q_h)
         pot_p, fld_p = pin(np.zeros(n)), pin(np.zeros((n, 3)))
         ctx2 = sf.Context(local)
-        tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
-        sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
+        if sharded:
+            ctx2.set_stream(stream.cuda_stream)
+
+        def e2e_step():
+            if not sharded:
+                tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
+                sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
+                return tr
+            pos_x = torch.from_numpy(pos_p).cuda(non_blocking=True)
+            q_x = torch.from_numpy(q_p).cuda(non_blocking=True)
+            pot_x = torch.from_numpy(pot_p).cuda(non_blocking=True)
+            fld_x = torch.from_numpy(fld_p).cuda(non_blocking=True)
+            tr = sf.Tree(pos_x, 20, LEAF, ctx=ctx2)
+            pl = sf.Plan(tr, p, 1, precision=args.precision).set_shard(rank, world)
+            pot_0, fld_0 = pot_x.clone(), fld_x.clone()
+            pl.evaluate_sharded(q_x, pot_x, fld_x, allreduce=dist.all_reduce)
+            pot_x.sub_(pot_0)                          # this shard's increments, summed over the shards
+            fld_x.sub_(fld_0)
+            dist.all_reduce(pot_x)
+            dist.all_reduce(fld_x)
+            pot_p[:] += pot_x.cpu().numpy()
+            fld_p[:] += fld_x.cpu().numpy()
+            return tr
+
+        e2e_step().close()
         et = []
         for _ in range(args.steps):
             pot_p[:] = 0
             fld_p[:] = 0
             flush.zero_()
             torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
             t0 = time.perf_counter()
-            tr.close()
-            tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
-            sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
+            tr = e2e_step()
+            torch.cuda.synchronize()
             et.append(time.perf_counter() - t0)
-        tr.close()
-        e2e = {"value": n * world / statistics.mean(et), "unit": "points/s",
+            tr.close()
+        e2e_s = statistics.mean(et)
+        if world > 1:
+            tt = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            e2e_s = float(tt.item())
+        e2e = {"value": n * (1 if sharded else world) / e2e_s, "unit": "points/s",
                "h2d_bytes_per_step": int(pos_p.nbytes + q_p.nbytes + pot_p.nbytes + fld_p.nbytes),
                "d2h_bytes_per_step": int(pot_p.nbytes + fld_p.nbytes)}
 
@@ -518,7 +563,7 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if sharded else "weak", "vs_baseline": None,
             "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
             "data": DATA_DESC.get(args.dist, f"synthetic (seeded {args.dist})"),
             "config": workload_config(args, n, world),

@@ -169,6 +169,33 @@ int fmm_rinv(fmm_plan* plan, const double* Q, double* U, int gradient, int where
    formulation of fmm.hpp:234-253 and 549-551. */
 int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, int where);
 
+/* ---- One solve split over several devices (no counterpart in the
+   reference's API; it mirrors the reference's MPI work split, fmm.hpp:503-522
+   and distributed.hpp:14-25, and its per-level MPI_Allreduce of moments and
+   locals, fmm.hpp:832-859).  Each process builds the same tree and a plan,
+   calls fmm_plan_set_shard(plan, index, count) and then evaluates in three
+   stages on device arrays, summing two exchange buffers across all shards
+   between them (an all-reduce, e.g. NCCL, on the context's stream):
+       fmm_evaluate_stage(plan, Q, pot, field, 0)   near field and moments of
+                                                    this shard's leaves
+       sum buffer 0 (moments) over the shards
+       fmm_evaluate_stage(plan, Q, pot, field, 1)   M2M, M2L into this shard's
+                                                    targets
+       sum buffers 1 and 2 (potential / field locals) over the shards
+       fmm_evaluate_stage(plan, Q, pot, field, 2)   L2L, L2P of this shard's
+                                                    leaves, sums into pot/field
+   pot / field then hold this shard's points' results added to their input
+   (other points unchanged); summing the shards' increments gives the solve.
+   Leaves are split level by level, balanced by points; M2L targets by
+   contiguous ranges of their parents.  Excluded interactions are removed by
+   shard 0.  The same pot / field pointers (or NULLs) must be passed to all
+   three stages.  count = 1 returns the plan to fmm_evaluate. */
+int fmm_plan_set_shard(fmm_plan* plan, int index, int count);
+int fmm_evaluate_stage(fmm_plan* plan, const double* Q, double* pot, double* field, int stage);
+/* Device address and length (doubles) of exchange buffer `which`: 0 the
+   moments, 1 the potential locals, 2 the field locals of every node. */
+int fmm_plan_exchange_buffer(fmm_plan* plan, int which, void** device_ptr, int64_t* count);
+
 /* Capture one evaluation of device arrays Q / pot / field (what fmm_evaluate
    with FMM_DEVICE does) as a CUDA graph, and launch it again on the context's
    stream with fmm_plan_replay -- for callers that evaluate the same tree

@@ -8,6 +8,7 @@
 // flat arrays.  Each function cites the reference lines it restates
 // (paths are relative to the reference checkout).  It is itself checked
 // against the compiled reference (oracle/_ref) by tests/test_oracle.py.
+#include "shard_ranges.h"   // the library's work split (simplefmm_b200/csrc), restated stages below
 #include <algorithm>
 #include <cmath>
 #include <complex>
@@ -471,6 +472,19 @@ struct Eval {
     std::vector<double> Zrho;             // per point x n2 (fmm.hpp:152)
     std::vector<cd> Zg;                   // per point x n2 x 3 (fmm.hpp:153)
     std::vector<std::vector<cd>> M, L;    // per level: node x n2 x nc
+    // sharded stages (oracle_eval_*): this shard's leaves per level, its
+    // parents of M2L targets per level, its points; empty = everything
+    std::vector<std::vector<char>> own_leaf;
+    std::vector<int64_t> own_par_b, own_par_e;
+    std::vector<char> own_pt;
+
+    bool leaf_mine(int l, size_t f) const { return own_leaf.empty() || own_leaf[l][f]; }
+    bool target_mine(int l, size_t i) const
+    {
+        if (own_par_b.empty()) return true;
+        const int64_t ip = T.lv[l].pl_idx[i];
+        return ip >= own_par_b[l - 1] && ip < own_par_e[l - 1];
+    }
 
     cd& m(int l, int node, int nm, int c) { return M[l][(size_t(node) * n2 + nm) * nc + c]; }
     cd& lc(int l, int node, int nm, int c) { return L[l][(size_t(node) * n2 + nm) * nc + c]; }
@@ -525,6 +539,7 @@ struct Eval {
     {
         const Level& Lv = T.lv[l];
         for (size_t f = 0; f < Lv.leaf_node.size(); ++f) {
+            if (!leaf_mine(l, f)) continue;
             const int node = Lv.leaf_node[f];
             for (int e = Lv.idx_ptr[f]; e < Lv.idx_ptr[f + 1]; ++e) {
                 const int i = Lv.idx[e];
@@ -622,8 +637,10 @@ struct Eval {
     void M2L(int l)   // fmm.hpp:700-712
     {
         const Level& Lv = T.lv[l];
-        for (size_t i = 0; i < Lv.keys.size(); ++i)
+        for (size_t i = 0; i < Lv.keys.size(); ++i) {
+            if (!target_mine(l, i)) continue;
             for (int e = Lv.il_ptr[i]; e < Lv.il_ptr[i + 1]; ++e) M2L_pair(l, Lv.il_d[e], Lv.il_src[e], int(i));
+        }
     }
 
     // fmm.hpp:714-745
@@ -654,6 +671,7 @@ struct Eval {
     {
         const Level& Lv = T.lv[l];
         for (size_t f = 0; f < Lv.leaf_node.size(); ++f) {
+            if (!leaf_mine(l, f)) continue;
             const int node = Lv.leaf_node[f];
             for (int e = Lv.idx_ptr[f]; e < Lv.idx_ptr[f + 1]; ++e) {
                 const int i = Lv.idx[e];
@@ -679,6 +697,7 @@ struct Eval {
         const double* X = T.pos.data();
 #pragma omp parallel for schedule(dynamic, 256)
         for (int64_t i = 0; i < T.n; ++i) {
+            if (!own_pt.empty() && !own_pt[i]) continue;
             const auto [li, fi] = T.part[i];
             const Level& Lv = T.lv[li];
             for (int e = Lv.nl_ptr[fi]; e < Lv.nl_ptr[fi + 1]; ++e) {
@@ -728,6 +747,63 @@ struct Eval {
             L2N(D, U);
         }
         N2N(Q, U);
+    }
+
+    // One shard's share (shard_ranges.h): leaves per level balanced by points,
+    // M2L targets by contiguous ranges of their parents per level.
+    void set_shard(int index, int count)
+    {
+        own_leaf.assign(T.depth + 1, {});
+        own_par_b.assign(T.depth + 1, 0);
+        own_par_e.assign(T.depth + 1, 0);
+        own_pt.assign(T.n, 0);
+        for (int l = 0; l <= T.depth; ++l) {
+            const Level& Lv = T.lv[l];
+            const int64_t nl = int64_t(Lv.leaf_node.size());
+            std::vector<int64_t> prefix(Lv.idx_ptr.begin(), Lv.idx_ptr.end());
+            const auto r = sfmm::balanced_leaf_range(prefix.data(), nl, count, index);
+            own_leaf[l].assign(nl, 0);
+            for (int64_t f = r.first; f < r.second; ++f) {
+                own_leaf[l][f] = 1;
+                for (int e = Lv.idx_ptr[f]; e < Lv.idx_ptr[f + 1]; ++e) own_pt[Lv.idx[e]] = 1;
+            }
+            const int64_t nn = int64_t(Lv.keys.size());
+            own_par_b[l] = sfmm::shard_begin(nn, count, index);
+            own_par_e[l] = sfmm::shard_end(nn, count, index);
+        }
+    }
+
+    // The stages of the sharded solve; the caller sums every level's M
+    // across shards after stage 0 and every level's L after stage 1.
+    void stage(int s, const double* Q, double* U)
+    {
+        const int D = T.depth;
+        if (s == 0) {
+            M.assign(D + 1, {});
+            L.assign(D + 1, {});
+            if (D >= 2) {
+                precompute();
+                for (int l = 0; l <= D; ++l) {
+                    M[l].assign(T.lv[l].keys.size() * n2 * nc, 0);
+                    L[l].assign(T.lv[l].keys.size() * n2 * nc, 0);
+                }
+                for (int l = D; l >= 2; --l) N2M(l, Q);
+            }
+        } else if (s == 1) {
+            if (D >= 2) {
+                for (int l = D - 1; l >= 2; --l) M2M(l);
+                for (int l = 2; l <= D; ++l) M2L(l);
+            }
+        } else {
+            if (D >= 2) {
+                for (int l = 2; l < D; ++l) {
+                    L2N(l, U);
+                    L2L(l + 1);
+                }
+                L2N(D, U);
+            }
+            N2N(Q, U);
+        }
     }
 };
 
@@ -817,6 +893,53 @@ int oracle_rinv(void* tp, int p, int mode, int ncomp, const double* Q, double* U
     Eval ev{T, tb, p, (p + 1) * (p + 1), ncomp, mode == 1, {}, {}, {}, {}, {}};
     ev.rinv(Q, U);
     return 0;
+}
+
+// Sharded stages (the library's fmm_plan_set_shard / fmm_evaluate_stage,
+// restated): an evaluator object keeps M and L between stages.
+struct StagedEval {
+    Tables tb;
+    Eval ev;
+    StagedEval(const Tree& T, int p, int mode, int ncomp)
+        : tb(make_tables(p)), ev{T, tb, p, (p + 1) * (p + 1), ncomp, mode == 1, {}, {}, {}, {}, {}, {}, {}, {}, {}}
+    {
+    }
+};
+
+void* oracle_eval_create(void* tp, int p, int mode, int ncomp)
+{
+    if (p < 0 || p > 30 || (mode == 1 && ncomp != 3) || ncomp < 1) return nullptr;
+    return new StagedEval(*static_cast<Tree*>(tp), p, mode, ncomp);
+}
+
+void oracle_eval_free(void* e) { delete static_cast<StagedEval*>(e); }
+
+int oracle_eval_set_shard(void* e, int index, int count)
+{
+    if (count < 1 || index < 0 || index >= count) return -1;
+    static_cast<StagedEval*>(e)->ev.set_shard(index, count);
+    return 0;
+}
+
+int oracle_eval_stage(void* e, int stage, const double* Q, double* U)
+{
+    if (stage < 0 || stage > 2) return -1;
+    static_cast<StagedEval*>(e)->ev.stage(stage, Q, U);
+    return 0;
+}
+
+// Level l's moments (which 0) or locals (which 1) as count doubles (complex
+// pairs), for the caller's sum across shards; NULL if not allocated.
+double* oracle_eval_buffer(void* e, int which, int l, int64_t* count)
+{
+    Eval& ev = static_cast<StagedEval*>(e)->ev;
+    auto& v = which == 0 ? ev.M : ev.L;
+    if (l < 0 || l >= int(v.size())) {
+        *count = 0;
+        return nullptr;
+    }
+    *count = int64_t(v[l].size()) * 2;
+    return reinterpret_cast<double*>(v[l].data());
 }
 
 // O(N^2)-per-target direct sums (main.cpp:70-96) for the listed targets:

@@ -43,6 +43,13 @@ def lib():
         L.oracle_tree_export.restype = i64
         L.oracle_rinv.argtypes = [vp, C.c_int, C.c_int, C.c_int, dp, dp]
         L.oracle_direct.argtypes = [dp, i64, C.c_int, C.c_int, dp, C.POINTER(C.c_int64), i64, dp]
+        L.oracle_eval_create.argtypes = [vp, C.c_int, C.c_int, C.c_int]
+        L.oracle_eval_create.restype = vp
+        L.oracle_eval_free.argtypes = [vp]
+        L.oracle_eval_set_shard.argtypes = [vp, C.c_int, C.c_int]
+        L.oracle_eval_stage.argtypes = [vp, C.c_int, dp, dp]
+        L.oracle_eval_buffer.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int64)]
+        L.oracle_eval_buffer.restype = dp
         _lib = L
     return _lib
 
@@ -195,3 +202,44 @@ def subtract_exclusions(tree: "Tree", pos, Q, row_ptr, cols, near_too, pot=None,
                     field[i] -= Q[j] * R / r**3
                 else:
                     field[i] -= np.cross(Q[j], R) / r**3
+
+
+class ShardedEval:
+    """Restated sharded solve (the library's fmm_plan_set_shard /
+    fmm_evaluate_stage): ``stage(s, Q, U)`` for s = 0, 1, 2; between them the
+    caller sums ``buffers(0)`` (every level's moments) and then ``buffers(1)``
+    (every level's locals) over the shards.  U is accumulated with this
+    shard's points' results."""
+
+    def __init__(self, tree: Tree, p: int, ncomp: int = 1, gradient: bool = False):
+        self.tree = tree
+        self._h = lib().oracle_eval_create(tree._h, p, 1 if gradient else 0, ncomp)
+        if not self._h:
+            raise ValueError("oracle_eval_create rejected its arguments")
+
+    def set_shard(self, index: int, count: int):
+        if lib().oracle_eval_set_shard(self._h, index, count) != 0:
+            raise ValueError("bad shard")
+        return self
+
+    def stage(self, s: int, Q, U):
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        assert U.flags.c_contiguous and U.dtype == np.float64
+        if lib().oracle_eval_stage(self._h, s, _dp(Q), _dp(U)) != 0:
+            raise ValueError("bad stage")
+
+    def buffers(self, which: int):
+        """Per level, a numpy view (no copy) of the moments (0) or locals (1)."""
+        out = []
+        for level in range(self.tree.depth + 1):
+            cnt = C.c_int64()
+            ptr = lib().oracle_eval_buffer(self._h, which, level, C.byref(cnt))
+            if cnt.value and ptr:
+                out.append(np.ctypeslib.as_array(ptr, shape=(cnt.value,)))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            lib().oracle_eval_free(h)
+            self._h = None

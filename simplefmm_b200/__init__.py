@@ -63,6 +63,9 @@ def load_library():
         "fmm_tree_build_box": ([vp, vp, i64, i32, C.POINTER(dbl), dbl, i32, i32, i32, dbl, C.POINTER(vp)], i32),
         "fmm_plan_set_exclusions": ([vp, vp, vp, i32, i32], i32),
         "fmm_plan_set_m2l": ([vp, i32], i32),
+        "fmm_plan_set_shard": ([vp, i32, i32], i32),
+        "fmm_evaluate_stage": ([vp, vp, vp, vp, i32], i32),
+        "fmm_plan_exchange_buffer": ([vp, i32, C.POINTER(vp), C.POINTER(i64)], i32),
         "fmm_plan_capture": ([vp, vp, vp, vp], i32),
         "fmm_plan_replay": ([vp], i32),
         "fmm_tree_depth": ([vp, C.POINTER(i32)], i32),
@@ -93,6 +96,14 @@ def load_library():
         f.restype = res
     _lib = L
     return L
+
+
+class _DeviceArray:
+    """A float64 device array by address, for torch.as_tensor."""
+
+    def __init__(self, ptr: int, count: int):
+        self.__cuda_array_interface__ = {"shape": (count,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
 
 
 def _check(rc: int):
@@ -260,6 +271,43 @@ class Plan:
         h = C.c_void_p()
         _check(load_library().fmm_plan_create(tree._h, p, qdim, PRECISION[precision], C.byref(h)))
         self._h = h
+
+    def set_shard(self, index: int, count: int):
+        """This plan's share of one solve split over `count` devices
+        (fmm_plan_set_shard); evaluate it with evaluate_sharded."""
+        _check(load_library().fmm_plan_set_shard(self._h, index, count))
+        return self
+
+    def exchange_buffer(self, which: int):
+        """Device buffer `which` (0 moments, 1 potential locals, 2 field
+        locals) as a flat float64 CUDA tensor sharing the plan's memory."""
+        import torch
+
+        ptr, cnt = C.c_void_p(), C.c_int64()
+        _check(load_library().fmm_plan_exchange_buffer(self._h, which, C.byref(ptr), C.byref(cnt)))
+        return torch.as_tensor(_DeviceArray(ptr.value, cnt.value), device="cuda")
+
+    def evaluate_stage(self, Q, pot, field, stage: int):
+        """One stage (0, 1, 2) of a sharded evaluation on CUDA tensors."""
+        ptrs = []
+        for arr in (Q, pot, field):
+            addr, where = _ptr(arr)
+            if arr is not None and where != DEVICE:
+                raise FMMError(1, "sharded evaluation takes device arrays")
+            ptrs.append(C.c_void_p(addr) if arr is not None else None)
+        _check(load_library().fmm_evaluate_stage(self._h, *ptrs, stage))
+
+    def evaluate_sharded(self, Q, pot=None, field=None, allreduce=None):
+        """All three stages of this shard's share; allreduce(tensor) must sum
+        a tensor in place over the shards (e.g. torch.distributed.all_reduce
+        on NCCL) -- it runs on the moments after stage 0 and on both locals
+        after stage 1.  pot / field receive this shard's points' results."""
+        self.evaluate_stage(Q, pot, field, 0)
+        allreduce(self.exchange_buffer(0))
+        self.evaluate_stage(Q, pot, field, 1)
+        allreduce(self.exchange_buffer(1))
+        allreduce(self.exchange_buffer(2))
+        self.evaluate_stage(Q, pot, field, 2)
 
     def set_m2l(self, method: str):
         """M2L formulation: "rotation" (default) or "direct", the reference's

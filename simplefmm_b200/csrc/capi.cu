@@ -274,6 +274,37 @@ int fmm_plan_set_m2l(fmm_plan* plan, int method)
     API_CATCH
 }
 
+int fmm_plan_set_shard(fmm_plan* plan, int index, int count)
+{
+    API_TRY
+    if (!plan) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL plan");
+    bind(*plan->pl.tree->ctx);
+    sfmm::plan_set_shard(plan->pl, index, count);
+    API_CATCH
+}
+
+int fmm_evaluate_stage(fmm_plan* plan, const double* Q, double* pot, double* field, int stage)
+{
+    API_TRY
+    if (!plan || !Q) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    sfmm::Plan& pl = plan->pl;
+    if (field && pl.qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs N = 1 or N = 3 charges");
+    bind(*pl.tree->ctx);
+    sfmm::plan_evaluate_stage(pl, Q, pot, field, stage);
+    API_CATCH
+}
+
+int fmm_plan_exchange_buffer(fmm_plan* plan, int which, void** device_ptr, int64_t* count)
+{
+    if (!plan || !device_ptr || !count) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    sfmm::Plan& pl = plan->pl;
+    sfmm::DevBuf<double2>* b = which == 0 ? &pl.M : which == 1 ? &pl.LA : which == 2 ? &pl.LB : nullptr;
+    if (!b) return fail(FMM_ERR_INVALID_ARGUMENT, "which must be 0 (moments), 1 (potential locals) or 2 (field locals)");
+    *device_ptr = b->ptr;
+    *count = static_cast<int64_t>(b->count) * 2;
+    return FMM_OK;
+}
+
 int fmm_tree_destroy(fmm_tree* tree)
 {
     API_TRY

@@ -23,6 +23,7 @@
 
 #include "eval_util.cuh"
 #include "fmm_tables.h"
+#include "shard_ranges.h"
 
 namespace sfmm {
 
@@ -60,6 +61,10 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
     const int64_t nfar = a.n_leaves - a.far_leaf0;
     for (int64_t f = blockIdx.x * int64_t(nw) + w; f < nfar; f += int64_t(gridDim.x) * nw) {
         const int g = a.leaf_node[a.far_leaf0 + f];
+        if (a.own_leaf && !a.own_leaf[a.far_leaf0 + f]) {      // another shard's leaf: zero moments
+            for (int t = lane; t < a.qdim * a.T; t += 32) a.M[int64_t(g) * a.qdim * a.T + t] = cplx{0, 0};
+            continue;
+        }
         const int l = level_of(a, g);
         double c[3];
         node_center(*a.box, a.key[g], l, c);
@@ -197,6 +202,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
     cplx* loc = reinterpret_cast<cplx*>(smem) + w * K * T;
     const int64_t nfar = a.n_leaves - a.far_leaf0;
     for (int64_t f = blockIdx.x * int64_t(nw) + w; f < nfar; f += int64_t(gridDim.x) * nw) {
+        if (a.own_leaf && !a.own_leaf[a.far_leaf0 + f]) continue;   // another shard's leaf
         const int64_t g = a.leaf_node[a.far_leaf0 + f];
         const int l = level_of(a, g);
         double c[3];
@@ -412,10 +418,9 @@ void plan_init(Plan& pl)
     pl.out2.alloc(size_t(t.n) * kmax, st);
 }
 
-void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
+static EvalArgs make_args(Plan& pl, double* pot, double* field)
 {
     Tree& t = *pl.tree;
-    cudaStream_t st = t.ctx->stream;
     EvalArgs a{};
     a.n = t.n;
     a.depth = t.depth;
@@ -509,6 +514,16 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     a.p2p_split = pl.p2p_rows > 0;
     a.out = pl.out.ptr;
     a.out2 = pl.out2.ptr;
+    a.own_leaf = pl.shard_count > 1 ? pl.own_leaf.ptr : nullptr;
+    return a;
+}
+
+void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
+{
+    Tree& t = *pl.tree;
+    cudaStream_t st = t.ctx->stream;
+    SFMM_REQUIRE(pl.shard_count == 1, FMM_ERR_INVALID_ARGUMENT, "a sharded plan evaluates by stages (fmm_evaluate_stage)");
+    EvalArgs a = make_args(pl, pot, field);
     if (a.K == 0) return;
     SFMM_REQUIRE(!(a.want_field && pl.qdim == 2), FMM_ERR_UNSUPPORTED,
                  "the field needs scalar (qdim 1) or vector (qdim 3) charges");
@@ -589,6 +604,135 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     SFMM_CHECK_LAUNCH();
     if (pl.ex_on) apply_exclusions(pl, Q, pot, field);
     SFMM_CUDA(cudaEventRecord(pl.ev[5], st));
+}
+
+// ------------------------------------------------------------------ sharded evaluation
+void plan_set_shard(Plan& pl, int index, int count)
+{
+    SFMM_REQUIRE(count >= 1 && count <= 4096 && index >= 0 && index < count, FMM_ERR_INVALID_ARGUMENT,
+                 "shard index must be in [0, count), 1 <= count <= 4096");
+    Tree& t = *pl.tree;
+    cudaStream_t st = t.ctx->stream;
+    pl.shard_index = index;
+    pl.shard_count = count;
+    pl.own_parent_b.clear();
+    pl.own_parent_e.clear();
+    if (count == 1) {
+        pl.own_leaf.release();
+        return;
+    }
+    // this shard's leaves, level by level, balanced by points (shard_ranges.h)
+    std::vector<int32_t> ln(t.n_leaves), pb(t.n_nodes), pe(t.n_nodes);
+    SFMM_CUDA(cudaMemcpyAsync(ln.data(), t.leaf_node.ptr, ln.size() * 4, cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaMemcpyAsync(pb.data(), t.pbeg.ptr, pb.size() * 4, cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaMemcpyAsync(pe.data(), t.pend.ptr, pe.size() * 4, cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    std::vector<uint8_t> own(std::max<int64_t>(t.n_leaves, 1), 0);
+    for (int l = 0; l <= t.depth; ++l) {
+        const int64_t f0 = t.leaf_off[l], nl = t.leaf_off[l + 1] - f0;
+        std::vector<int64_t> prefix(nl + 1, 0);
+        for (int64_t i = 0; i < nl; ++i) prefix[i + 1] = prefix[i] + (pe[ln[f0 + i]] - pb[ln[f0 + i]]);
+        const auto r = balanced_leaf_range(prefix.data(), nl, count, index);
+        for (int64_t i = r.first; i < r.second; ++i) own[f0 + i] = 1;
+    }
+    pl.own_leaf.alloc(own.size(), st);
+    SFMM_CUDA(cudaMemcpyAsync(pl.own_leaf.ptr, own.data(), own.size(), cudaMemcpyHostToDevice, st));
+    SFMM_CUDA(cudaStreamSynchronize(st));
+    // this shard's parents of M2L targets, level by level (contiguous ranges)
+    for (int q = 0; q <= t.depth; ++q) {
+        const int64_t b = t.lvl_off[q], nq = t.lvl_off[q + 1] - b;
+        pl.own_parent_b.push_back(b + shard_begin(nq, count, index));
+        pl.own_parent_e.push_back(b + shard_end(nq, count, index));
+    }
+}
+
+void plan_evaluate_stage(Plan& pl, const double* Q, double* pot, double* field, int stage)
+{
+    Tree& t = *pl.tree;
+    cudaStream_t st = t.ctx->stream;
+    SFMM_REQUIRE(stage >= 0 && stage <= 2, FMM_ERR_INVALID_ARGUMENT, "stage must be 0, 1 or 2");
+    EvalArgs a = make_args(pl, pot, field);
+    if (a.K == 0) return;
+    SFMM_REQUIRE(!(a.want_field && pl.qdim == 2), FMM_ERR_UNSUPPORTED,
+                 "the field needs scalar (qdim 1) or vector (qdim 3) charges");
+    const int K = a.K, T = pl.T, T1 = pl.T1, qd = pl.qdim;
+    const int sms = t.ctx->sm_count;
+    const bool far = t.depth >= 2;
+    const int64_t nfar = t.n_leaves - a.far_leaf0;
+    cudaStream_t side = t.ctx->side ? t.ctx->side : st;
+    if (stage == 0) {
+        // charges; the near field of this shard's leaves on the side stream
+        // (others' targets stay zero); moments of this shard's leaves
+        k_gather_q<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(Q, t.order.ptr, t.n, qd, pl.qs.ptr, t.pts.ptr,
+                                                                   pl.src4.ptr, pl.src2.ptr);
+        SFMM_CHECK_LAUNCH();
+        SFMM_CUDA(cudaMemsetAsync(pl.out.ptr, 0, size_t(t.n) * K * sizeof(double), st));
+        SFMM_CUDA(cudaMemsetAsync(pl.out2.ptr, 0, size_t(t.n) * K * sizeof(double), st));
+        SFMM_CUDA(cudaEventRecord(pl.fork, st));
+        SFMM_CUDA(cudaStreamWaitEvent(side, pl.fork, 0));
+        launch_p2p(a, sms, side);
+        SFMM_CUDA(cudaEventRecord(pl.join, side));
+        if (far) {
+            const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx);
+            const int w_p2m = warps_for(0, sm_p2m_w);
+            allow_smem(k_p2m, sm_p2m_w * w_p2m);
+            k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
+            SFMM_CHECK_LAUNCH();
+        }
+        return;
+    }
+    if (stage == 1) {
+        // moments summed over the shards by the caller: M2M in full, then
+        // M2L into the children of this shard's parents
+        if (!far) return;
+        const size_t head = (32 + 2 * 4 * (2 * kMaxOrder + 1)) * sizeof(double);
+        const size_t sm_m2m_w = 2 * size_t(qd) * T * sizeof(cplx);
+        const int w_m2m = warps_for(head, sm_m2m_w);
+        allow_smem(k_m2m, head + sm_m2m_w * w_m2m);
+        for (int l = t.depth - 1; l >= 2; --l) {
+            if (pl.shift_on) {
+                shift_m2m(pl, a, l, st);
+                continue;
+            }
+            const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
+            k_m2m<<<blocks_for(c, w_m2m, 65535), w_m2m * 32, head + sm_m2m_w * w_m2m, st>>>(a, l, t.lvl_off[l], c);
+            SFMM_CHECK_LAUNCH();
+        }
+        SFMM_CUDA(cudaMemsetAsync(pl.LA.ptr, 0, pl.LA.bytes(), st));
+        SFMM_CUDA(cudaMemsetAsync(pl.LB.ptr, 0, pl.LB.bytes(), st));
+        for (int q = 1; q < t.depth; ++q) {
+            if (a.m2l_direct) launch_m2l_direct(a, pl.own_parent_b[q], pl.own_parent_e[q], sms, st);
+            else launch_m2l(a, pl.own_parent_b[q], pl.own_parent_e[q], sms, st);
+        }
+        return;
+    }
+    // locals summed over the shards by the caller: L2L in full, L2P of this
+    // shard's leaves, then the sums (zero at other shards' points)
+    if (far) {
+        const size_t head2 = (32 + 2 * 4 * (2 * kMaxOrder + 1) + 2 * 4 * (2 * kMaxOrder + 3)) * sizeof(double);
+        const size_t sm_l2l_w = size_t(qd) * (T + T1) * sizeof(cplx);
+        const int w_l2l = warps_for(head2, sm_l2l_w);
+        allow_smem(k_l2l, head2 + sm_l2l_w * w_l2l);
+        for (int l = 3; l <= t.depth; ++l) {
+            if (pl.shift_on) {
+                shift_l2l(pl, a, l, st);
+                continue;
+            }
+            const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
+            k_l2l<<<blocks_for(c, w_l2l, 65535), w_l2l * 32, head2 + sm_l2l_w * w_l2l, st>>>(a, l, t.lvl_off[l], c);
+            SFMM_CHECK_LAUNCH();
+        }
+        const size_t sm_l2p_w = size_t(K) * T * sizeof(cplx);
+        const int w_l2p = warps_for(0, sm_l2p_w);
+        allow_smem(k_l2p, sm_l2p_w * w_l2p);
+        k_l2p<<<blocks_for(nfar, w_l2p, 65535), w_l2p * 32, sm_l2p_w * w_l2p, st>>>(a);
+        SFMM_CHECK_LAUNCH();
+    }
+    SFMM_CUDA(cudaStreamWaitEvent(st, pl.join, 0));
+    k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
+    SFMM_CHECK_LAUNCH();
+    // excluded interactions are removed once, by shard 0, for every target
+    if (pl.ex_on && pl.shard_index == 0) apply_exclusions(pl, Q, pot, field);
 }
 
 void plan_read_timings(Plan& pl, double* ms6)

@@ -84,6 +84,7 @@ struct EvalArgs {
     int* p2p_ctr;
     int* m2l_ctr;                         // FP64 M2L: the counter blocks take sibling groups from
     int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
+    const uint8_t* own_leaf;              // sharded plan: 1 for this shard's leaves (global leaf id); NULL = all
     // direct M2L (m2l_direct.cu, FMM_M2L_DIRECT): dense coefficient table,
     // Z of the interaction-list angles, phases; row lengths
     int m2l_direct;
@@ -139,6 +140,10 @@ struct Plan {
     DevBuf<int32_t> m2l_ctr;                  // M2L group counter (m2l.cu)
     bool m2l_force_rows = false;              // SFMM_M2L_KERNEL=rows at plan creation
     int m2l_method = FMM_M2L_ROTATION;        // fmm_plan_set_m2l
+    // sharded evaluation (fmm_plan_set_shard): this plan's share of one solve
+    int shard_index = 0, shard_count = 1;
+    DevBuf<uint8_t> own_leaf;                 // per global leaf id
+    std::vector<int64_t> own_parent_b, own_parent_e;   // per parent level q: node range [b, e)
     std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_DIRECT
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
@@ -175,6 +180,13 @@ void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field
 // Selects the M2L formulation (FMM_M2L_ROTATION / FMM_M2L_DIRECT); the
 // direct one's tables are built on first use per (device, p).
 void plan_set_m2l(Plan& pl, int method);
+// Sharded evaluation of one solve (shard_ranges.h): set_shard fixes the
+// plan's share; evaluate_stage runs stage 0 (charges, near field and
+// moments of own leaves), 1 (M2M, M2L into own targets) or 2 (L2L, L2P of
+// own leaves, sums); the caller sums the shards' moments (after stage 0) and
+// locals (after stage 1) across shards, and finally their outputs.
+void plan_set_shard(Plan& pl, int index, int count);
+void plan_evaluate_stage(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev, int stage);
 void plan_read_timings(Plan& pl, double* ms6);
 // Exclusions (exclude.cu): ptr / cols are device arrays (n + 1, ptr[n]).
 void plan_set_exclusions(Plan& pl, const int64_t* ptr, const int32_t* cols, int near_too);

@@ -126,7 +126,7 @@ __global__ void k_p2p_reduce(EvalArgs a)
     const int64_t stride = (int64_t(gridDim.x) * blockDim.x) >> 5;
     for (int64_t f = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; f < a.n_leaves; f += stride) {
         const int np = a.p2p_parts[f];
-        if (np <= 1) continue;
+        if (np <= 1 || (a.own_leaf && !a.own_leaf[f])) continue;
         const int g = a.leaf_node[f];
         const int t0 = a.pbeg[g], nt = a.pend[g] - t0;
         const int64_t rb = a.p2p_rowoff[f];
@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
 
     for (int it = next_item(a.p2p_ctr, lane); it < a.p2p_items; it = next_item(a.p2p_ctr, lane)) {
         const int4 item = a.p2p_item[it];
+        if (a.own_leaf && !a.own_leaf[item.x]) continue;        // another shard's leaf
         const int row = a.p2p_row[it];
         const int g = a.leaf_node[item.x];
         const int t0 = a.pbeg[g], t1 = a.pend[g];
@@ -408,6 +409,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
 
     for (int it = next_item(a.p2p_ctr, lane); it < a.p2p_items; it = next_item(a.p2p_ctr, lane)) {
         const int4 item = a.p2p_item[it];
+        if (a.own_leaf && !a.own_leaf[item.x]) continue;        // another shard's leaf
         const int row = a.p2p_row[it];
         const int g = a.leaf_node[item.x];
         // origin: the leaf's first point (any point near the leaf keeps the
