@@ -58,7 +58,7 @@ enum { FMM_PRECISION_FP64 = 0, FMM_PRECISION_MIXED = 1 };
 /* M2L formulation: rotate / z-translate / rotate back (the reference's
    default M2Lc_rtr, fmm.hpp:620-688), or the dense direct sum the reference
    compiles with -DFMM_M2L_DIRECT (M2Lc_direct, fmm.hpp:592-618). */
-enum { FMM_M2L_ROTATION = 0, FMM_M2L_DIRECT = 1 };
+enum { FMM_M2L_METHOD_ROTATION = 0, FMM_M2L_METHOD_DIRECT = 1 };
 
 /* Tree export selectors for fmm_tree_export (one level at a time). */
 enum {
@@ -150,8 +150,8 @@ int fmm_plan_destroy(fmm_plan* plan);
    (rinv(Q, U)); near_too = 1 removes all of them -- rinv(Q, U, is_self) with
    an is_self true exactly on the listed pairs.  row_ptr = NULL clears. */
 int fmm_plan_set_exclusions(fmm_plan* plan, const int64_t* row_ptr, const int32_t* cols, int where, int near_too);
-/* Chooses the plan's M2L formulation for later evaluations: FMM_M2L_ROTATION
-   (default) or FMM_M2L_DIRECT, the reference's FMM_M2L_DIRECT build option
+/* Chooses the plan's M2L formulation for later evaluations: FMM_M2L_METHOD_ROTATION
+   (default) or FMM_M2L_METHOD_DIRECT, the reference's FMM_M2L_DIRECT build option
    (fmm.hpp:700-712 calling M2Lc_direct, fmm.hpp:592-618; tables
    fmm.hpp:317-337).  The direct form is FP64 only and costs (p+1)^2 terms
    per coefficient and pair; its tables are built on first use per device

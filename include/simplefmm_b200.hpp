@@ -173,7 +173,7 @@ public:
         plan_.reset(pl);
 #ifdef FMM_M2L_DIRECT
         // the reference's build option for the dense M2L (fmm.hpp:700-712)
-        check(fmm_plan_set_m2l(plan_.get(), FMM_M2L_DIRECT));
+        check(fmm_plan_set_m2l(plan_.get(), FMM_M2L_METHOD_DIRECT));
 #endif
     }
 

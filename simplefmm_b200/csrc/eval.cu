@@ -369,9 +369,9 @@ static std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int 
 
 void plan_set_m2l(Plan& pl, int method)
 {
-    SFMM_REQUIRE(method == FMM_M2L_ROTATION || method == FMM_M2L_DIRECT, FMM_ERR_INVALID_ARGUMENT,
-                 "method must be FMM_M2L_ROTATION or FMM_M2L_DIRECT");
-    if (method == FMM_M2L_DIRECT) {
+    SFMM_REQUIRE(method == FMM_M2L_METHOD_ROTATION || method == FMM_M2L_METHOD_DIRECT, FMM_ERR_INVALID_ARGUMENT,
+                 "method must be FMM_M2L_METHOD_ROTATION or FMM_M2L_METHOD_DIRECT");
+    if (method == FMM_M2L_METHOD_DIRECT) {
         SFMM_REQUIRE(pl.precision == FMM_PRECISION_FP64, FMM_ERR_UNSUPPORTED, "the direct M2L is FP64 only");
         SFMM_REQUIRE(pl.T + pl.T1 <= 512, FMM_ERR_UNSUPPORTED, "the direct M2L takes p <= 20");
         if (!pl.dtab) pl.dtab = direct_tables_on_device(pl.tree->ctx->device, pl.p, pl.tree->ctx->stream);
@@ -502,7 +502,7 @@ static EvalArgs make_args(Plan& pl, double* pot, double* field)
     a.p2p_ctr = pl.p2p_ctr.ptr;
     a.m2l_ctr = pl.m2l_ctr.ptr;
     a.m2l_force_rows = pl.m2l_force_rows;
-    a.m2l_direct = pl.m2l_method == FMM_M2L_DIRECT;
+    a.m2l_direct = pl.m2l_method == FMM_M2L_METHOD_DIRECT;
     if (a.m2l_direct) {
         a.dcoef = pl.dtab->coef.ptr;
         a.dncoef = pl.dtab->ncoef;

@@ -85,7 +85,7 @@ struct EvalArgs {
     int* m2l_ctr;                         // FP64 M2L: the counter blocks take sibling groups from
     int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
     const uint8_t* own_leaf;              // sharded plan: 1 for this shard's leaves (global leaf id); NULL = all
-    // direct M2L (m2l_direct.cu, FMM_M2L_DIRECT): dense coefficient table,
+    // direct M2L (m2l_direct.cu, FMM_M2L_METHOD_DIRECT): dense coefficient table,
     // Z of the interaction-list angles, phases; row lengths
     int m2l_direct;
     const double* dcoef;
@@ -139,12 +139,12 @@ struct Plan {
     DevBuf<int32_t> p2p_row, p2p_parts, p2p_rowoff, p2p_ctr;
     DevBuf<int32_t> m2l_ctr;                  // M2L group counter (m2l.cu)
     bool m2l_force_rows = false;              // SFMM_M2L_KERNEL=rows at plan creation
-    int m2l_method = FMM_M2L_ROTATION;        // fmm_plan_set_m2l
+    int m2l_method = FMM_M2L_METHOD_ROTATION;        // fmm_plan_set_m2l
     // sharded evaluation (fmm_plan_set_shard): this plan's share of one solve
     int shard_index = 0, shard_count = 1;
     DevBuf<uint8_t> own_leaf;                 // per global leaf id
     std::vector<int64_t> own_parent_b, own_parent_e;   // per parent level q: node range [b, e)
-    std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_DIRECT
+    std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_METHOD_DIRECT
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
@@ -177,7 +177,7 @@ void p2p_setup(Plan& pl);
 // FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
 void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);
 void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
-// Selects the M2L formulation (FMM_M2L_ROTATION / FMM_M2L_DIRECT); the
+// Selects the M2L formulation (FMM_M2L_METHOD_ROTATION / FMM_M2L_METHOD_DIRECT); the
 // direct one's tables are built on first use per (device, p).
 void plan_set_m2l(Plan& pl, int method);
 // Sharded evaluation of one solve (shard_ranges.h): set_shard fixes the

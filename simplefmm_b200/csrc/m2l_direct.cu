@@ -1,6 +1,6 @@
 // Direct M2L: the reference's compile-time alternative M2Lc_direct
-// (FMM_M2L_DIRECT, fmm.hpp:592-618 with the tables of fmm.hpp:317-337),
-// selected per plan with fmm_plan_set_m2l(plan, FMM_M2L_DIRECT).
+// (its build option FMM_M2L_DIRECT, fmm.hpp:592-618 with the tables of fmm.hpp:317-337),
+// selected per plan with fmm_plan_set_m2l(plan, FMM_M2L_METHOD_DIRECT).
 //
 // For each (target, source, offset d) of the interaction list, every output
 // coefficient is the dense sum over the source's coefficients

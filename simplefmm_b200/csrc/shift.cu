@@ -37,7 +37,7 @@ namespace {
 
 constexpr int kShiftCols = 32;            // M2M columns per block: four 8-column MMA tiles
 constexpr int kL2LTiles = 8;              // L2L: eight 8-column MMA tiles (64 columns) per block
-constexpr int kL2LRowGroups = 4;          // L2L: the 8R output rows split over 4 blocks
+constexpr int kL2LRowGroups = 4;          // L2L: the 8R output rows split over at least 4 blocks
 constexpr int kM2MRowGroups = 2;          // M2M: the R output rows split over 2 blocks
 constexpr int kShiftWarps = 8;
 
@@ -400,7 +400,12 @@ void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st)
     const int64_t ncols = n * qd;
     constexpr int NC = 8 * kL2LTiles;
     const size_t smem = size_t(NC) * shift_ld(4 * cdiv(RB, 4)) * sizeof(double);
-    k_l2l_mma<kL2LTiles><<<dim3(static_cast<unsigned>((ncols + NC - 1) / NC), 2, kL2LRowGroups), 32 * kShiftWarps, smem, st>>>(
+    // small levels (few column tiles) split their rows over more blocks so
+    // the level still spreads over the SMs (each block keeps >= 8 row tiles)
+    const int64_t ctiles = (ncols + NC - 1) / NC;
+    const int rg = static_cast<int>(std::min<int64_t>(std::max<int64_t>(kL2LRowGroups, int64_t(t.ctx->sm_count) / ctiles),
+                                                      std::max(1, RA / kShiftWarps)));
+    k_l2l_mma<kL2LTiles><<<dim3(static_cast<unsigned>(ctiles), 2, static_cast<unsigned>(rg)), 32 * kShiftWarps, smem, st>>>(
         sa, sb, pl.sh_list.ptr, slot0, ncols, qd, t.child_beg.ptr, t.nchild.ptr, t.key.ptr);
     SFMM_CHECK_LAUNCH();
 }

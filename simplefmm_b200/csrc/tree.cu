@@ -751,9 +751,11 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         DevBuf<int32_t> icnt;
         icnt.alloc(total, st);
         SFMM_CUDA(cudaMemsetAsync(icnt.ptr, 0, total * 4, st));
-        for (int l = 2; l <= t.depth; ++l) {
-            const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
-            k_ilist<false><<<blocks_for(c, 128), 128, 0, st>>>(t.lvl_off[l], c, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
+        // every level >= 2 at once: nodes are stored level after level, and a
+        // node's list depends only on its parent's colleagues
+        const int64_t i0 = t.depth >= 2 ? t.lvl_off[2] : total, ic = total - i0;
+        if (ic > 0) {
+            k_ilist<false><<<blocks_for(ic, 128), 128, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
                                                                 t.nchild.ptr, t.colleague.ptr, icnt.ptr, nullptr, nullptr);
             SFMM_CHECK_LAUNCH();
         }
@@ -765,9 +767,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         require_i32_total(t.il_nnz, "the interaction list");
         t.il_src.alloc(std::max<int64_t>(t.il_nnz, 1), st);
         t.il_code.alloc(std::max<int64_t>(t.il_nnz, 1), st);
-        for (int l = 2; l <= t.depth; ++l) {
-            const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
-            k_ilist<true><<<blocks_for(c, 128), 128, 0, st>>>(t.lvl_off[l], c, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
+        if (ic > 0) {
+            k_ilist<true><<<blocks_for(ic, 128), 128, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
                                                                t.nchild.ptr, t.colleague.ptr, t.il_ptr.ptr, t.il_src.ptr,
                                                                t.il_code.ptr);
             SFMM_CHECK_LAUNCH();

@@ -20,8 +20,32 @@ def exe(tmp_path_factory):
     return out
 
 
-def test_facade_compiles(exe):
-    assert exe.exists()
+@pytest.fixture(scope="module")
+def exe_direct(tmp_path_factory):
+    """The same program built with the reference's -DFMM_M2L_DIRECT option."""
+    lib = B.build()
+    out = tmp_path_factory.mktemp("facade_direct") / "facade_main_direct"
+    subprocess.run(["g++", "-std=c++17", "-O2", "-DFMM_M2L_DIRECT", f"-I{ROOT / 'include'}",
+                    str(ROOT / "tests/native/facade_main.cpp"), f"-L{lib.parent}", "-lsimplefmm_b200",
+                    f"-Wl,-rpath,{lib.parent}", "-o", str(out)], check=True)
+    return out
+
+
+def test_facade_compiles(exe, exe_direct):
+    assert exe.exists() and exe_direct.exists()
+
+
+@pytest.mark.gpu
+def test_facade_direct_m2l_option_runs_reference_example(exe, exe_direct):
+    """-DFMM_M2L_DIRECT (the dense M2L) prints the same errors as the default build."""
+    r0 = subprocess.run([str(exe)], capture_output=True, text=True, timeout=600)
+    r1 = subprocess.run([str(exe_direct)], capture_output=True, text=True, timeout=1200)
+    assert r0.returncode == 0 and r1.returncode == 0, r1.stdout + r1.stderr
+    e0 = [float(x.split("=")[1]) for x in r0.stdout.splitlines() if "Relative l2 error" in x]
+    e1 = [float(x.split("=")[1]) for x in r1.stdout.splitlines() if "Relative l2 error" in x]
+    assert len(e0) == 2 and len(e1) == 2
+    for a, b in zip(e0, e1):
+        assert abs(a - b) <= 1e-3 * a
 
 
 @pytest.mark.gpu
