@@ -227,9 +227,9 @@ def run_reference_arm(args):
     first --ref-sample points (and their charges) of the same seeded point
     set, p and leaf size, potential + field, as one shim rank per host core.
     A full solve of the 4M-point workload did not finish in 20 minutes on the
-    GPU box's host cores (1M points take 75 s on 8 cores of a build
-    container), so each step is this bounded sample; one solve is timed per
-    step after the warm-up solves."""
+    16 host cores of a B200 machine (1M points take 24 s there, 75 s on an
+    8-core workstation), so each step is this bounded sample; one solve is
+    timed per step after the warm-up solves."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
@@ -259,7 +259,7 @@ def run_reference_arm(args):
             "same_config": same,
             "sample": (f"the full workload" if same else
                        f"first {n} of the workload's {args.n} points (same seeded set and charges), p={args.p}, "
-                       f"leaf {LEAF}, potential + field; the full solve does not finish within minutes on the host"),
+                       f"leaf {LEAF}, potential + field; the full solve does not finish within minutes on these cores"),
             "reference_phases_s": phases[-1] if phases else None,
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "reference",
                              "sample": f"{n} points, tree + FMM3D set-up + rinv (potential) + FMM3D<3,grad> set-up "

@@ -1,7 +1,7 @@
 // CPU restatement of the reference FMM evaluation path -- TEST ORACLE ONLY.
 //
 // Only the test suite, __graft_entry__.smoke() and bench.py's CPU-baseline leg
-// load this library (through ctypes).  It is the checker, never the product:
+// load this library (through ctypes).  It is a test oracle, never the product:
 // the product path is the CUDA library and fails loudly without it.
 //
 // Written from the reference's algorithm, step by step, with runtime p and
@@ -890,7 +890,7 @@ int oracle_rinv(void* tp, int p, int mode, int ncomp, const double* Q, double* U
     if (p < 0 || p > 30 || (mode == 1 && ncomp != 3) || ncomp < 1) return -1;
     const Tree& T = *static_cast<Tree*>(tp);
     const Tables tb = make_tables(p);
-    Eval ev{T, tb, p, (p + 1) * (p + 1), ncomp, mode == 1, {}, {}, {}, {}, {}};
+    Eval ev{T, tb, p, (p + 1) * (p + 1), ncomp, mode == 1, {}, {}, {}, {}, {}, {}, {}, {}, {}};
     ev.rinv(Q, U);
     return 0;
 }

@@ -1,7 +1,7 @@
 """Test-infrastructure helpers around the compiled reference (``oracle/_ref``).
 
 Only tests, ``__graft_entry__.smoke`` and the CPU-baseline leg of ``bench.py``
-use this module: it is the checker, never the thing measured or shipped.
+use this module: it is a test oracle, never the thing measured or shipped.
 
 ``run_reference`` writes an input file in the format ``ref_driver.cpp``
 documents, runs the reference binary (optionally as several shim ranks, like
