@@ -74,6 +74,10 @@ void release_context(fmm_context* ctx)
         cudaStreamSynchronize(ctx->c.side);
         cudaStreamDestroy(ctx->c.side);
     }
+    if (ctx->c.copy) {
+        cudaStreamSynchronize(ctx->c.copy);
+        cudaStreamDestroy(ctx->c.copy);
+    }
     if (ctx->c.retired) {
         cudaStreamSynchronize(ctx->c.retired);
         cudaStreamDestroy(ctx->c.retired);
@@ -129,11 +133,13 @@ int fmm_context_create(int device, fmm_context** out)
         SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking));
         ctx->c.own_stream = true;
         SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.side, cudaStreamNonBlocking));
+        SFMM_CUDA(cudaStreamCreateWithFlags(&ctx->c.copy, cudaStreamNonBlocking));
         SFMM_CUDA(cudaDeviceGetAttribute(&ctx->c.sm_count, cudaDevAttrMultiProcessorCount, device));
         (void)sfmm::device_pool(device);
     } catch (...) {
         if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
         if (ctx->c.side) cudaStreamDestroy(ctx->c.side);
+        if (ctx->c.copy) cudaStreamDestroy(ctx->c.copy);
         delete ctx;
         throw;
     }
@@ -389,6 +395,8 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
         for (auto& e : pl->pl.ev) SFMM_CUDA(cudaEventCreate(&e));
         SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.fork, cudaEventDisableTiming));
         SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.join, cudaEventDisableTiming));
+        SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.io_start, cudaEventDisableTiming));
+        SFMM_CUDA(cudaEventCreateWithFlags(&pl->pl.io_done, cudaEventDisableTiming));
         sfmm::plan_init(pl->pl);
         SFMM_CUDA(cudaStreamSynchronize(tree->t.ctx->stream));
         sfmm::check_scan_error();
@@ -397,6 +405,8 @@ int fmm_plan_create(fmm_tree* tree, int p, int qdim, int precision, fmm_plan** o
             if (e) cudaEventDestroy(e);
         if (pl->pl.fork) cudaEventDestroy(pl->pl.fork);
         if (pl->pl.join) cudaEventDestroy(pl->pl.join);
+        if (pl->pl.io_start) cudaEventDestroy(pl->pl.io_start);
+        if (pl->pl.io_done) cudaEventDestroy(pl->pl.io_done);
         delete pl;
         release_tree(tree);
         throw;
@@ -415,6 +425,8 @@ int fmm_plan_destroy(fmm_plan* plan)
         if (e) cudaEventDestroy(e);
     if (plan->pl.fork) cudaEventDestroy(plan->pl.fork);
     if (plan->pl.join) cudaEventDestroy(plan->pl.join);
+    if (plan->pl.io_start) cudaEventDestroy(plan->pl.io_start);
+    if (plan->pl.io_done) cudaEventDestroy(plan->pl.io_done);
     if (plan->pl.graph_exec) cudaGraphExecDestroy(plan->pl.graph_exec);
     if (plan->pl.graph) cudaGraphDestroy(plan->pl.graph);
     fmm_tree* owner = plan->owner;
@@ -486,20 +498,31 @@ int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, in
     cudaStream_t st = c.stream;
     const size_t qb = size_t(n) * pl.qdim * sizeof(double);
     if (pl.qin.count < size_t(n) * pl.qdim) pl.qin.alloc(size_t(n) * pl.qdim, st);
-    SFMM_CUDA(cudaMemcpyAsync(pl.qin.ptr, Q, qb, cudaMemcpyHostToDevice, st));
     double* dpot = nullptr;
     double* dfield = nullptr;
-    if (pot) {
-        if (pl.uio_pot.count < size_t(n) * pl.qdim) pl.uio_pot.alloc(size_t(n) * pl.qdim, st);
-        SFMM_CUDA(cudaMemcpyAsync(pl.uio_pot.ptr, pot, qb, cudaMemcpyHostToDevice, st));
-        dpot = pl.uio_pot.ptr;
+    if (pot && pl.uio_pot.count < size_t(n) * pl.qdim) pl.uio_pot.alloc(size_t(n) * pl.qdim, st);
+    if (field && pl.uio_field.count < size_t(n) * 3) pl.uio_field.alloc(size_t(n) * 3, st);
+    SFMM_CUDA(cudaMemcpyAsync(pl.qin.ptr, Q, qb, cudaMemcpyHostToDevice, st));
+    // the accumulated outputs are only needed by the final sums: copy them in
+    // on the context's copy stream while the far field runs (after the
+    // stream's earlier work, which may still read the staging buffers)
+    cudaEvent_t io = nullptr;
+    if (pot || field) {
+        cudaStream_t cp = c.copy ? c.copy : st;
+        SFMM_CUDA(cudaEventRecord(pl.io_start, st));
+        SFMM_CUDA(cudaStreamWaitEvent(cp, pl.io_start, 0));
+        if (pot) {
+            SFMM_CUDA(cudaMemcpyAsync(pl.uio_pot.ptr, pot, qb, cudaMemcpyHostToDevice, cp));
+            dpot = pl.uio_pot.ptr;
+        }
+        if (field) {
+            SFMM_CUDA(cudaMemcpyAsync(pl.uio_field.ptr, field, size_t(n) * 3 * sizeof(double), cudaMemcpyHostToDevice, cp));
+            dfield = pl.uio_field.ptr;
+        }
+        SFMM_CUDA(cudaEventRecord(pl.io_done, cp));
+        io = pl.io_done;
     }
-    if (field) {
-        if (pl.uio_field.count < size_t(n) * 3) pl.uio_field.alloc(size_t(n) * 3, st);
-        SFMM_CUDA(cudaMemcpyAsync(pl.uio_field.ptr, field, size_t(n) * 3 * sizeof(double), cudaMemcpyHostToDevice, st));
-        dfield = pl.uio_field.ptr;
-    }
-    sfmm::plan_evaluate(pl, pl.qin.ptr, dpot, dfield);
+    sfmm::plan_evaluate(pl, pl.qin.ptr, dpot, dfield, io);
     if (pot) SFMM_CUDA(cudaMemcpyAsync(pot, dpot, qb, cudaMemcpyDeviceToHost, st));
     if (field) SFMM_CUDA(cudaMemcpyAsync(field, dfield, size_t(n) * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));

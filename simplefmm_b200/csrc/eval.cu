@@ -518,7 +518,7 @@ static EvalArgs make_args(Plan& pl, double* pot, double* field)
     return a;
 }
 
-void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
+void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field, cudaEvent_t before_sums)
 {
     Tree& t = *pl.tree;
     cudaStream_t st = t.ctx->stream;
@@ -599,6 +599,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field)
     }
     SFMM_CUDA(cudaEventRecord(pl.ev[3], st));
     SFMM_CUDA(cudaStreamWaitEvent(st, pl.join, 0));
+    if (before_sums) SFMM_CUDA(cudaStreamWaitEvent(st, before_sums, 0));
     SFMM_CUDA(cudaEventRecord(pl.ev[4], st));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
     SFMM_CHECK_LAUNCH();

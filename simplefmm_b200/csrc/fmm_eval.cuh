@@ -159,6 +159,7 @@ struct Plan {
     // ev[6] / ev[7] bracket the near field on the side stream
     cudaEvent_t ev[8] = {};
     cudaEvent_t fork = nullptr, join = nullptr;   // side stream: start after the charges, join before the sums
+    cudaEvent_t io_start = nullptr, io_done = nullptr;   // host-array evaluations: output copies on the copy stream
     // one captured evaluation (fmm_plan_capture / fmm_plan_replay)
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
@@ -176,7 +177,10 @@ void p2p_setup(Plan& pl);
 // Fills the fragment-order operators of tb (rfrag / tzfrag / tzl, and the
 // FP32 ones when mixed) from its rotation and translation tables (m2l.cu).
 void build_m2l_fragments(PlanTables& tb, int p, bool mixed, cudaStream_t st);
-void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev);
+// before_sums (may be NULL): an event the stream waits for before the final
+// sums into pot / field (their host-to-device copies on another stream).
+void plan_evaluate(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev,
+                   cudaEvent_t before_sums = nullptr);
 // Selects the M2L formulation (FMM_M2L_METHOD_ROTATION / FMM_M2L_METHOD_DIRECT); the
 // direct one's tables are built on first use per (device, p).
 void plan_set_m2l(Plan& pl, int method);

@@ -173,6 +173,8 @@ struct Context {
     bool own_stream = false;
     cudaStream_t retired = nullptr;       // the context's own stream after the caller set theirs:
                                           // buffers allocated before still free on it
+    cudaStream_t copy = nullptr;          // host-array evaluations copy the accumulated outputs in on it,
+                                          // beside the far field
     cudaStream_t side = nullptr;          // the library's second stream: the near field runs
                                           // on it beside the far field (forked from and joined
                                           // back into `stream` with events)
