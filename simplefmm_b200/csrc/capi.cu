@@ -526,6 +526,7 @@ int fmm_evaluate(fmm_plan* plan, const double* Q, double* pot, double* field, in
     if (pot) SFMM_CUDA(cudaMemcpyAsync(pot, dpot, qb, cudaMemcpyDeviceToHost, st));
     if (field) SFMM_CUDA(cudaMemcpyAsync(field, dfield, size_t(n) * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
+    sfmm::m2l_i8_check(pl);
     API_CATCH
 }
 
@@ -542,6 +543,7 @@ int fmm_plan_timings(const fmm_plan* plan, double* ms6)
     if (!plan || !ms6) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
     bind(*plan->pl.tree->ctx);
     sfmm::plan_read_timings(const_cast<sfmm::Plan&>(plan->pl), ms6);
+    sfmm::m2l_i8_check(const_cast<sfmm::Plan&>(plan->pl));
     API_CATCH
 }
 

@@ -347,7 +347,7 @@ static std::shared_ptr<PlanTables> tables_on_device(int device, int p, bool mixe
     return t;
 }
 
-static std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int p, cudaStream_t st)
+std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int p, cudaStream_t st)
 {
     static std::mutex mu;
     static auto* cache = new std::map<std::pair<int, int>, std::shared_ptr<DirectDevTables>>();   // kept until exit
@@ -408,6 +408,7 @@ void plan_init(Plan& pl)
     // test switch: the row-owner M2L kernel instead of the tensor-core ones
     const char* mk = std::getenv("SFMM_M2L_KERNEL");
     pl.m2l_force_rows = mk && std::strcmp(mk, "rows") == 0;
+    pl.m2l_rotation_only = mk && std::strcmp(mk, "rotation") == 0;
     const int kmax = pl.qdim + 3;
     pl.qs.alloc(size_t(t.n) * pl.qdim, st);
     if (pl.precision == FMM_PRECISION_FP64) {
@@ -416,6 +417,7 @@ void plan_init(Plan& pl)
     }
     pl.out.alloc(size_t(t.n) * kmax, st);
     pl.out2.alloc(size_t(t.n) * kmax, st);
+    m2l_i8_setup(pl);
 }
 
 static EvalArgs make_args(Plan& pl, double* pot, double* field)
@@ -571,6 +573,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field, cudaEv
         }
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
         if (a.m2l_direct) launch_m2l_direct(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
+        else if (pl.i8) launch_m2l_i8(pl, a, st);
         else launch_m2l(a, t.lvl_off[1], t.lvl_off[t.depth], sms, st);
         near_field();
         SFMM_CUDA(cudaEventRecord(pl.ev[2], st));
@@ -616,6 +619,7 @@ void plan_set_shard(Plan& pl, int index, int count)
     cudaStream_t st = t.ctx->stream;
     pl.shard_index = index;
     pl.shard_count = count;
+    if (count > 1) pl.i8.reset();                 // sharded mixed plans take the rotation M2L
     pl.own_parent_b.clear();
     pl.own_parent_e.clear();
     if (count == 1) {

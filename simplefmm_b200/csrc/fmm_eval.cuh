@@ -118,6 +118,20 @@ struct DirectDevTables {
     int ncoef = 0, nz = 0, ne = 0;
 };
 
+// Direct-M2L tables as kernel arguments.
+struct DirectArgs {
+    const double* coef;
+    int ncoef;
+    const double* zil;
+    int nz;
+    const cplx* eil2;
+    int ne;
+};
+
+// Dense int8-slice M2L of mixed plans (m2l_i8.cu): per-plan target blocks,
+// slot tables and moment digits.
+struct I8PlanData;
+
 struct Plan {
     Tree* tree = nullptr;
     int p = 0, T = 0, T1 = 0, qdim = 1, precision = FMM_PRECISION_FP64;
@@ -145,6 +159,8 @@ struct Plan {
     DevBuf<uint8_t> own_leaf;                 // per global leaf id
     std::vector<int64_t> own_parent_b, own_parent_e;   // per parent level q: node range [b, e)
     std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_METHOD_DIRECT
+    std::shared_ptr<I8PlanData> i8;           // mixed plans: the tensor-core (tcgen05, int8 slices) M2L
+    bool m2l_rotation_only = false;           // SFMM_M2L_KERNEL=rotation: mixed plans keep the TF32 rotation M2L
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
     DevBuf<double> qin, uio_pot, uio_field;   // staging for host pointers
@@ -192,6 +208,15 @@ void plan_set_m2l(Plan& pl, int method);
 void plan_set_shard(Plan& pl, int index, int count);
 void plan_evaluate_stage(Plan& pl, const double* Q_dev, double* pot_dev, double* field_dev, int stage);
 void plan_read_timings(Plan& pl, double* ms6);
+// Direct-M2L tables of order p on a device, built on first use and kept (eval.cu).
+std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int p, cudaStream_t st);
+// m2l_i8.cu: whether a plan takes the tensor-core M2L; its set-up at plan
+// creation (fills pl.i8); the launch (moment digits, then the M2L of every
+// level); the report of an expired pipeline wait (throws FMM_ERR_TIMEOUT).
+bool m2l_i8_supported(const Plan& pl);
+void m2l_i8_setup(Plan& pl);
+void launch_m2l_i8(Plan& pl, const EvalArgs& a, cudaStream_t st);
+void m2l_i8_check(Plan& pl);
 // Exclusions (exclude.cu): ptr / cols are device arrays (n + 1, ptr[n]).
 void plan_set_exclusions(Plan& pl, const int64_t* ptr, const int32_t* cols, int near_too);
 void plan_clear_exclusions(Plan& pl);
