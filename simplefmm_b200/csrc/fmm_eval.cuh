@@ -2,6 +2,7 @@
 #pragma once
 
 #include "fmm_internal.cuh"
+#include "i8_ops.h"
 
 #include <memory>
 
@@ -116,16 +117,6 @@ struct PlanTables {
 struct DirectDevTables {
     DevBuf<double> coef, zil, eil2;
     int ncoef = 0, nz = 0, ne = 0;
-};
-
-// Direct-M2L tables as kernel arguments.
-struct DirectArgs {
-    const double* coef;
-    int ncoef;
-    const double* zil;
-    int nz;
-    const cplx* eil2;
-    int ne;
 };
 
 // Dense int8-slice M2L of mixed plans (m2l_i8.cu): per-plan target blocks,

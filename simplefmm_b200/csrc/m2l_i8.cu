@@ -54,6 +54,7 @@
 // its MMAs and copies and frees tensor memory (the host reports
 // FMM_ERR_TIMEOUT).
 #include "eval_util.cuh"
+#include "i8_ops.h"
 
 #include <cstdlib>
 #include <cstring>
@@ -63,7 +64,6 @@
 
 namespace sfmm {
 
-constexpr int kI8MaxOrder = 12;
 constexpr int kI8Slots = 216;
 constexpr int kI8M = 128;                 // operator rows per item (MMA M, tensor-memory lanes)
 constexpr int kI8Stages = 6;
@@ -79,7 +79,6 @@ struct I8Cfg {
     static constexpr int N = ND == 3 ? 160 : 128;
     static constexpr int OpSlab = ND * kI8M * 32;
     static constexpr int MdSlab = ND * N * 32;
-    static constexpr int64_t Q = int64_t(127) << (8 * (ND - 1));
     static constexpr size_t Smem = size_t(kI8Stages) * (OpSlab + MdSlab);
 };
 
@@ -104,84 +103,7 @@ struct I8PlanData {
 
 namespace {
 
-// ------------------------------------------------------------------ real-form layout
-__host__ __device__ inline void real_nm(int r, int& n, int& m, int& im)
-{
-    n = 0;
-    while ((n + 1) * (n + 1) <= r) ++n;
-    const int o = r - n * n;
-    m = (o + 1) / 2;
-    im = (o > 0 && (o & 1) == 0) ? 1 : 0;
-}
-
 __host__ __device__ inline int rdiv_up(int a, int b) { return (a + b - 1) / b; }
-
-// byte offset of element (row, k) of a K-major operand slab with no swizzle:
-// 8-row x 16-byte core matrices, the two K halves 128 B apart, row groups 256 B apart
-__host__ __device__ inline int canon_off(int row, int k) { return (row >> 3) * 256 + (k >> 4) * 128 + (row & 7) * 16 + (k & 15); }
-
-// x in [-1, 1] -> ND balanced signed digits, most significant first:
-// round(x Q) = sum_i d_i 2^(8 (ND-1-i)), |d_0| <= 127, d_i in [-128, 127]
-template<int ND>
-__device__ inline void split_digits(double x, int8_t* d)
-{
-    x = fmin(fmax(x, -1.0), 1.0);
-    int X = __double2int_rn(x * double(I8Cfg<ND>::Q));
-#pragma unroll
-    for (int i = ND - 1; i > 0; --i) {
-        const int di = ((X + 128) & 255) - 128;
-        d[i] = static_cast<int8_t>(di);
-        X = (X - di) >> 8;
-    }
-    d[0] = static_cast<int8_t>(X);
-}
-
-// ------------------------------------------------------------------ operator tables
-// T_d[r][k] for offset index c = (dx+3) + 7 (dy+3) + 49 (dz+3): the terms of
-// the direct M2L (m2l_direct.cu) with rho^-(j+n+1) -> |d|^-(j+n+1).
-__device__ double op_entry(const DirectArgs& t, int p, int RA, int c, int r, int k)
-{
-    const int dx = c % 7 - 3, dy = (c / 7) % 7 - 3, dz = c / 49 - 3;
-    int j, kk, po, n, m, pi;
-    int nmax = p;
-    if (r < RA) {
-        real_nm(r, j, kk, po);
-    } else {
-        real_nm(r - RA, j, kk, po);
-        nmax = p - 1;
-    }
-    if (k >= (p + 1) * (p + 1)) return 0.0;
-    real_nm(k, n, m, pi);
-    if (n > nmax) return 0.0;
-    const int d2 = dx * dx + dy * dy + dz * dz;
-    const double rho = sqrt(double(d2));
-    const int zrow = 16 * abs(dz) + 4 * abs(dy) + abs(dx);
-    const int erow = 7 * (dy + 3) + (dx + 3);
-    const int jn = j + n;
-    const double pw = pow(rho, -double(jn + 1));
-    auto w = [&](int mm) {
-        const int q = mm - kk;
-        double v = t.coef[int64_t(j * (j + 1) / 2 + kk) * t.ncoef + n * (n + 1) + mm] * pw *
-                   t.zil[int64_t(zrow) * t.nz + jn * (jn + 1) / 2 + (q < 0 ? -q : q)];
-        if (dz < 0 && ((jn - q) & 1)) v = -v;
-        const cplx e = t.eil2[int64_t(erow) * t.ne + q + (t.ne >> 1)];
-        return cplx{v * e.re, v * e.im};
-    };
-    cplx cf;
-    if (m == 0) {
-        cf = w(0);
-    } else {
-        const cplx a = w(m), b = w(-m);
-        cf = pi == 0 ? cplx{a.re + b.re, a.im + b.im} : cplx{-(a.im - b.im), a.re - b.re};
-    }
-    return po == 0 ? cf.re : cf.im;
-}
-
-__device__ inline bool offset_valid(int c)
-{
-    const int dx = c % 7 - 3, dy = (c / 7) % 7 - 3, dz = c / 49 - 3;
-    return abs(dx) > 1 || abs(dy) > 1 || abs(dz) > 1;
-}
 
 // beta_r = max over offsets and k of |T_d[r][k]| gamma_k (as float bits, rounded up)
 __global__ void k_i8_beta(DirectArgs t, int p, int RA, int R, int KP, uint32_t* __restrict__ beta_bits)
@@ -194,7 +116,7 @@ __global__ void k_i8_beta(DirectArgs t, int p, int RA, int R, int KP, uint32_t* 
         if (!offset_valid(c)) continue;
         int n, m, pi;
         real_nm(k, n, m, pi);
-        const double v = fabs(op_entry(t, p, RA, c, r, k)) * pow(0.8660254037844386, double(n));
+        const double v = fabs(op_entry(t, p, RA, c, r, k)) * i8_gamma(n);
         mx = fmaxf(mx, __double2float_ru(v));
     }
     for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -218,7 +140,7 @@ __global__ void k_i8_opdigits(DirectArgs t, int p, int RA, int R, int NCH, int K
             const double b = double(__uint_as_float(beta_bits[r]));
             int n, m, pi;
             real_nm(k, n, m, pi);
-            if (b > 0) split_digits<ND>(op_entry(t, p, RA, c, r, k) * pow(0.8660254037844386, double(n)) / b, d);
+            if (b > 0) split_digits<ND>(op_entry(t, p, RA, c, r, k) * i8_gamma(n) / b, d);
         }
         int8_t* slab = op + ((int64_t(c) * NCH + ch) * KS + k / 32) * I8Cfg<ND>::OpSlab;
         for (int i = 0; i < ND; ++i) slab[i * (kI8M * 32) + canon_off(rr, k % 32)] = d[i];
@@ -300,7 +222,7 @@ __global__ void k_i8_alpha(EvalArgs a, uint32_t* __restrict__ alpha_bits)
             int n, m;
             tri_nm(t, n, m);
             const cplx v = a.M[(g * qd + w % qd) * T + t];
-            const double sc = pow(s / 0.8660254037844386, double(n));
+            const double sc = pow(s, double(n)) / i8_gamma(n);
             mx = fmaxf(mx, __double2float_ru(fmax(fabs(v.re), fabs(v.im)) * sc));
         }
         for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
@@ -328,7 +250,7 @@ __global__ void k_i8_mdigits(EvalArgs a, int KS, const uint32_t* __restrict__ al
                 int n, m, im;
                 real_nm(k, n, m, im);
                 const cplx v = a.M[(g * qd + c) * T + n * (n + 1) / 2 + m];
-                split_digits<ND>((im ? v.im : v.re) * pow(s / 0.8660254037844386, double(n)) / al, d);
+                split_digits<ND>((im ? v.im : v.re) * pow(s, double(n)) / i8_gamma(n) / al, d);
             }
             int8_t* o = dst + (k / 32) * (32 * ND) + (k % 32);
 #pragma unroll

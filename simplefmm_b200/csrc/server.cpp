@@ -43,6 +43,7 @@
 #include <vector>
 
 #include "alloc_meter.h"
+#include "i8_ops.h"
 #include "simplefmm_b200.h"
 
 namespace sfmm {
@@ -76,12 +77,16 @@ constexpr int kLeafCandidates[] = {32, 64, 128};
 // (expansions of order p for qdim components, outputs).  Nodes per point and
 // interaction-list entries per node are taken at their high end (Plummer-like
 // clustering) so the budget is not overrun.
-size_t estimate_bytes(int64_t n, int p, int qdim, int leaf)
+size_t estimate_bytes(int64_t n, int p, int qdim, int leaf, int precision)
 {
     const double T = (p + 1) * (p + 2) / 2.0, T1 = (p + 2) * (p + 3) / 2.0;
     const double nodes = std::max<double>(64.0, 2.5 * double(n) / std::max(leaf, 8));
     const double per_point = 48 + 48 + 48 + 8.0 * (qdim + 3) * 3;     // points (two frames), sort scratch, I/O
-    const double per_node = 16.0 * qdim * (2 * T + T1) + 190 * 8 + 64;   // M, LA, LB, ilist, node arrays
+    double per_node = 16.0 * qdim * (2 * T + T1) + 190 * 8 + 64;         // M, LA, LB, ilist, node arrays
+    // mixed plans' tensor-core M2L (m2l_i8.cu): slot table, block lists and
+    // four digits of the padded real moments per node
+    if (precision == FMM_PRECISION_MIXED && p <= sfmm::kI8MaxOrder)
+        per_node += 216 * 4 + 16 + 4.0 * 32 * ((p + 1) * (p + 1) / 32 + 1) * qdim;
     return static_cast<size_t>(per_point * double(n) + per_node * nodes + (64 << 20));
 }
 
@@ -260,7 +265,7 @@ int fmm_server_submit(fmm_server* s, const double* xyz, int64_t n, const double*
     // the budget check takes the smallest candidate leaf (the largest
     // estimate) for an autotuned request, before it takes a trial
     r->leaf = r->tuned ? kLeafCandidates[0] : max_particles_per_node;
-    r->bytes = estimate_bytes(n, p, qdim, r->leaf);
+    r->bytes = estimate_bytes(n, p, qdim, r->leaf, r->precision);
     if (r->bytes > s->budget)
         return sfmm::record_failure(FMM_ERR_OVER_BUDGET, "request's estimated device memory exceeds the server budget");
     if (r->tuned) r->leaf = s->tuner.choose(*r);
