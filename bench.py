@@ -170,6 +170,34 @@ def fp64_peak_tflops(torch) -> float:
     return best
 
 
+def int8_peak_tops(torch) -> float:
+    """Measured int8 dense GEMM rate (cuBLASLt through torch._int_mm, int32
+    accumulation), best of 3."""
+    n = 8192
+    a = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+    b = torch.randint(-128, 127, (n, n), dtype=torch.int8, device="cuda")
+    torch._int_mm(a, b)
+    best = 0.0
+    for _ in range(3):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch._int_mm(a, b)
+        e.record()
+        e.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def m2l_i8_ops(p: int) -> int:
+    """int8 tensor-core operations of the mixed plans' M2L (k_m2l_i8) per
+    ilist pair and charge component, on the nonzero entries of its dense
+    operator: potential-local rows (p+1)^2 x (p+1)^2 moments, field-local
+    rows (p+2)^2 x p^2, each a product of four-digit numbers taken as ten
+    8-bit digit products (2 ops per multiply-add)."""
+    return 2 * 10 * ((p + 1) ** 4 + (p + 2) ** 2 * p ** 2)
+
+
 DATA_DESC = {
     "plummer": "synthetic (seeded Plummer sphere, a=1, r<=10; charges U[-1,1])",
     "uniform": "synthetic (seeded uniform unit cube; charges U[-1,1])",
@@ -178,20 +206,20 @@ DATA_DESC = {
 }
 
 
-def reference_solve(pos, q, p: int, cores: int):
+def reference_solve(pos, q, p: int, cores: int, leaf: int = LEAF):
     """One solve of the reference's own CPU implementation (the compiled,
     unmodified reference headers: tree + FMM3D set-up + rinv for the
     potential, FMM3D<3, grad> set-up + two rinv<true> runs for the field),
     as `cores` shim ranks (mpirun -n cores).  Returns (seconds, phases)."""
     from oracle import refio
 
-    out = refio.run_reference(pos, q, p=p, max_level=20, max_ppn=LEAF,
+    out = refio.run_reference(pos, q, p=p, max_level=20, max_ppn=leaf,
                               flags=refio.FLAG_POT | refio.FLAG_FIELD, ranks=cores, timeout=1800)
     ph = {k: out[k] for k in ("T_TREE", "T_CTOR1", "T_POT", "T_CTOR3G", "T_FIELD")}
     return sum(ph.values()), ph
 
 
-def cpu_baseline(dist: str, n_total: int, n_sample: int, p: int, steps: int = 1):
+def cpu_baseline(dist: str, n_total: int, n_sample: int, p: int, steps: int = 1, leaf: int = LEAF):
     """The reference's CPU implementation on a bounded sample of the workload
     (the first n_sample of its n_total seeded points and their charges), one
     shim rank per host core; the oracle's restatement on 1 core if the
@@ -207,19 +235,41 @@ def cpu_baseline(dist: str, n_total: int, n_sample: int, p: int, steps: int = 1)
     vals = []
     if refio.have_reference():
         for _ in range(steps):
-            t, _ = reference_solve(pos, q, p, cores)
+            t, _ = reference_solve(pos, q, p, cores, leaf)
             vals.append(n_sample / t)
     else:
         from oracle import pyoracle
         kind, cores = "port", 1
         for _ in range(steps):
             t0 = time.perf_counter()
-            tr = pyoracle.Tree(pos, 20, LEAF)
+            tr = pyoracle.Tree(pos, 20, leaf)
             tr.potential_field(p, q)
             vals.append(n_sample / (time.perf_counter() - t0))
     return vals, {"unit": "points/s", "cores": cores, "kind": kind,
-                  "sample": f"first {n_sample} of the workload's {n_total} {dist} points, p={p}, leaf {LEAF}, potential + field "
+                  "sample": f"first {n_sample} of the workload's {n_total} {dist} points, p={p}, leaf {leaf}, potential + field "
                             f"(tree + FMM3D set-up + rinv, field via two rinv<true> runs)"}
+
+
+def roofline_i8(torch, pairs: int, p: int, m2l_ms: float, m2l_bytes: int) -> dict:
+    """Roofline of the mixed plans' dominant kernel, the int8-slice M2L on
+    the tensor cores, against the measured int8 GEMM rate."""
+    ops = pairs * m2l_i8_ops(p)
+    achieved = ops / (m2l_ms * 1e-3) / 1e12
+    peak = int8_peak_tops(torch)
+    rows, k = (p + 1) ** 2 + (p + 2) ** 2, (p + 1) ** 2
+    # what the instruction shape allows: N = 128 of the 256 an MMA costs the
+    # same for (four int32 accumulators fill tensor memory), rows padded to
+    # 128, K to 32
+    shape = 0.5 * rows / (128 * -(-rows // 128)) * k / (32 * -(-k // 32))
+    return {"bound": "tensor", "pipe": "int8 tensor cores (tcgen05.mma kind::i8, M=128 N=128 K=32)", "kernel": "k_m2l_i8",
+            "achieved": achieved, "peak": peak, "unit": "TOPS", "frac": achieved / peak,
+            "peak_source": "int8 GEMM (torch._int_mm 8192^3, cuBLASLt) measured in this run; MEASURED_PEAKS.json "
+                           "has no int8 figure",
+            "work": f"ilist pairs x {m2l_i8_ops(p)} int8 ops per pair (nonzero dense-operator entries x 10 digit "
+                    f"products x 2), per launch {ops:.4g}; time = mean CUDA-event M2L phase (moment digits included)",
+            "frac_of_shape_bound": achieved / peak / shape, "shape_bound": shape,
+            "traffic": None, "traffic_model_bytes": m2l_bytes,
+            "traffic_note": "measured DRAM bytes per launch come from an ncu capture (profiles/), not from this run"}
 
 
 def run_reference_arm(args):
@@ -246,7 +296,7 @@ def run_reference_arm(args):
     q = W.charges(args.n, SEED)[:n]
     vals, phases = [], []
     for i in range(args.warmup + args.steps):
-        t, ph = reference_solve(pos, q, args.p, cores)
+        t, ph = reference_solve(pos, q, args.p, cores, args.leaf)
         if i >= args.warmup:
             vals.append(n / t)
             phases.append(ph)
@@ -259,7 +309,7 @@ def run_reference_arm(args):
             "same_config": same,
             "sample": (f"the full workload" if same else
                        f"first {n} of the workload's {args.n} points (same seeded set and charges), p={args.p}, "
-                       f"leaf {LEAF}, potential + field; the full solve does not finish within minutes on these cores"),
+                       f"leaf {args.leaf}, potential + field; the full solve does not finish within minutes on these cores"),
             "reference_phases_s": phases[-1] if phases else None,
             "cpu_baseline": {"value": v, "unit": "points/s", "cores": cores, "kind": "reference",
                              "sample": f"{n} points, tree + FMM3D set-up + rinv (potential) + FMM3D<3,grad> set-up "
@@ -270,8 +320,9 @@ def run_reference_arm(args):
 
 def workload_config(args, n: int, world: int) -> dict:
     par = f"shard x{world} (one solve, NCCL all-reduce)" if getattr(args, "shard", False) and world > 1 else f"replicas x{world}"
-    return {"workload": f"{args.dist}_n{n}_p{args.p}_leaf{LEAF}_{args.precision}_potential+field", "n": n,
-            "p": args.p, "leaf": LEAF, "distribution": args.dist, "precision": args.precision,
+    leaf = getattr(args, "leaf", LEAF)
+    return {"workload": f"{args.dist}_n{n}_p{args.p}_leaf{leaf}_{args.precision}_potential+field", "n": n,
+            "p": args.p, "leaf": leaf, "distribution": args.dist, "precision": args.precision,
             "parallelism": par, "l2": "flushed (256 MiB write) between timed steps"}
 
 
@@ -372,6 +423,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_DEFAULT)
     ap.add_argument("--p", type=int, default=P_DEFAULT)
+    ap.add_argument("--leaf", type=int, default=LEAF, help="max points per leaf (max_particles_per_node)")
     ap.add_argument("--dist", default="plummer")
     ap.add_argument("--ref-sample", type=int, default=1_000_000,
                     help="reference arm: the first this many points of the workload (0 = all of it)")
@@ -431,7 +483,7 @@ def main():
             live.pop().close()
         pot_d.zero_()
         fld_d.zero_()
-        tree = sf.Tree(pos_d, 20, LEAF, ctx=ctx)
+        tree = sf.Tree(pos_d, 20, args.leaf, ctx=ctx)
         plan = sf.Plan(tree, p, 1, precision=args.precision)
         if sharded:
             plan.set_shard(rank, world)
@@ -487,6 +539,7 @@ def main():
     useful = pairs * m2l_useful_flops(p)                # per launch
     achieved = useful / (m2l_avg * 1e-3) / 1e12
     peak = fp64_peak_tflops(torch)
+    tensor_i8 = args.precision == "mixed" and 2 <= p <= 12
     peaks, peaks_src = measured_peaks()
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     T, T1 = (p + 1) * (p + 2) // 2, (p + 2) * (p + 3) // 2
@@ -512,14 +565,14 @@ def main():
 
         def e2e_step():
             if not sharded:
-                tr = sf.Tree(pos_p, 20, LEAF, ctx=ctx2)
+                tr = sf.Tree(pos_p, 20, args.leaf, ctx=ctx2)
                 sf.Plan(tr, p, 1, precision=args.precision).evaluate(q_p, pot_p, fld_p)
                 return tr
             pos_x = torch.from_numpy(pos_p).cuda(non_blocking=True)
             q_x = torch.from_numpy(q_p).cuda(non_blocking=True)
             pot_x = torch.from_numpy(pot_p).cuda(non_blocking=True)
             fld_x = torch.from_numpy(fld_p).cuda(non_blocking=True)
-            tr = sf.Tree(pos_x, 20, LEAF, ctx=ctx2)
+            tr = sf.Tree(pos_x, 20, args.leaf, ctx=ctx2)
             pl = sf.Plan(tr, p, 1, precision=args.precision).set_shard(rank, world)
             pot_0, fld_0 = pot_x.clone(), fld_x.clone()
             pl.evaluate_sharded(q_x, pot_x, fld_x, allreduce=dist.all_reduce)
@@ -556,7 +609,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        vals, info = cpu_baseline(args.dist, n, args.cpu_sample, p)
+        vals, info = cpu_baseline(args.dist, n, args.cpu_sample, p, leaf=args.leaf)
         cpu = dict(info, value=statistics.median(vals))
 
     if rank == 0:
@@ -564,7 +617,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "strong" if sharded else "weak", "vs_baseline": None,
-            "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
+            "dtype": "f64" if args.precision == "fp64" else (
+                "f32 near field; M2L in int8 slices on the tensor cores (32-bit fixed point, exact int32 sums); "
+                "f64 moments, locals and sums"),
             "data": DATA_DESC.get(args.dist, f"synthetic (seeded {args.dist})"),
             "config": workload_config(args, n, world),
             "tree": {"depth": tree.depth, **stats},
@@ -574,7 +629,8 @@ def main():
             "tree_ms_per_step": [round(ph["tree_ms"], 3) for ph in phases],
             "tree_build_phases": dict(build, peak_hbm_gbs=hbm, peak_source=peaks_src,
                                       work="algorithmic bytes of each phase (fmm_tree_build_phases) / its device time"),
-            "roofline": {"bound": "tensor", "pipe": "FP64 tensor cores (DMMA 8x8x4)", "kernel": "k_m2l_mma",
+            "roofline": roofline_i8(torch, pairs, p, m2l_avg, m2l_bytes) if tensor_i8 else {
+                         "bound": "tensor", "pipe": "FP64 tensor cores (DMMA 8x8x4)", "kernel": "k_m2l_mma",
                          "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
                          "peak_source": "FP64 DGEMM (torch float64 matmul 8192^3, cuBLAS DMMA) measured in this run; "
                                         "MEASURED_PEAKS.json has no FP64 figure",

@@ -373,12 +373,6 @@ __device__ __forceinline__ void two_sum_add(Sum2& a, float x)
     a.s = s;
 }
 
-template<int QD>
-struct P2PSmemF {
-    static constexpr int per_warp = kChunk * (32 + (QD > 1 ? 8 : 0) + 4);
-    static constexpr int total = kWarps * per_warp;
-};
-
 // x = hi + lo with hi = float(x): differences of nearby points keep FP32
 // relative precision in the separation itself (the hi parts subtract exactly)
 struct F2 {
@@ -391,6 +385,71 @@ __device__ __forceinline__ F2 split_f(double x)
     return F2{h, static_cast<float>(x - static_cast<double>(h))};
 }
 
+template<int QD>
+struct P2PSmemF {
+    static constexpr int per_warp = kChunk * (32 + (QD > 1 ? 8 : 0));
+    static constexpr int total = kWarps * per_warp;
+};
+
+// 1/sqrt(r2): the hardware approximation (rsqrt.approx.ftz, relative error
+// ~2^-22.9; a denormal r2 -- separations below 1e-19 of the leaf's scale --
+// counts as 0) and one Newton-Raphson step.  r2 = 0 gives +inf, as 1/0 does
+// in FP64: the step runs on min(y, 2^126) so that 0 x inf never forms.
+__device__ __forceinline__ float rsqrt_newton(float r2)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(r2));
+    const float yc = fminf(y, 8.507059e37f);
+    const float e = fmaf(-0.5f * r2 * yc, yc, 0.5f);
+    return fmaf(y, e, y);
+}
+
+// One staged tile against NP target passes of the lane: plain FP32 partial
+// sums (the caller folds them into two-sums after the tile).  ks[p] is the
+// tile slot of pass p's own target (-1 if it is not in this tile).
+template<int NP, int QD, bool POT, bool FLD, int NO, int MP>
+__device__ __forceinline__ void p2p_mixed_tile(const float4* __restrict__ sxq, const float4* __restrict__ sxl,
+                                               const float2* __restrict__ sq12, int s, int slices, int fill,
+                                               const F2 (&xi)[MP], const F2 (&yi)[MP], const F2 (&zi)[MP],
+                                               const int (&ks)[MP], float (&part)[MP][NO > 0 ? NO : 1])
+{
+    for (int k = s; k < fill; k += slices) {
+        const float4 xq = sxq[k], xl = sxl[k];
+        float2 qq = make_float2(0.f, 0.f);
+        if (QD > 1) qq = sq12[k];
+#pragma unroll
+        for (int p = 0; p < NP; ++p) {
+            const float dx = (xi[p].h - xq.x) + (xi[p].l - xl.x);
+            const float dy = (yi[p].h - xq.y) + (yi[p].l - xl.y);
+            const float dz = (zi[p].h - xq.z) + (zi[p].l - xl.z);
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float ir = k == ks[p] ? 0.f : rsqrt_newton(r2);
+            int o = 0;
+            if (POT) {
+                part[p][o] = fmaf(xq.w, ir, part[p][o]);
+                ++o;
+                if (QD > 1) { part[p][o] = fmaf(qq.x, ir, part[p][o]); ++o; }
+                if (QD > 2) { part[p][o] = fmaf(qq.y, ir, part[p][o]); ++o; }
+            }
+            if (FLD) {
+                const float ir3 = ir * ir * ir;
+                if (QD == 1) {
+                    const float cq = xq.w * ir3;
+                    part[p][o] = fmaf(cq, dx, part[p][o]);
+                    part[p][o + 1] = fmaf(cq, dy, part[p][o + 1]);
+                    part[p][o + 2] = fmaf(cq, dz, part[p][o + 2]);
+                } else {
+                    const float qa = xq.w, qb = qq.x, qc = qq.y;
+                    part[p][o] = fmaf(qb * dz - qc * dy, ir3, part[p][o]);
+                    part[p][o + 1] = fmaf(qc * dx - qa * dz, ir3, part[p][o + 1]);
+                    part[p][o + 2] = fmaf(qa * dy - qb * dx, ir3, part[p][o + 2]);
+                }
+            }
+        }
+    }
+}
+
+
 template<int QD, bool POT, bool FLD, int kMaxPass, int MINB>
 __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
 {
@@ -402,7 +461,6 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
     float4* sxq = reinterpret_cast<float4*>(mine);                 // x y z q0, high parts (leaf-centred)
     float4* sxl = sxq + kChunk;                                     // x y z low parts
     float2* sq12 = reinterpret_cast<float2*>(mine + kChunk * 32);   // only for QD > 1
-    int* sj = reinterpret_cast<int*>(mine + kChunk * (32 + (QD > 1 ? 8 : 0)));
     const double* q0 = a.qs;
     const double* q1 = a.qs + (QD > 1 ? a.n : 0);
     const double* q2 = a.qs + (QD > 2 ? 2 * a.n : 0);
@@ -443,16 +501,22 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
             int ri = item.y, roff = item.z, rem = item.w;
             while (rem > 0 && ri < r1) {
                 int fill = 0;
+                int self_s0 = 0, self_j0 = 0, self_len = 0;   // the tile's segment of the target leaf's own points
                 while (rem > 0 && ri < r1 && fill < kChunk) {
                     const int2 rg = a.nr[ri];
                     const int len = min(min(rg.y - rg.x - roff, kChunk - fill), rem);
+                    const int j0 = rg.x + roff;
                     for (int k = lane; k < len; k += 32) {
-                        const int j = rg.x + roff + k;
+                        const int j = j0 + k;
                         const F2 x = split_f(a.px[j] - c[0]), y = split_f(a.py[j] - c[1]), z = split_f(a.pz[j] - c[2]);
                         sxq[fill + k] = make_float4(x.h, y.h, z.h, static_cast<float>(q0[j]));
                         sxl[fill + k] = make_float4(x.l, y.l, z.l, 0.f);
                         if (QD > 1) sq12[fill + k] = make_float2(static_cast<float>(q1[j]), static_cast<float>(q2[j]));
-                        sj[fill + k] = j;
+                    }
+                    if (j0 < t1 && j0 + len > t0) {
+                        self_s0 = fill;
+                        self_j0 = j0;
+                        self_len = len;
                     }
                     fill += len;
                     roff += len;
@@ -467,44 +531,19 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p_mixed(EvalArgs a)
                 for (int p = 0; p < kMaxPass; ++p)
 #pragma unroll
                     for (int o = 0; o < NO; ++o) part[p][o] = 0.f;
-                for (int k = s; k < fill; k += slices) {
-                    const float4 xq = sxq[k], xl = sxl[k];
-                    float2 qq = make_float2(0.f, 0.f);
-                    if (QD > 1) qq = sq12[k];
-                    const int j = sj[k];
+                int ks[kMaxPass];
 #pragma unroll
-                    for (int p = 0; p < kMaxPass; ++p) {
-                        if (p >= passes) break;
-                        const float dx = (xi[p].h - xq.x) + (xi[p].l - xl.x);
-                        const float dy = (yi[p].h - xq.y) + (yi[p].l - xl.y);
-                        const float dz = (zi[p].h - xq.z) + (zi[p].l - xl.z);
-                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        float ir = rsqrtf(r2);
-                        ir = ir * fmaf(-0.5f * r2 * ir, ir, 1.5f);      // one Newton step
-                        ir = j == ii[p] ? 0.f : (r2 > 0.f ? ir : __int_as_float(0x7f800000));
-                        int o = 0;
-                        if (POT) {
-                            part[p][o] = fmaf(xq.w, ir, part[p][o]);
-                            ++o;
-                            if (QD > 1) { part[p][o] = fmaf(qq.x, ir, part[p][o]); ++o; }
-                            if (QD > 2) { part[p][o] = fmaf(qq.y, ir, part[p][o]); ++o; }
-                        }
-                        if (FLD) {
-                            const float ir3 = ir * ir * ir;
-                            if (QD == 1) {
-                                const float cq = xq.w * ir3;
-                                part[p][o] = fmaf(cq, dx, part[p][o]);
-                                part[p][o + 1] = fmaf(cq, dy, part[p][o + 1]);
-                                part[p][o + 2] = fmaf(cq, dz, part[p][o + 2]);
-                            } else {
-                                const float qa = xq.w, qb = qq.x, qc = qq.y;
-                                part[p][o] = fmaf(qb * dz - qc * dy, ir3, part[p][o]);
-                                part[p][o + 1] = fmaf(qc * dx - qa * dz, ir3, part[p][o + 1]);
-                                part[p][o + 2] = fmaf(qa * dy - qb * dx, ir3, part[p][o + 2]);
-                            }
-                        }
-                    }
+                for (int p = 0; p < kMaxPass; ++p) {
+                    const unsigned d = static_cast<unsigned>(ii[p] - self_j0);
+                    ks[p] = ii[p] >= 0 && d < static_cast<unsigned>(self_len) ? self_s0 + static_cast<int>(d) : -1;
                 }
+                static_assert(kMaxPass <= 3, "passes dispatched up to 3");
+                if (passes == 1)
+                    p2p_mixed_tile<1, QD, POT, FLD, NO>(sxq, sxl, sq12, s, slices, fill, xi, yi, zi, ks, part);
+                else if (passes == 2)
+                    p2p_mixed_tile<(kMaxPass >= 2 ? 2 : 1), QD, POT, FLD, NO>(sxq, sxl, sq12, s, slices, fill, xi, yi, zi, ks, part);
+                else
+                    p2p_mixed_tile<kMaxPass, QD, POT, FLD, NO>(sxq, sxl, sq12, s, slices, fill, xi, yi, zi, ks, part);
                 // fold the chunk's partials (at most kChunk / slices terms each) into the two-sums
 #pragma unroll
                 for (int p = 0; p < kMaxPass; ++p)
