@@ -52,7 +52,12 @@ typedef enum fmm_status {
 enum { FMM_HOST = 0, FMM_DEVICE = 1 };
 
 /* Plan precision: FP64 throughout (matches the reference to 1e-12), or the
-   mixed-precision form. */
+   mixed-precision form: near field in FP32 with compensated sums; M2L (orders
+   2..12) as dense per-offset operators in four 8-bit slices on the int8
+   tensor cores with exact int32 sums (about 1e-7 relative to the FP64 path);
+   moments, locals and the final sums in FP64.  A pipeline wait of that M2L
+   that expires is reported as FMM_ERR_TIMEOUT by the next host-array
+   fmm_evaluate or fmm_plan_timings of the plan. */
 enum { FMM_PRECISION_FP64 = 0, FMM_PRECISION_MIXED = 1 };
 
 /* M2L formulation: rotate / z-translate / rotate back (the reference's

@@ -35,7 +35,8 @@
 // parent's 27 neighbours that are not adjacent; partition.hpp:283-297),
 // 216 slots in a 6 x 6 x 6 box.  A row block is up to 128 target rows
 // (target x charge component) of one group; its slot table lists each
-// target's source per slot.  A work item is a row block and 128 operator rows;
+// target's source per slot.  The blocks of a level are numbered with the 8
+// octants of a region adjacent, so blocks that run together share sources.  A work item is a row block and 128 operator rows;
 // it runs over the slots that occur in the block and over K in steps of 32
 // bytes.  Per step, the operator slab (128 rows x 32 B x 4 digits, stored in
 // the MMA's canonical layout: one bulk copy) and the 128 sources' moment
@@ -56,6 +57,8 @@
 #include "eval_util.cuh"
 #include "i8_ops.h"
 
+#include <cub/device/device_radix_sort.cuh>
+
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -67,7 +70,7 @@ namespace sfmm {
 constexpr int kI8Slots = 216;
 constexpr int kI8M = 128;                 // operator rows per item (MMA M, tensor-memory lanes)
 constexpr int kI8Stages = 6;
-constexpr int kI8Lag = 2;                 // gather stages in flight per producer thread
+constexpr int kI8Lag = 4;                 // gather stages in flight per producer thread
 constexpr int kI8Threads = 9 * 32;
 constexpr long kI8Spin = 1L << 22;        // mbarrier polls before a wait gives up
 
@@ -149,17 +152,39 @@ __global__ void k_i8_opdigits(DirectArgs t, int p, int RA, int R, int NCH, int K
 }
 
 // ------------------------------------------------------------------ per-plan set-up
-// Octant groups: position of each target in its (level, octant) group.
-__global__ void k_i8_count(const uint64_t* __restrict__ key, int64_t g0, int64_t g1, const int64_t* __restrict__ lvl_off, int depth,
-                           int32_t* __restrict__ cnt, int32_t* __restrict__ pos)
+// Sort key of each target: its (level, octant) group, then the pattern of its
+// parent's 27 neighbours that have children (which of the 189 slots can hold
+// a source).  Blocks of targets with one pattern use the same slots: near the
+// edge of a level's refined region, where interaction lists are partly empty,
+// Morton order alone would give each block the union of many patterns.
+__global__ void k_i8_keys(const uint64_t* __restrict__ key, int64_t g0, int64_t g1, const int64_t* __restrict__ lvl_off, int depth,
+                          const int32_t* __restrict__ parent, const int32_t* __restrict__ col, const int32_t* __restrict__ nchild,
+                          uint64_t* __restrict__ skey, int32_t* __restrict__ sval, int32_t* __restrict__ cnt)
 {
     for (int64_t g = g0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < g1; g += int64_t(gridDim.x) * blockDim.x) {
         int l = 2;
         while (l < depth && g >= lvl_off[l + 1]) ++l;
         const uint64_t k = key[g];
         const int oct = int(compact3(k) & 1) | int(compact3(k >> 1) & 1) << 1 | int(compact3(k >> 2) & 1) << 2;
-        pos[g - g0] = atomicAdd(cnt + (l - 2) * 8 + oct, 1);
+        const int grp = (l - 2) * 8 + oct;
+        const int32_t* pc = col + 27 * int64_t(parent[g]);
+        uint32_t mask = 0;
+        for (int s = 0; s < 27; ++s) {
+            const int P = pc[s];
+            if (P >= 0 && nchild[P] > 0) mask |= 1u << s;
+        }
+        skey[g - g0] = uint64_t(grp) << 27 | mask;
+        sval[g - g0] = static_cast<int32_t>(g);
+        atomicAdd(cnt + grp, 1);
     }
+}
+
+// Position of each target in its group from the sorted order.
+__global__ void k_i8_pos(int64_t n, int64_t g0, const uint64_t* __restrict__ skey, const int32_t* __restrict__ sval,
+                         const int32_t* __restrict__ grp_start, int32_t* __restrict__ pos)
+{
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x)
+        pos[sval[i] - g0] = static_cast<int32_t>(i - grp_start[skey[i] >> 27]);
 }
 
 __global__ void k_i8_assign(const uint64_t* __restrict__ key, int64_t g0, int64_t g1, const int64_t* __restrict__ lvl_off, int depth,
@@ -174,7 +199,7 @@ __global__ void k_i8_assign(const uint64_t* __restrict__ key, int64_t g0, int64_
         const int cx = compact3(k) & 1, cy = compact3(k >> 1) & 1, cz = compact3(k >> 2) & 1;
         const int oct = cx | cy << 1 | cz << 2;
         const int ps = pos[g - g0];
-        const int64_t rb = rb_off[(l - 2) * 8 + oct] + ps / tpb;
+        const int64_t rb = rb_off[(l - 2) * 8 + oct] + int64_t(ps / tpb) * 8;
         const int t = ps % tpb;
         rb_tgt[rb * tpb + t] = static_cast<int32_t>(g);
         atomicMax(rb_info + rb, l | oct << 8 | (t + 1) << 12);
@@ -637,21 +662,52 @@ void m2l_i8_setup(Plan& pl)
     DevBuf<int64_t> loff;
     loff.alloc(t.depth + 2, st);
     SFMM_CUDA(cudaMemcpyAsync(loff.ptr, t.lvl_off.data(), (t.depth + 2) * sizeof(int64_t), cudaMemcpyHostToDevice, st));
-    DevBuf<int32_t> cnt, pos, rb_off;
+    const int64_t nt = g1 - g0;
+    DevBuf<int32_t> cnt, pos, rb_off, gstart, v0, v1;
+    DevBuf<uint64_t> k0, k1;
     cnt.alloc(ngrp, st);
-    pos.alloc(std::max<int64_t>(g1 - g0, 1), st);
+    pos.alloc(std::max<int64_t>(nt, 1), st);
+    k0.alloc(std::max<int64_t>(nt, 1), st);
+    k1.alloc(std::max<int64_t>(nt, 1), st);
+    v0.alloc(std::max<int64_t>(nt, 1), st);
+    v1.alloc(std::max<int64_t>(nt, 1), st);
     SFMM_CUDA(cudaMemsetAsync(cnt.ptr, 0, cnt.bytes(), st));
     const int sms = t.ctx->sm_count;
-    const unsigned grid = static_cast<unsigned>(std::min<int64_t>((g1 - g0) / 256 + 1, int64_t(sms) * 8));
-    k_i8_count<<<grid, 256, 0, st>>>(t.key.ptr, g0, g1, loff.ptr, t.depth, cnt.ptr, pos.ptr);
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(nt / 256 + 1, int64_t(sms) * 8));
+    k_i8_keys<<<grid, 256, 0, st>>>(t.key.ptr, g0, g1, loff.ptr, t.depth, t.parent.ptr, t.colleague.ptr, t.nchild.ptr, k0.ptr,
+                                    v0.ptr, cnt.ptr);
     SFMM_CHECK_LAUNCH();
-    std::vector<int32_t> hc(ngrp), ho(ngrp);
+    // stable radix sort of (group, pattern) keys; Morton order within a key
+    int end_bit = 27;
+    while ((int64_t(1) << (end_bit - 27)) < ngrp) ++end_bit;
+    cub::DoubleBuffer<uint64_t> kb(k0.ptr, k1.ptr);
+    cub::DoubleBuffer<int32_t> vb(v0.ptr, v1.ptr);
+    size_t tmp_bytes = 0;
+    SFMM_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, kb, vb, static_cast<int>(nt), 0, end_bit, st));
+    DevBuf<uint8_t> tmp;
+    tmp.alloc(std::max<size_t>(tmp_bytes, 1), st);
+    SFMM_CUDA(cub::DeviceRadixSort::SortPairs(tmp.ptr, tmp_bytes, kb, vb, static_cast<int>(nt), 0, end_bit, st));
+    std::vector<int32_t> hc(ngrp), ho(ngrp), hs(ngrp);
     SFMM_CUDA(cudaMemcpyAsync(hc.data(), cnt.ptr, ngrp * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0, acc = 0; i < ngrp; ++i) {
+        hs[i] = acc;
+        acc += hc[i];
+    }
+    gstart.alloc(ngrp, st);
+    SFMM_CUDA(cudaMemcpyAsync(gstart.ptr, hs.data(), ngrp * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    k_i8_pos<<<grid, 256, 0, st>>>(nt, g0, kb.Current(), vb.Current(), gstart.ptr, pos.ptr);
+    SFMM_CHECK_LAUNCH();
+    // row blocks of a level interleaved by octant: block b of the 8 octant
+    // groups (targets that share most sources) are adjacent, so the items that
+    // run together gather the same source moments; an octant with fewer
+    // blocks leaves empty ones (no targets, no work)
     int64_t nrb = 0;
-    for (int i = 0; i < ngrp; ++i) {
-        ho[i] = static_cast<int32_t>(nrb);
-        nrb += rdiv_up(hc[i], d->tpb);
+    for (int l = 0; l < t.depth - 1; ++l) {
+        int nb = 0;
+        for (int o = 0; o < 8; ++o) nb = std::max(nb, rdiv_up(hc[l * 8 + o], d->tpb));
+        for (int o = 0; o < 8; ++o) ho[l * 8 + o] = static_cast<int32_t>(nrb + o);
+        nrb += int64_t(nb) * 8;
     }
     d->nrb = nrb;
     rb_off.alloc(ngrp, st);
