@@ -211,6 +211,34 @@ int fmm_plan_exchange_buffer(fmm_plan* plan, int which, void** device_ptr, int64
 int fmm_plan_capture(fmm_plan* plan, const double* Q, double* pot, double* field);
 int fmm_plan_replay(fmm_plan* plan);
 
+/* ---- Batched solves (no counterpart in the reference): several independent
+   point sets, each with its own charges, solved by one plan and one set of
+   kernel launches.  Each set's tree is built exactly as fmm_tree_build builds
+   it (its own fitted root cube, max_particles_per_node = leaf); the trees are
+   merged into one forest, the points of each scaled into the unit cube by
+   its own box, and evaluated at once: the persistent near-field and M2L
+   kernels take the work of all sets.  The evaluation runs as a CUDA graph
+   that the context keeps per launch shape and updates in place for the next
+   batch of that shape.  pot (n x qdim) / field (n x 3) are accumulated like
+   fmm_evaluate's; all items of a batch pass pot (or all NULL) and field (or
+   all NULL).  Each set's result is the same as that set solved by a batch of
+   one (bit for bit in FP64); against fmm_evaluate of the set's own tree it
+   differs by the rounding of the scaled coordinates (1e-14 to 1e-12
+   relative in FP64).  Host
+   arrays; the axis is z and phideg 0. */
+typedef struct {
+    const double* xyz;        /* n x 3 */
+    int64_t n;
+    const double* Q;          /* n x qdim */
+    int leaf;                 /* max_particles_per_node of this set's tree */
+    double* pot;              /* n x qdim, or NULL */
+    double* field;            /* n x 3, or NULL */
+} fmm_batch_item;
+int fmm_solve_batch(fmm_context* ctx, const fmm_batch_item* items, int count, int p, int qdim, int precision, int max_level);
+/* Graph executables instantiated and updated in place by this context's
+   batches so far. */
+int fmm_batch_graph_stats(const fmm_context* ctx, int64_t* instantiated, int64_t* updated);
+
 /* Device time (ms) of each phase of the last evaluation: [0] P2M+M2M,
    [1] M2L, [2] L2L+L2P, [3] P2P (it runs on a second stream beside the far
    field, so [0] + [1] + [2] + [3] can exceed [4]), [4] total; and of the last

@@ -89,6 +89,8 @@ def load_library():
         "fmm_server_wait": ([vp, i64, C.POINTER(dbl)], i32),
         "fmm_server_stats": ([vp, C.POINTER(dbl)], i32),
         "fmm_server_memory": ([vp, C.POINTER(dbl)], i32),
+        "fmm_solve_batch": ([vp, vp, i32, i32, i32, i32, i32], i32),
+        "fmm_batch_graph_stats": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)
@@ -406,6 +408,42 @@ def direct(positions, Q, targets, pot=True, field=True, ctx: Context | None = No
     if po is not None and qdim == 1:
         po = po[:, 0]
     return po, fo
+
+
+class _BatchItem(C.Structure):
+    _fields_ = [("xyz", C.c_void_p), ("n", C.c_int64), ("Q", C.c_void_p), ("leaf", C.c_int), ("pot", C.c_void_p),
+                ("field", C.c_void_p)]
+
+
+def solve_batch(sets, p: int, qdim: int = 1, precision: str = "fp64", leaf=64, pot=True, field=True,
+                ctx: Context | None = None, max_level: int = 20):
+    """Solve several independent point sets with one plan (fmm_solve_batch):
+    ``sets`` is a list of (positions, charges); ``leaf`` one leaf size or one
+    per set.  Returns a list of (pot, field) per set; numpy in, numpy out."""
+    ctx = ctx or default_context()
+    leaves = list(leaf) if np.ndim(leaf) else [leaf] * len(sets)
+    keep, items, outs = [], (_BatchItem * len(sets))(), []
+    for k, (pos, Q) in enumerate(sets):
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        Q = np.ascontiguousarray(Q, dtype=np.float64)
+        n = pos.shape[0]
+        po = np.zeros((n,) if qdim == 1 else (n, qdim)) if pot else None
+        fo = np.zeros((n, 3)) if field else None
+        keep += [pos, Q]
+        items[k] = _BatchItem(pos.ctypes.data, n, Q.ctypes.data, int(leaves[k]), po.ctypes.data if pot else None,
+                              fo.ctypes.data if field else None)
+        outs.append((po, fo))
+    _check(load_library().fmm_solve_batch(ctx._h, C.cast(items, C.c_void_p), len(sets), p, qdim, PRECISION[precision],
+                                          max_level))
+    return outs
+
+
+def batch_graph_stats(ctx: Context | None = None) -> dict:
+    """Graph executables the context's batches instantiated and updated in place."""
+    ctx = ctx or default_context()
+    a, b = C.c_int64(), C.c_int64()
+    _check(load_library().fmm_batch_graph_stats(ctx._h, C.byref(a), C.byref(b)))
+    return {"instantiated": a.value, "updated": b.value}
 
 
 class Server:

@@ -1,6 +1,8 @@
 // C ABI of the library (include/simplefmm_b200.h).  Every entry point
 // converts exceptions to an fmm_status and records a per-thread message.
+#include <algorithm>
 #include <atomic>
+#include <memory>
 #include <cstring>
 #include <new>
 #include <string>
@@ -82,6 +84,8 @@ void release_context(fmm_context* ctx)
         cudaStreamSynchronize(ctx->c.retired);
         cudaStreamDestroy(ctx->c.retired);
     }
+    for (auto& e : ctx->c.batch_graphs)
+        if (e.second) cudaGraphExecDestroy(e.second);
     if (ctx->c.own_stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
 }
@@ -467,6 +471,179 @@ int fmm_plan_capture(fmm_plan* plan, const double* Q, double* pot, double* field
     SFMM_CUDA(cudaStreamEndCapture(c.stream, &pl.graph));
     SFMM_CUDA(cudaGraphInstantiate(&pl.graph_exec, pl.graph, 0));
     API_CATCH
+}
+
+// One evaluation of the batch's forest plan through the context's graph
+// executable for its launch shape (a new one when none can be updated).
+static void evaluate_graph(sfmm::Plan& pl, const double* Q, double* pot, double* field)
+{
+    sfmm::Context& c = *pl.tree->ctx;
+    cudaGraph_t g = nullptr;
+    SFMM_CUDA(cudaStreamBeginCapture(c.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+        sfmm::plan_evaluate(pl, Q, pot, field);
+    } catch (...) {
+        cudaStreamEndCapture(c.stream, &g);
+        if (g) cudaGraphDestroy(g);
+        throw;
+    }
+    SFMM_CUDA(cudaStreamEndCapture(c.stream, &g));
+    // launch shape: the kernel sequence depends on the depth, the order, the
+    // precision, the charge components and the outputs
+    const uint64_t shape = uint64_t(pl.tree->depth) | uint64_t(pl.p) << 8 | uint64_t(pl.precision) << 16 |
+                           uint64_t(pl.qdim) << 20 | uint64_t(pot != nullptr) << 24 | uint64_t(field != nullptr) << 25 |
+                           uint64_t(pl.i8 != nullptr) << 26;
+    cudaGraphExec_t exec = nullptr;
+    for (auto& e : c.batch_graphs)
+        if (e.first == shape) {
+            cudaGraphExecUpdateResultInfo info{};
+            if (cudaGraphExecUpdate(e.second, g, &info) == cudaSuccess) {
+                exec = e.second;
+                ++c.batch_graph_updates;
+            } else {
+                cudaGetLastError();
+                cudaGraphExecDestroy(e.second);
+                e.second = nullptr;
+            }
+            break;
+        }
+    if (!exec) {
+        const cudaError_t rc = cudaGraphInstantiate(&exec, g, 0);
+        if (rc != cudaSuccess) {
+            cudaGraphDestroy(g);
+            SFMM_CUDA(rc);
+        }
+        ++c.batch_graph_instantiations;
+        bool placed = false;
+        for (auto& e : c.batch_graphs)
+            if (e.first == shape) {
+                e.second = exec;
+                placed = true;
+            }
+        if (!placed) {
+            if (c.batch_graphs.size() >= 16) {           // a few shapes are live at a time
+                cudaGraphExecDestroy(c.batch_graphs.front().second);
+                c.batch_graphs.erase(c.batch_graphs.begin());
+            }
+            c.batch_graphs.emplace_back(shape, exec);
+        }
+    }
+    cudaGraphDestroy(g);
+    SFMM_CUDA(cudaGraphLaunch(exec, c.stream));
+}
+
+int fmm_solve_batch(fmm_context* ctx, const fmm_batch_item* items, int count, int p, int qdim, int precision, int max_level)
+{
+    API_TRY
+    if (!ctx || !items || count < 1) return fail(FMM_ERR_INVALID_ARGUMENT, "need a context and at least one item");
+    if (qdim < 1 || qdim > 3 || p < 0 || p > 16 || max_level < 1 || max_level > sfmm::kKeyLevel)
+        return fail(FMM_ERR_INVALID_ARGUMENT, "bad qdim, p or max_level");
+    if (precision != FMM_PRECISION_FP64 && precision != FMM_PRECISION_MIXED)
+        return fail(FMM_ERR_INVALID_ARGUMENT, "precision must be FMM_PRECISION_FP64 or FMM_PRECISION_MIXED");
+    const bool want_pot = items[0].pot != nullptr, want_field = items[0].field != nullptr;
+    if (!want_pot && !want_field) return fail(FMM_ERR_INVALID_ARGUMENT, "items ask for no output");
+    if (want_field && qdim == 2) return fail(FMM_ERR_UNSUPPORTED, "the field needs N = 1 or N = 3 charges");
+    int64_t N = 0;
+    for (int r = 0; r < count; ++r) {
+        const fmm_batch_item& it = items[r];
+        if (!it.xyz || !it.Q || it.n <= 0 || it.leaf < 1) return fail(FMM_ERR_INVALID_ARGUMENT, "bad batch item");
+        if ((it.pot != nullptr) != want_pot || (it.field != nullptr) != want_field)
+            return fail(FMM_ERR_INVALID_ARGUMENT, "all items must ask for the same outputs");
+        N += it.n;
+    }
+    if (N >= (int64_t(1) << 31)) return fail(FMM_ERR_UNSUPPORTED, "a batch holds fewer than 2^31 points");
+    sfmm::Context& c = ctx->c;
+    bind(c);
+    if (c.stream == nullptr || c.stream == cudaStreamLegacy || c.stream == cudaStreamPerThread)
+        return fail(FMM_ERR_UNSUPPORTED, "batches need the context's own stream, not a default stream");
+    cudaStream_t st = c.stream;
+    // inputs, concatenated
+    std::vector<double> hx(size_t(3) * N), hq(size_t(N) * qdim);
+    std::vector<int64_t> base(count + 1, 0);
+    for (int r = 0; r < count; ++r) {
+        base[r + 1] = base[r] + items[r].n;
+        std::copy(items[r].xyz, items[r].xyz + 3 * items[r].n, hx.begin() + 3 * base[r]);
+        std::copy(items[r].Q, items[r].Q + qdim * items[r].n, hq.begin() + qdim * base[r]);
+    }
+    sfmm::DevBuf<double> dx, dq, dpot, dfield;
+    dx.alloc(size_t(3) * N, st);
+    dq.alloc(size_t(N) * qdim, st);
+    SFMM_CUDA(cudaMemcpyAsync(dx.ptr, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    SFMM_CUDA(cudaMemcpyAsync(dq.ptr, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    // member trees, each as a single solve builds it
+    std::vector<std::unique_ptr<sfmm::Tree>> trees;
+    std::vector<const sfmm::Tree*> members;
+    for (int r = 0; r < count; ++r) {
+        trees.emplace_back(new sfmm::Tree);
+        sfmm::Tree& t = *trees.back();
+        t.ctx = &c;
+        t.n = items[r].n;
+        sfmm::build_tree(t, dx.ptr + 3 * base[r], max_level, items[r].leaf, 2, 0.0);
+        members.push_back(&t);
+    }
+    sfmm::Tree F;
+    sfmm::build_forest(F, members);
+    trees.clear();
+    members.clear();
+    {
+        sfmm::Plan pl;
+        // the plan's events, destroyed when the batch is done (after the sync below)
+        struct Events {
+            sfmm::Plan& pl;
+            explicit Events(sfmm::Plan& q) : pl(q)
+            {
+                for (auto& e : pl.ev) SFMM_CUDA(cudaEventCreate(&e));
+                for (cudaEvent_t* e : {&pl.fork, &pl.join, &pl.io_start, &pl.io_done})
+                    SFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+            }
+            ~Events()
+            {
+                for (auto& e : pl.ev)
+                    if (e) cudaEventDestroy(e);
+                for (cudaEvent_t e : {pl.fork, pl.join, pl.io_start, pl.io_done})
+                    if (e) cudaEventDestroy(e);
+            }
+        } events(pl);
+        pl.tree = &F;
+        pl.p = p;
+        pl.qdim = qdim;
+        pl.precision = precision;
+        sfmm::plan_init(pl);
+        if (want_pot) {
+            dpot.alloc(size_t(N) * qdim, st);
+            SFMM_CUDA(cudaMemsetAsync(dpot.ptr, 0, dpot.bytes(), st));
+        }
+        if (want_field) {
+            dfield.alloc(size_t(N) * 3, st);
+            SFMM_CUDA(cudaMemsetAsync(dfield.ptr, 0, dfield.bytes(), st));
+        }
+        evaluate_graph(pl, dq.ptr, dpot.ptr, dfield.ptr);
+        if (want_pot) SFMM_CUDA(cudaMemcpyAsync(hq.data(), dpot.ptr, size_t(N) * qdim * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (want_field) {
+            hx.resize(size_t(3) * N);
+            SFMM_CUDA(cudaMemcpyAsync(hx.data(), dfield.ptr, size_t(N) * 3 * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+        SFMM_CUDA(cudaStreamSynchronize(st));
+        sfmm::m2l_i8_check(pl);
+    }
+    // back to each set's units: potential / width, field / width^2
+    for (int r = 0; r < count; ++r) {
+        const double w = F.member_width.empty() ? 1.0 : F.member_width[r];
+        const double s1 = 1.0 / w, s2 = s1 * s1;
+        if (want_pot)
+            for (int64_t i = 0; i < items[r].n * qdim; ++i) items[r].pot[i] += s1 * hq[qdim * base[r] + i];
+        if (want_field)
+            for (int64_t i = 0; i < items[r].n * 3; ++i) items[r].field[i] += s2 * hx[3 * base[r] + i];
+    }
+    API_CATCH
+}
+
+int fmm_batch_graph_stats(const fmm_context* ctx, int64_t* instantiated, int64_t* updated)
+{
+    if (!ctx || !instantiated || !updated) return fail(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    *instantiated = ctx->c.batch_graph_instantiations;
+    *updated = ctx->c.batch_graph_updates;
+    return FMM_OK;
 }
 
 int fmm_plan_replay(fmm_plan* plan)

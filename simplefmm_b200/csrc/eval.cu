@@ -430,6 +430,7 @@ static EvalArgs make_args(Plan& pl, double* pot, double* field)
     a.n_leaves = t.n_leaves;
     a.far_leaf0 = t.depth >= 2 ? t.leaf_off[2] : t.n_leaves;
     a.box = t.d_box.ptr;
+    a.node_tree = t.n_trees > 1 ? t.node_tree.ptr : nullptr;
     a.key = t.key.ptr;
     a.pbeg = t.pbeg.ptr;
     a.pend = t.pend.ptr;

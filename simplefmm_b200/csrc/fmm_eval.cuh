@@ -86,6 +86,7 @@ struct EvalArgs {
     int* m2l_ctr;                         // FP64 M2L: the counter blocks take sibling groups from
     int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
     const uint8_t* own_leaf;              // sharded plan: 1 for this shard's leaves (global leaf id); NULL = all
+    const int32_t* node_tree;             // forest: member tree of each node; NULL = one tree
     // direct M2L (m2l_direct.cu, FMM_M2L_METHOD_DIRECT): dense coefficient table,
     // Z of the interaction-list angles, phases; row lengths
     int m2l_direct;

@@ -179,6 +179,10 @@ struct Context {
                                           // on it beside the far field (forked from and joined
                                           // back into `stream` with events)
     int sm_count = 148;
+    // batched solves (fmm_solve_batch): executable graphs of the batch
+    // evaluation kept per launch shape, updated in place for the next batch
+    std::vector<std::pair<uint64_t, cudaGraphExec_t>> batch_graphs;
+    int64_t batch_graph_instantiations = 0, batch_graph_updates = 0;
 };
 
 // Device-resident octree: nodes of all levels concatenated level by level
@@ -226,6 +230,12 @@ struct Tree {
     // device time of the build's phases: keys, refinement, leaves and points,
     // colleagues, interaction lists, near-field lists
     float phase_ms[6] = {};
+
+    // a forest of independent trees (forest.cu): the member of each node; empty
+    // for a single tree
+    DevBuf<int32_t> node_tree;
+    int n_trees = 1;
+    std::vector<double> member_width;     // root-cube width of each member
 };
 
 struct Plan;
@@ -236,6 +246,9 @@ struct Plan;
 void build_tree(Tree& t, const double* xyz_dev, int max_level, int max_ppn, int vertical_axis, double phideg,
                 const double* corner3 = nullptr, double width = 0.0);
 int64_t tree_export(const Tree& t, int level, int what, void* host_out);
+// forest.cu: merge trees built on one context into a forest F (member points
+// scaled into the unit cube, each by its own box; lists never cross members)
+void build_forest(Tree& F, const std::vector<const Tree*>& members);
 void tree_phase_bytes(const Tree& t, double* bytes6);
 
 // direct.cu: a target index outside [0, n) is not read; its outputs are NaN

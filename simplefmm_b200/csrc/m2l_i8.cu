@@ -100,7 +100,7 @@ struct I8PlanData {
     DevBuf<int32_t> used, nused;              // [row block][216]: slots that occur; their count
     DevBuf<int32_t> rb_tgt, rb_info;          // [row block][tpb] target nodes; level | octant << 8 | ntgt << 12
     DevBuf<int8_t> md;                        // moment digits [node][qdim][K steps][ND digits][32 B]
-    DevBuf<uint32_t> alpha;                   // per level: float bits of alpha_l
+    DevBuf<uint32_t> alpha;                   // per (member tree, level): float bits of alpha
     DevBuf<int32_t> err;                      // wait expired
 };
 
@@ -251,7 +251,8 @@ __global__ void k_i8_alpha(EvalArgs a, uint32_t* __restrict__ alpha_bits)
             mx = fmaxf(mx, __double2float_ru(fmax(fabs(v.re), fabs(v.im)) * sc));
         }
         for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0 && mx > 0.f) atomicMax(alpha_bits + l, __float_as_uint(mx));
+        const int tr = a.node_tree ? a.node_tree[g] : 0;
+        if (lane == 0 && mx > 0.f) atomicMax(alpha_bits + tr * (kKeyLevel + 2) + l, __float_as_uint(mx));
     }
 }
 
@@ -266,7 +267,8 @@ __global__ void k_i8_mdigits(EvalArgs a, int KS, const uint32_t* __restrict__ al
         const int64_t g = g0 + w / qd;
         const int c = static_cast<int>(w % qd);
         const int l = level_of(a, g);
-        const double al = double(__uint_as_float(alpha_bits[l]));
+        const int tr = a.node_tree ? a.node_tree[g] : 0;
+        const double al = double(__uint_as_float(alpha_bits[tr * (kKeyLevel + 2) + l]));
         const double s = double(1 << l) / a.box->width;
         int8_t* dst = md + (g * qd + c) * int64_t(KS) * (32 * ND);
         for (int k = lane; k < KP; k += 32) {
@@ -545,11 +547,9 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_m2l_i8(EvalArgs a, I8Args g)
                 }
                 on = isA ? a.want_pot : a.want_field;
             }
+            // alpha of the column's tree (a forest's members keep their own moment scales)
             double scale = 0.0;
-            if (on && nst > 0) {
-                const double al = double(__uint_as_float(g.alpha[l]));
-                scale = al * g.beta[r] / (127.0 * 127.0) * pow(double(1 << l) / a.box->width, double(j + 1));
-            }
+            if (on && nst > 0) scale = g.beta[r] / (127.0 * 127.0) * pow(double(1 << l) / a.box->width, double(j + 1));
             if (nst > 0) {
                 const bool got = bar_wait(&ctl.tfull, static_cast<uint32_t>(nb) & 1, abort);
                 if (!__all_sync(0xffffffffu, got)) {          // warp-uniform: the loads below are .aligned
@@ -575,13 +575,14 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_m2l_i8(EvalArgs a, I8Args g)
                     const int col = c0 + e;
                     const int t = col / qd, comp = col % qd;
                     if (t >= ntg || t >= tpb) continue;
+                    const int64_t node = g.rb_tgt[rb * tpb + t];
                     double v = 0.0;
                     if (nst > 0) {
 #pragma unroll
                         for (int gsum = ND - 1; gsum >= 0; --gsum) v = v * (1.0 / 256) + double(int(sg[gsum][e]));
-                        v *= scale;
+                        const int tr = a.node_tree ? a.node_tree[node] : 0;
+                        v *= scale * double(__uint_as_float(g.alpha[tr * (kKeyLevel + 2) + l]));
                     }
-                    const int64_t node = g.rb_tgt[rb * tpb + t];
                     double* dst = base + 2 * ((node * qd + comp) * stride + tri_i);
                     dst[po] = v;
                     if (kk == 0) dst[1] = 0.0;               // Im of an m = 0 coefficient
@@ -726,7 +727,7 @@ void m2l_i8_setup(Plan& pl)
                                                                                                      d->used.ptr, d->nused.ptr);
     SFMM_CHECK_LAUNCH();
     d->md.alloc(size_t(t.n_nodes) * pl.qdim * d->tab->KS * 32 * d->ND, st);
-    d->alpha.alloc(kKeyLevel + 2, st);
+    d->alpha.alloc(size_t(kKeyLevel + 2) * t.n_trees, st);
     d->err.alloc(1, st);
     SFMM_CUDA(cudaMemsetAsync(d->err.ptr, 0, sizeof(int32_t), st));
     SFMM_CUDA(cudaStreamSynchronize(st));       // the set-up's temporaries are freed on return
