@@ -370,7 +370,7 @@ def serve_bench(args):
             lat.append(l_ms)
         th.join()
         span = time.perf_counter() - t0
-        st = srv.stats()
+        st = dict(srv.stats(), **srv.batch_stats())
         srv.close()
         return np.array(lat), span, st
 
@@ -400,8 +400,11 @@ def serve_bench(args):
     line = {
         "metric": "solves/s on a served mixed-size stream (p50/p99 latency beside)", "value": k / span_s,
         "unit": "solves/s", "n_gpus": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32 near field, 3xtf32 M2L, f64 moments and sums",
+        "dtype": "f64" if args.precision == "fp64" else (
+            "f32 near field; M2L in int8 slices on the tensor cores (32-bit fixed point, exact int32 sums); "
+            "f64 moments, locals and sums"),
         "data": "synthetic (seeded; Poisson arrivals; N log-uniform [1e3, 1e6]; uniform / Plummer / shell; p in {6, 10})",
+        "batching": "requests of <= 65,536 points solved in batches sharing one plan and one graph-launched evaluation",
         "config": {"workload": f"serving_stream_{k}_requests_rate{args.rate:g}", "requests": k, "rate_per_s": args.rate,
                    "points_total": total_points, "slots": args.slots, "budget_gib": args.budget_gib,
                    "precision": args.precision, "leaf": "autotuned {32, 64, 128}"},

@@ -304,6 +304,10 @@ int fmm_server_stats(fmm_server* server, double* stats8);
    p and precision, built by the first request that needs them) count toward
    that request. */
 int fmm_server_memory(fmm_server* server, double* out3);
+/* Small requests (at most 65,536 points) are solved in batches with the
+   queued requests that can share their plan (fmm_solve_batch); the number of
+   batches and of requests solved in them so far. */
+int fmm_server_batch_stats(fmm_server* server, int64_t* batches, int64_t* batched_requests);
 
 /* Number of kernels this library has launched in this process. */
 int fmm_launch_count(int64_t* count);

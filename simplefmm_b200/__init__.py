@@ -90,6 +90,7 @@ def load_library():
         "fmm_server_stats": ([vp, C.POINTER(dbl)], i32),
         "fmm_server_memory": ([vp, C.POINTER(dbl)], i32),
         "fmm_solve_batch": ([vp, vp, i32, i32, i32, i32, i32], i32),
+        "fmm_server_batch_stats": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
         "fmm_batch_graph_stats": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
     }
     for name, (args, res) in sig.items():
@@ -490,6 +491,12 @@ class Server:
         _check(load_library().fmm_server_stats(self._h, s))
         return dict(completed=int(s[0]), p50_ms=s[1], p99_ms=s[2], mean_ms=s[3], peak_running=int(s[4]),
                     peak_bytes=int(s[5]), budget_bytes=int(s[6]), queued=int(s[7]))
+
+    def batch_stats(self) -> dict:
+        """Batches of small requests solved together so far (fmm_server_batch_stats)."""
+        a, b = C.c_int64(), C.c_int64()
+        _check(load_library().fmm_server_batch_stats(self._h, C.byref(a), C.byref(b)))
+        return {"batches": a.value, "batched_requests": b.value}
 
     def memory(self) -> dict:
         """Measured device memory of the running requests (fmm_server_memory)."""

@@ -25,6 +25,16 @@
 // evaluation on the device (CUDA events on its stream, after the operator
 // tables exist), keeps each candidate's best rate, and then uses the fastest.
 //
+// Small solves are batched: a worker that admits a request of at most
+// kBatchMaxPoints points also takes the queued requests that can share its
+// plan (same order, precision, charge components and outputs), up to
+// kBatchMaxCount requests or kBatchPoints points in all, scanning the first
+// kBatchScan queued requests, and solves them together with fmm_solve_batch:
+// their trees merged into one forest, one plan, one graph-launched evaluation
+// whose persistent near-field and M2L kernels take the work of all of them.
+// A small request always goes this way, alone or with others, so its result
+// does not depend on its company (bit for bit: no sum crosses two requests).
+//
 // Latency is measured from submission to completion (queueing included);
 // fmm_server_stats reports its p50 / p99 over completed requests.
 #include <algorithm>
@@ -72,6 +82,10 @@ struct Request {
 };
 
 constexpr int kLeafCandidates[] = {32, 64, 128};
+constexpr int64_t kBatchMaxPoints = 65536;      // requests batched with others
+constexpr int kBatchMaxCount = 32;
+constexpr int64_t kBatchPoints = 1 << 20;
+constexpr size_t kBatchScan = 256;
 
 // Device memory of one solve: tree (points, keys, lists) and plan
 // (expansions of order p for qdim components, outputs).  Nodes per point and
@@ -145,11 +159,47 @@ struct fmm_server {
     int64_t next_id = 1;
     bool stopping = false;
     std::vector<double> latencies_ms;
+    int64_t batches = 0, batched = 0;
     Autotuner tuner;
 
     void worker(int slot);
     void run(fmm_context* c, Request& r);
+    void run_batch(fmm_context* c, std::vector<std::shared_ptr<Request>>& rs);
+    void finish(Request& r);
 };
+
+void fmm_server::run_batch(fmm_context* c, std::vector<std::shared_ptr<Request>>& rs)
+{
+    sfmm::AllocMeter own;
+    sfmm::set_thread_alloc_meters(&own, &meter);
+    std::vector<fmm_batch_item> items(rs.size());
+    for (size_t k = 0; k < rs.size(); ++k) {
+        const Request& r = *rs[k];
+        items[k] = fmm_batch_item{r.xyz, r.n, r.Q, r.leaf, r.pot, r.field};
+    }
+    const Request& r0 = *rs[0];
+    const int rc = fmm_solve_batch(c, items.data(), static_cast<int>(items.size()), r0.p, r0.qdim, r0.precision, 20);
+    const std::string err = rc == FMM_OK ? std::string() : std::string(fmm_last_error());
+    sfmm::set_thread_alloc_meters(nullptr, nullptr);
+    // the batch's measured peak, shared in proportion to the requests' estimates
+    size_t total = 0;
+    for (auto& r : rs) total += r->bytes;
+    for (auto& r : rs) {
+        r->status = rc;
+        r->error = err;
+        r->measured = total ? int64_t(double(own.peak.load()) * double(r->bytes) / double(total)) : 0;
+    }
+}
+
+void fmm_server::finish(Request& r)
+{
+    r.t_done = Clock::now();
+    r.done = true;
+    in_use -= r.bytes;
+    --running;
+    if (r.bytes) worst_ratio = std::max(worst_ratio, double(r.measured) / double(r.bytes));
+    if (r.status == FMM_OK) latencies_ms.push_back(std::chrono::duration<double, std::milli>(r.t_done - r.t_submit).count());
+}
 
 void fmm_server::run(fmm_context* c, Request& r)
 {
@@ -176,7 +226,7 @@ void fmm_server::worker(int slot)
     fmm_context* c = ctx[slot];
     sfmm::set_thread_block_cache(false);
     for (;;) {
-        std::shared_ptr<Request> r;
+        std::vector<std::shared_ptr<Request>> rs;
         {
             std::unique_lock<std::mutex> lk(mu);
             // admit the oldest queued request once its memory fits beside the running ones
@@ -184,23 +234,39 @@ void fmm_server::worker(int slot)
                 return (!queue.empty() && in_use + queue.front()->bytes <= budget) || (stopping && queue.empty());
             });
             if (queue.empty()) return;                      // stopping and drained
-            r = queue.front();
+            rs.push_back(queue.front());
             queue.pop_front();
-            in_use += r->bytes;
+            in_use += rs[0]->bytes;
+            const Request& r0 = *rs[0];
+            if (r0.n <= kBatchMaxPoints) {
+                // the queued small requests that can share its plan, while memory allows
+                int64_t pts = r0.n;
+                for (auto it = queue.begin(); it != queue.end() && size_t(it - queue.begin()) < kBatchScan &&
+                                              rs.size() < size_t(kBatchMaxCount);) {
+                    const Request& q = **it;
+                    if (q.n <= kBatchMaxPoints && q.p == r0.p && q.precision == r0.precision && q.qdim == r0.qdim &&
+                        (q.pot != nullptr) == (r0.pot != nullptr) && (q.field != nullptr) == (r0.field != nullptr) &&
+                        pts + q.n <= kBatchPoints && in_use + q.bytes <= budget) {
+                        pts += q.n;
+                        in_use += q.bytes;
+                        rs.push_back(*it);
+                        it = queue.erase(it);
+                    } else {
+                        ++it;
+                    }
+                }
+                ++batches;
+                batched += int64_t(rs.size());
+            }
             peak_in_use = std::max(peak_in_use, in_use);
-            ++running;
+            running += int(rs.size());
             peak_running = std::max(peak_running, running);
         }
-        run(c, *r);
+        if (rs[0]->n <= kBatchMaxPoints) run_batch(c, rs);
+        else run(c, *rs[0]);
         {
             std::lock_guard<std::mutex> lk(mu);
-            r->t_done = Clock::now();
-            r->done = true;
-            in_use -= r->bytes;
-            --running;
-            if (r->bytes) worst_ratio = std::max(worst_ratio, double(r->measured) / double(r->bytes));
-            if (r->status == FMM_OK)
-                latencies_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+            for (auto& r : rs) finish(*r);
         }
         cv_done.notify_all();
         cv_work.notify_all();
@@ -330,6 +396,15 @@ int fmm_server_stats(fmm_server* s, double* stats8)
     stats8[5] = double(s->peak_in_use);
     stats8[6] = double(s->budget);
     stats8[7] = double(s->queue.size());
+    return FMM_OK;
+}
+
+int fmm_server_batch_stats(fmm_server* s, int64_t* batches, int64_t* batched_requests)
+{
+    if (!s || !batches || !batched_requests) return sfmm::record_failure(FMM_ERR_INVALID_ARGUMENT, "NULL argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    *batches = s->batches;
+    *batched_requests = s->batched;
     return FMM_OK;
 }
 
