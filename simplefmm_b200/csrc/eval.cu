@@ -405,6 +405,8 @@ void plan_init(Plan& pl)
     shift_setup(pl);
     p2p_setup(pl);
     pl.m2l_ctr.alloc(1, st);
+    pl.wait_err.alloc(1, st);
+    SFMM_CUDA(cudaMemsetAsync(pl.wait_err.ptr, 0, sizeof(int32_t), st));
     // test switch: the row-owner M2L kernel instead of the tensor-core ones
     const char* mk = std::getenv("SFMM_M2L_KERNEL");
     pl.m2l_force_rows = mk && std::strcmp(mk, "rows") == 0;
@@ -431,6 +433,7 @@ static EvalArgs make_args(Plan& pl, double* pot, double* field)
     a.far_leaf0 = t.depth >= 2 ? t.leaf_off[2] : t.n_leaves;
     a.box = t.d_box.ptr;
     a.node_tree = t.n_trees > 1 ? t.node_tree.ptr : nullptr;
+    a.wait_err = pl.wait_err.ptr;
     a.key = t.key.ptr;
     a.pbeg = t.pbeg.ptr;
     a.pend = t.pend.ptr;

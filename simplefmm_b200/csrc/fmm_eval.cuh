@@ -87,6 +87,7 @@ struct EvalArgs {
     int m2l_force_rows;                   // run the row-owner M2L kernel (plan made with SFMM_M2L_KERNEL=rows)
     const uint8_t* own_leaf;              // sharded plan: 1 for this shard's leaves (global leaf id); NULL = all
     const int32_t* node_tree;             // forest: member tree of each node; NULL = one tree
+    int* wait_err;                        // set by a kernel whose bounded pipeline wait expired
     // direct M2L (m2l_direct.cu, FMM_M2L_METHOD_DIRECT): dense coefficient table,
     // Z of the interaction-list angles, phases; row lengths
     int m2l_direct;
@@ -152,6 +153,7 @@ struct Plan {
     std::vector<int64_t> own_parent_b, own_parent_e;   // per parent level q: node range [b, e)
     std::shared_ptr<DirectDevTables> dtab;    // FMM_M2L_METHOD_DIRECT
     std::shared_ptr<I8PlanData> i8;           // mixed plans: the tensor-core (tcgen05, int8 slices) M2L
+    DevBuf<int32_t> wait_err;                 // a kernel's bounded wait expired (EvalArgs::wait_err)
     bool m2l_rotation_only = false;           // SFMM_M2L_KERNEL=rotation: mixed plans keep the TF32 rotation M2L
     DevBuf<double> p2p_part;
     int64_t p2p_items = 0, p2p_rows = 0;
@@ -204,7 +206,8 @@ void plan_read_timings(Plan& pl, double* ms6);
 std::shared_ptr<DirectDevTables> direct_tables_on_device(int device, int p, cudaStream_t st);
 // m2l_i8.cu: whether a plan takes the tensor-core M2L; its set-up at plan
 // creation (fills pl.i8); the launch (moment digits, then the M2L of every
-// level); the report of an expired pipeline wait (throws FMM_ERR_TIMEOUT).
+// level); the report of an expired pipeline wait of the plan's kernels (the
+// tensor-core M2L, the near field's bulk copies): throws FMM_ERR_TIMEOUT.
 bool m2l_i8_supported(const Plan& pl);
 void m2l_i8_setup(Plan& pl);
 void launch_m2l_i8(Plan& pl, const EvalArgs& a, cudaStream_t st);

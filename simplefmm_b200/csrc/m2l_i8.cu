@@ -101,7 +101,6 @@ struct I8PlanData {
     DevBuf<int32_t> rb_tgt, rb_info;          // [row block][tpb] target nodes; level | octant << 8 | ntgt << 12
     DevBuf<int8_t> md;                        // moment digits [node][qdim][K steps][ND digits][32 B]
     DevBuf<uint32_t> alpha;                   // per (member tree, level): float bits of alpha
-    DevBuf<int32_t> err;                      // wait expired
 };
 
 namespace {
@@ -189,45 +188,62 @@ __global__ void k_i8_pos(int64_t n, int64_t g0, const uint64_t* __restrict__ ske
 
 __global__ void k_i8_assign(const uint64_t* __restrict__ key, int64_t g0, int64_t g1, const int64_t* __restrict__ lvl_off, int depth,
                             const int32_t* __restrict__ pos, const int32_t* __restrict__ rb_off, int tpb,
-                            const int32_t* __restrict__ il_ptr, const int32_t* __restrict__ il_src, const int32_t* __restrict__ il_code,
-                            int32_t* __restrict__ rb_tgt, int32_t* __restrict__ rb_info, int32_t* __restrict__ slot_src)
+                            int32_t* __restrict__ rb_tgt, int32_t* __restrict__ rb_info)
 {
     for (int64_t g = g0 + blockIdx.x * int64_t(blockDim.x) + threadIdx.x; g < g1; g += int64_t(gridDim.x) * blockDim.x) {
         int l = 2;
         while (l < depth && g >= lvl_off[l + 1]) ++l;
         const uint64_t k = key[g];
-        const int cx = compact3(k) & 1, cy = compact3(k >> 1) & 1, cz = compact3(k >> 2) & 1;
-        const int oct = cx | cy << 1 | cz << 2;
+        const int oct = int(compact3(k) & 1) | int(compact3(k >> 1) & 1) << 1 | int(compact3(k >> 2) & 1) << 2;
         const int ps = pos[g - g0];
         const int64_t rb = rb_off[(l - 2) * 8 + oct] + int64_t(ps / tpb) * 8;
         const int t = ps % tpb;
         rb_tgt[rb * tpb + t] = static_cast<int32_t>(g);
         atomicMax(rb_info + rb, l | oct << 8 | (t + 1) << 12);
-        for (int e = il_ptr[g]; e < il_ptr[g + 1]; ++e) {
-            const int code = il_code[e];
-            const int dx = (code & 7) - 3, dy = ((code >> 3) & 7) - 3, dz = ((code >> 6) & 7) - 3;
-            const int slot = (dx + 2 + cx) + 6 * (dy + 2 + cy) + 36 * (dz + 2 + cz);
-            slot_src[(rb * kI8Slots + slot) * tpb + t] = il_src[e];
-        }
     }
 }
 
-// Slots that occur in each row block, in slot order (warp per row block).
-__global__ void k_i8_used(int64_t nrb, int tpb, const int32_t* __restrict__ slot_src, int32_t* __restrict__ used,
-                          int32_t* __restrict__ nused)
+// Slot table of one row block (a block per row block): each target's sources
+// by slot, built in shared memory from the interaction lists and written out
+// whole; then the slots that occur, in slot order.
+constexpr int kI8FillThreads = 256;
+__global__ void __launch_bounds__(kI8FillThreads) k_i8_fill(int64_t nrb, int tpb, const int32_t* __restrict__ rb_tgt,
+                                                           const int32_t* __restrict__ rb_info, const int32_t* __restrict__ il_ptr,
+                                                           const int32_t* __restrict__ il_src, const int32_t* __restrict__ il_code,
+                                                           int32_t* __restrict__ slot_src, int32_t* __restrict__ used,
+                                                           int32_t* __restrict__ nused)
 {
-    const int lane = threadIdx.x & 31;
-    for (int64_t rb = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; rb < nrb; rb += (int64_t(gridDim.x) * blockDim.x) >> 5) {
-        int cnt = 0;
-        for (int s = 0; s < kI8Slots; ++s) {
-            bool any = false;
-            for (int t = lane; t < tpb; t += 32) any |= slot_src[(rb * kI8Slots + s) * tpb + t] >= 0;
-            if (__any_sync(0xffffffffu, any)) {
-                if (lane == 0) used[rb * kI8Slots + cnt] = s;
-                ++cnt;
+    extern __shared__ int32_t tab[];                     // [216][tpb]
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kI8FillThreads / 32;
+    for (int64_t rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
+        const int info = rb_info[rb];
+        const int oct = (info >> 8) & 7, ntg = info >> 12;
+        const int cx = oct & 1, cy = (oct >> 1) & 1, cz = oct >> 2;
+        for (int e = threadIdx.x; e < kI8Slots * tpb; e += kI8FillThreads) tab[e] = -1;
+        __syncthreads();
+        for (int t = warp; t < ntg; t += nw) {
+            const int g = rb_tgt[rb * tpb + t];
+            for (int e = il_ptr[g] + lane; e < il_ptr[g + 1]; e += 32) {
+                const int code = il_code[e];
+                const int dx = (code & 7) - 3, dy = ((code >> 3) & 7) - 3, dz = ((code >> 6) & 7) - 3;
+                tab[((dx + 2 + cx) + 6 * (dy + 2 + cy) + 36 * (dz + 2 + cz)) * tpb + t] = il_src[e];
             }
         }
-        if (lane == 0) nused[rb] = cnt;
+        __syncthreads();
+        for (int e = threadIdx.x; e < kI8Slots * tpb; e += kI8FillThreads) slot_src[rb * kI8Slots * tpb + e] = tab[e];
+        if (warp == 0) {
+            int cnt = 0;
+            for (int sl = 0; sl < kI8Slots; ++sl) {
+                bool any = false;
+                for (int t = lane; t < ntg; t += 32) any |= tab[sl * tpb + t] >= 0;
+                if (__any_sync(0xffffffffu, any)) {
+                    if (lane == 0) used[rb * kI8Slots + cnt] = sl;
+                    ++cnt;
+                }
+            }
+            if (lane == 0) nused[rb] = cnt;
+        }
+        __syncthreads();
     }
 }
 
@@ -718,18 +734,22 @@ void m2l_i8_setup(Plan& pl)
     d->nused.alloc(nrb, st);
     d->rb_tgt.alloc(size_t(nrb) * d->tpb, st);
     d->rb_info.alloc(nrb, st);
-    SFMM_CUDA(cudaMemsetAsync(d->slot_src.ptr, 0xFF, d->slot_src.bytes(), st));
     SFMM_CUDA(cudaMemsetAsync(d->rb_info.ptr, 0, d->rb_info.bytes(), st));
-    k_i8_assign<<<grid, 256, 0, st>>>(t.key.ptr, g0, g1, loff.ptr, t.depth, pos.ptr, rb_off.ptr, d->tpb, t.il_ptr.ptr, t.il_src.ptr,
-                                      t.il_code.ptr, d->rb_tgt.ptr, d->rb_info.ptr, d->slot_src.ptr);
+    k_i8_assign<<<grid, 256, 0, st>>>(t.key.ptr, g0, g1, loff.ptr, t.depth, pos.ptr, rb_off.ptr, d->tpb, d->rb_tgt.ptr,
+                                      d->rb_info.ptr);
     SFMM_CHECK_LAUNCH();
-    k_i8_used<<<static_cast<unsigned>(std::min<int64_t>(nrb / 8 + 1, int64_t(sms) * 8)), 256, 0, st>>>(nrb, d->tpb, d->slot_src.ptr,
-                                                                                                     d->used.ptr, d->nused.ptr);
+    const size_t fill_smem = size_t(kI8Slots) * d->tpb * sizeof(int32_t);
+    static std::once_flag fill_attr;
+    std::call_once(fill_attr, [] {
+        SFMM_CUDA(cudaFuncSetAttribute(k_i8_fill, cudaFuncAttributeMaxDynamicSharedMemorySize, kI8Slots * 128 * 4));
+    });
+    const unsigned fill_grid = static_cast<unsigned>(std::max<int64_t>(std::min<int64_t>(nrb, int64_t(sms) * 2), 1));
+    k_i8_fill<<<fill_grid, kI8FillThreads, fill_smem, st>>>(nrb, d->tpb, d->rb_tgt.ptr, d->rb_info.ptr, t.il_ptr.ptr,
+                                                           t.il_src.ptr, t.il_code.ptr, d->slot_src.ptr, d->used.ptr,
+                                                           d->nused.ptr);
     SFMM_CHECK_LAUNCH();
     d->md.alloc(size_t(t.n_nodes) * pl.qdim * d->tab->KS * 32 * d->ND, st);
     d->alpha.alloc(size_t(kKeyLevel + 2) * t.n_trees, st);
-    d->err.alloc(1, st);
-    SFMM_CUDA(cudaMemsetAsync(d->err.ptr, 0, sizeof(int32_t), st));
     SFMM_CUDA(cudaStreamSynchronize(st));       // the set-up's temporaries are freed on return
     pl.i8 = d;
 }
@@ -747,7 +767,7 @@ void launch_m2l_i8(Plan& pl, const EvalArgs& a, cudaStream_t st)
     k_i8_mdigits<4><<<gw, 256, 0, st>>>(a, tb.KS, d.alpha.ptr, d.md.ptr);
     SFMM_CHECK_LAUNCH();
     I8Args g{tb.op.ptr, tb.beta.ptr, d.md.ptr, d.alpha.ptr, d.slot_src.ptr, d.used.ptr, d.nused.ptr, d.rb_tgt.ptr,
-             d.rb_info.ptr, d.nrb, d.tpb, tb.NCH, tb.KS, tb.RA, tb.R, d.err.ptr};
+             d.rb_info.ptr, d.nrb, d.tpb, tb.NCH, tb.KS, tb.RA, tb.R, a.wait_err};
     static std::once_flag attr;
     std::call_once(attr, [] {
         SFMM_CUDA(cudaFuncSetAttribute(k_m2l_i8<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(I8Cfg<4>::Smem)));
@@ -760,14 +780,14 @@ void launch_m2l_i8(Plan& pl, const EvalArgs& a, cudaStream_t st)
 
 void m2l_i8_check(Plan& pl)
 {
-    if (!pl.i8) return;
+    if (!pl.wait_err.ptr) return;
     cudaStream_t st = pl.tree->ctx->stream;
     int v = 0;
-    SFMM_CUDA(cudaMemcpyAsync(&v, pl.i8->err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SFMM_CUDA(cudaMemcpyAsync(&v, pl.wait_err.ptr, sizeof(int), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
     if (v) {
-        SFMM_CUDA(cudaMemsetAsync(pl.i8->err.ptr, 0, sizeof(int), st));
-        throw Error(FMM_ERR_TIMEOUT, "tensor-core M2L: a pipeline wait expired");
+        SFMM_CUDA(cudaMemsetAsync(pl.wait_err.ptr, 0, sizeof(int), st));
+        throw Error(FMM_ERR_TIMEOUT, "a pipeline wait of the evaluation expired (tensor-core M2L or near-field copies)");
     }
 }
 

@@ -28,8 +28,42 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
     const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(smem));
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_prev() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+// Bulk (TMA engine) copies of contiguous source runs into a warp's tile,
+// completed on the tile buffer's mbarrier (one arrival per fill plus the
+// bytes in flight).  Waits are bounded: an expired wait records an error that
+// the host reports (FMM_ERR_TIMEOUT).
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+__device__ __forceinline__ void tile_bar_init(uint64_t* bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tile_expect(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.expect_tx.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tile_arrive(uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool tile_wait(uint64_t* bar, uint32_t parity, int* err)
+{
+    for (long it = 0; it < (1L << 22); ++it) {
+        uint32_t ok;
+        asm volatile("{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\nselp.u32 %0, 1, 0, q;\n}\n"
+                     : "=r"(ok)
+                     : "r"(smem_u32(bar)), "r"(parity)
+                     : "memory");
+        if (ok) return true;
+    }
+    if (err) atomicExch(err, 1);
+    return false;
+}
 
 // ---------------------------------------------------------------- work items
 // A coarse leaf beside a dense region can hold most of the points in its
@@ -158,7 +192,7 @@ __device__ __forceinline__ void put_near(const EvalArgs& a, int row, int t0, int
 template<int QD>
 struct P2PSmem {
     static constexpr int tile = kChunk * (32 + (QD > 1 ? 16 : 0));   // double4 (+ double2) per source
-    static constexpr int per_warp = 2 * tile;
+    static constexpr int per_warp = 2 * tile + 16;                    // two tiles, their two mbarriers
     static constexpr int total = kWarps * per_warp;
 };
 
@@ -187,9 +221,12 @@ struct RangeWalk {
     template<int QD>
     __device__ __forceinline__ int fill_tile(const int2* __restrict__ nr, const double4* __restrict__ src4,
                                              const double2* __restrict__ src2, double4* t4, double2* t2, int lane,
-                                             int t0, int t1, int& self_s0, int& self_j0, int& self_len)
+                                             int t0, int t1, int& self_s0, int& self_j0, int& self_len, uint64_t* bar)
     {
         int fill = 0;
+        // the buffer was last read by this warp's generic loads (ordered by the
+        // caller's __syncwarp); order those before the bulk copies' writes
+        if (lane == 0) asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         self_s0 = 0;
         self_j0 = 0;
         self_len = 0;
@@ -202,11 +239,12 @@ struct RangeWalk {
             const int ry = __shfl_sync(0xffffffffu, mine.y, ri - base);
             const int j0 = rx + roff;
             const int len = min(min(ry - j0, kChunk - fill), rem);
-            const char* g4 = reinterpret_cast<const char*>(src4 + j0);
-            char* d4 = reinterpret_cast<char*>(t4 + fill);
-            for (int c = lane; c < 2 * len; c += 32) cp_async16(d4 + 16 * c, g4 + 16 * c);
-            if (QD > 1)
-                for (int c = lane; c < len; c += 32) cp_async16(t2 + fill + c, src2 + j0 + c);
+            if (lane == 0) {
+                // one bulk copy per run: len packed 32-byte records (and their 16-byte extra charges)
+                tile_expect(bar, uint32_t(len) * (QD > 1 ? 48u : 32u));
+                bulk_copy(t4 + fill, src4 + j0, uint32_t(len) * 32u, bar);
+                if (QD > 1) bulk_copy(t2 + fill, src2 + j0, uint32_t(len) * 16u, bar);
+            }
             if (j0 < t1 && j0 + len > t0) {
                 self_s0 = fill;
                 self_j0 = j0;
@@ -220,7 +258,7 @@ struct RangeWalk {
                 roff = 0;
             }
         }
-        cp_async_commit();
+        if (lane == 0) tile_arrive(bar);
         return fill;
     }
 };
@@ -240,6 +278,15 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
         t4[b] = reinterpret_cast<double4*>(mine + b * P2PSmem<QD>::tile);
         t2[b] = reinterpret_cast<double2*>(mine + b * P2PSmem<QD>::tile + kChunk * 32);
     }
+    uint64_t* bars = reinterpret_cast<uint64_t*>(mine + 2 * P2PSmem<QD>::tile);
+    if (lane == 0) {
+        tile_bar_init(bars);
+        tile_bar_init(bars + 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    uint32_t par = 0;                                   // bit b: parity of the next wait on tile buffer b
+    bool broken = false;                                // a wait expired: stop (the host reports it)
 
     for (int it = next_item(a.p2p_ctr, lane); it < a.p2p_items; it = next_item(a.p2p_ctr, lane)) {
         const int4 item = a.p2p_item[it];
@@ -258,7 +305,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
             RangeWalk wk;
             wk.start(a.nr, item, r1, lane);
             int cs0, cj0, clen;
-            int fill = wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[0], t2[0], lane, t0, t1, cs0, cj0, clen);
+            int fill = wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[0], t2[0], lane, t0, t1, cs0, cj0, clen, bars);
             double xi[kMaxPass], yi[kMaxPass], zi[kMaxPass];
             int ii[kMaxPass];
             double acc[kMaxPass][NO > 0 ? NO : 1];
@@ -275,12 +322,19 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                 for (int o = 0; o < NO; ++o) acc[p][o] = 0;
             }
             int buf = 0;
-            while (fill > 0) {
+            for (;;) {
+                // every fill of a buffer (the last one is empty) is waited for once
+                const bool got = tile_wait(bars + buf, (par >> buf) & 1u, a.wait_err);
+                if (!__all_sync(0xffffffffu, got)) {
+                    broken = true;
+                    tile_wait(bars + (buf ^ 1), (par >> (buf ^ 1)) & 1u, nullptr);   // a copy of the other buffer in flight
+                    break;
+                }
+                par ^= 1u << buf;
+                if (fill == 0) break;
                 int ns0, nj0, nlen;
-                const int nfill =
-                    wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[buf ^ 1], t2[buf ^ 1], lane, t0, t1, ns0, nj0, nlen);
-                cp_async_wait_prev();
-                __syncwarp();
+                const int nfill = wk.fill_tile<QD>(a.nr, a.src4, a.src2, t4[buf ^ 1], t2[buf ^ 1], lane, t0, t1, ns0, nj0,
+                                                   nlen, bars + (buf ^ 1));
                 // slot of the lane's own target in this tile, if it is here
                 int ks[kMaxPass];
 #pragma unroll
@@ -330,6 +384,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                 cj0 = nj0;
                 clen = nlen;
             }
+            if (broken) break;
             // sum the slices of each target (consecutive lanes)
 #pragma unroll
             for (int p = 0; p < kMaxPass; ++p)
@@ -348,6 +403,7 @@ __global__ void __launch_bounds__(kWarps * 32, MINB) k_p2p(EvalArgs a)
                 }
             }
         }
+        if (broken) break;
     }
 }
 
