@@ -217,9 +217,10 @@ int fmm_plan_replay(fmm_plan* plan);
    it (its own fitted root cube, max_particles_per_node = leaf); the trees are
    merged into one forest, the points of each scaled into the unit cube by
    its own box, and evaluated at once: the persistent near-field and M2L
-   kernels take the work of all sets.  The evaluation runs as a CUDA graph
-   that the context keeps per launch shape and updates in place for the next
-   batch of that shape.  pot (n x qdim) / field (n x 3) are accumulated like
+   kernels take the work of all sets.  A batch of two or more sets runs its
+   evaluation as a CUDA graph that the context keeps per launch shape and
+   updates in place for the next batch of that shape (a set alone launches
+   directly).  pot (n x qdim) / field (n x 3) are accumulated like
    fmm_evaluate's; all items of a batch pass pot (or all NULL) and field (or
    all NULL).  Each set's result is the same as that set solved by a batch of
    one (bit for bit in FP64); against fmm_evaluate of the set's own tree it

@@ -521,7 +521,7 @@ static void evaluate_graph(sfmm::Plan& pl, const double* Q, double* pot, double*
                 placed = true;
             }
         if (!placed) {
-            if (c.batch_graphs.size() >= 16) {           // a few shapes are live at a time
+            if (c.batch_graphs.size() >= 64) {           // a few dozen shapes are live at a time
                 cudaGraphExecDestroy(c.batch_graphs.front().second);
                 c.batch_graphs.erase(c.batch_graphs.begin());
             }
@@ -617,7 +617,10 @@ int fmm_solve_batch(fmm_context* ctx, const fmm_batch_item* items, int count, in
             dfield.alloc(size_t(N) * 3, st);
             SFMM_CUDA(cudaMemsetAsync(dfield.ptr, 0, dfield.bytes(), st));
         }
-        evaluate_graph(pl, dq.ptr, dpot.ptr, dfield.ptr);
+        // a batch of several sets runs through the context's graph of its launch
+        // shape; a set alone launches directly (the same kernels, one use)
+        if (count > 1) evaluate_graph(pl, dq.ptr, dpot.ptr, dfield.ptr);
+        else sfmm::plan_evaluate(pl, dq.ptr, dpot.ptr, dfield.ptr);
         if (want_pot) SFMM_CUDA(cudaMemcpyAsync(hq.data(), dpot.ptr, size_t(N) * qdim * sizeof(double), cudaMemcpyDeviceToHost, st));
         if (want_field) {
             hx.resize(size_t(3) * N);
