@@ -433,6 +433,7 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=400_000, help="cpu_baseline leg: points of its bounded sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision form beside the FP64 step")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark instead of the solve benchmark")
     ap.add_argument("--shard", action="store_true",
@@ -479,7 +480,7 @@ def main():
     live = []
     sharded = args.shard and world > 1
 
-    def step():
+    def step(precision=None):
         # one evaluation as a time-stepping caller runs it: release the
         # previous step's tree and plan, build the tree, set up, evaluate
         while live:
@@ -487,7 +488,7 @@ def main():
         pot_d.zero_()
         fld_d.zero_()
         tree = sf.Tree(pos_d, 20, args.leaf, ctx=ctx)
-        plan = sf.Plan(tree, p, 1, precision=args.precision)
+        plan = sf.Plan(tree, p, 1, precision=precision or args.precision)
         if sharded:
             plan.set_shard(rank, world)
             plan.evaluate_sharded(q_d, pot_d, fld_d, allreduce=dist.all_reduce)
@@ -537,6 +538,7 @@ def main():
     err_fld = float(np.linalg.norm(fld_h[tg] - dfld) / np.linalg.norm(dfld))
 
     stats = tree.stats()
+    depth = tree.depth
     m2l_avg = statistics.mean(m2l_ms)
     pairs = stats["ilist_pairs"]
     useful = pairs * m2l_useful_flops(p)                # per launch
@@ -610,6 +612,41 @@ def main():
                "h2d_bytes_per_step": int(pos_p.nbytes + q_p.nbytes + pot_p.nbytes + fld_p.nbytes),
                "d2h_bytes_per_step": int(pot_p.nbytes + fld_p.nbytes)}
 
+    # the mixed-precision form on the same workload, in the same run: the same
+    # step (tree, plan, evaluation), timed the same way, checked against the
+    # same direct-sum targets
+    mixed = None
+    if args.precision == "fp64" and world == 1 and not args.no_mixed:
+        for _ in range(args.warmup):
+            step("mixed")
+            flush.zero_()
+        torch.cuda.synchronize()
+        mt = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s_.record(stream)
+            _, mplan = step("mixed")
+            e_.record(stream)
+            e_.synchronize()
+            mt.append(s_.elapsed_time(e_))
+        mtm = mplan.timings()
+        mpot, mfld = pot_d.cpu().numpy(), fld_d.cpu().numpy()
+        m_ms = sum(mt) / len(mt)
+        mixed = {"value": n / (m_ms * 1e-3), "unit": "points/s", "ms_per_step": m_ms,
+                 "speedup_vs_fp64": (total_ms / args.steps) / m_ms,
+                 "rel_error_vs_direct": {"potential": float(np.linalg.norm(mpot[tg] - dpot) / np.linalg.norm(dpot)),
+                                         "field": float(np.linalg.norm(mfld[tg] - dfld) / np.linalg.norm(dfld)),
+                                         "targets": n_check},
+                 "rel_l2_vs_fp64_path": {"potential": float(np.linalg.norm(mpot - pot_h) / np.linalg.norm(pot_h)),
+                                         "field": float(np.linalg.norm(mfld - fld_h) / np.linalg.norm(fld_h))},
+                 "m2l_ms": mtm["m2l_ms"], "p2p_ms": mtm["p2p_ms"],
+                 "dtype": "f32 near field; M2L in int8 slices on the tensor cores (32-bit fixed point, exact int32 sums); "
+                          "f64 moments, locals and sums"}
+        while live:
+            live.pop().close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         vals, info = cpu_baseline(args.dist, n, args.cpu_sample, p, leaf=args.leaf)
@@ -625,7 +662,7 @@ def main():
                 "f64 moments, locals and sums"),
             "data": DATA_DESC.get(args.dist, f"synthetic (seeded {args.dist})"),
             "config": workload_config(args, n, world),
-            "tree": {"depth": tree.depth, **stats},
+            "tree": {"depth": depth, **stats},
             "rel_error_vs_direct": {"potential": err_pot, "field": err_fld, "targets": n_check},
             "phases_ms": {k: round(statistics.mean(ph[k] for ph in phases), 3) for k in phases[0]},
             "step_ms": [round(x, 3) for x in times],
@@ -651,6 +688,7 @@ def main():
             "clocks": clk.summary(),
             "e2e": e2e,
             "gpu_launches": int(launches),
+            "mixed": mixed,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)

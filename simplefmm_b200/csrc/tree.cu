@@ -532,6 +532,15 @@ T read_one(const T* d, cudaStream_t s)
     return v;
 }
 
+// Two device values read back with one synchronisation.
+template<typename T>
+void read_two(const T* d0, const T* d1, T& v0, T& v1, cudaStream_t s)
+{
+    SFMM_CUDA(cudaMemcpyAsync(&v0, d0, sizeof(T), cudaMemcpyDeviceToHost, s));
+    SFMM_CUDA(cudaMemcpyAsync(&v1, d1, sizeof(T), cudaMemcpyDeviceToHost, s));
+    SFMM_CUDA(cudaStreamSynchronize(s));
+}
+
 }  // namespace
 
 void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vertical_axis, double phideg,
@@ -673,8 +682,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         split_base.alloc(S + 1, st);
         exclusive_scan_i32(nch.ptr, child_base.ptr, S, st);
         exclusive_scan_i32(nsp.ptr, split_base.ptr, S, st);
-        const int NC = read_one(child_base.ptr + S, st);
-        const int NS = read_one(split_base.ptr + S, st);
+        int NC = 0, NS = 0;
+        read_two(child_base.ptr + S, split_base.ptr + S, NC, NS, st);
         grow_nodes(total + NC, total);
         sp_next.alloc(std::max(NS, 1), st);
         k_children<<<blocks_for(S, 256), 256, 0, st>>>(sp.ptr, S, total, child_base.ptr, split_base.ptr, cnt.ptr, offs.ptr,
