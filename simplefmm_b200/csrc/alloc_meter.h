@@ -24,6 +24,10 @@ struct AllocMeter {
 };
 
 void set_thread_alloc_meters(AllocMeter* request, AllocMeter* server) noexcept;
+// The calling thread's meters and cache setting (a helper thread that works
+// for a request takes them over).
+void get_thread_alloc_meters(AllocMeter** request, AllocMeter** server) noexcept;
+bool thread_block_cache() noexcept;
 
 // While off for a thread, the device blocks it releases go straight back to
 // the memory pool instead of the block cache, so a server holds no device

@@ -4,8 +4,11 @@
 #include <atomic>
 #include <memory>
 #include <cstring>
+#include <exception>
 #include <new>
 #include <string>
+#include <thread>
+#include <vector>
 
 #include "fmm_eval.cuh"
 
@@ -570,21 +573,81 @@ int fmm_solve_batch(fmm_context* ctx, const fmm_batch_item* items, int count, in
     dq.alloc(size_t(N) * qdim, st);
     SFMM_CUDA(cudaMemcpyAsync(dx.ptr, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     SFMM_CUDA(cudaMemcpyAsync(dq.ptr, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, st));
-    // member trees, each as a single solve builds it
-    std::vector<std::unique_ptr<sfmm::Tree>> trees;
-    std::vector<const sfmm::Tree*> members;
-    for (int r = 0; r < count; ++r) {
-        trees.emplace_back(new sfmm::Tree);
-        sfmm::Tree& t = *trees.back();
-        t.ctx = &c;
-        t.n = items[r].n;
-        sfmm::build_tree(t, dx.ptr + 3 * base[r], max_level, items[r].leaf, 2, 0.0);
-        members.push_back(&t);
-    }
+    // member trees, each as a single solve builds it.  A build waits on the
+    // host for its level sizes, so several members are built at once: worker
+    // threads, each on a stream of its own, take every kBuilders-th member.
+    constexpr int kBuilders = 4;
+    const int nb = std::min(count, kBuilders);
+    std::vector<std::unique_ptr<sfmm::Tree>> trees(count);
+    std::vector<sfmm::Context> wc(nb);
     sfmm::Tree F;
-    sfmm::build_forest(F, members);
+    cudaEvent_t uploaded = nullptr;
+    SFMM_CUDA(cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming));
+    SFMM_CUDA(cudaEventRecord(uploaded, st));
+    for (int w = 0; w < nb; ++w) {
+        wc[w].device = c.device;
+        wc[w].sm_count = c.sm_count;
+        if (nb == 1) {
+            wc[w].stream = st;
+        } else {
+            SFMM_CUDA(cudaStreamCreateWithFlags(&wc[w].stream, cudaStreamNonBlocking));
+            SFMM_CUDA(cudaStreamWaitEvent(wc[w].stream, uploaded, 0));
+        }
+    }
+    auto destroy_streams = [&] {
+        if (nb > 1)
+            for (auto& x : wc)
+                if (x.stream) {
+                    cudaStreamSynchronize(x.stream);
+                    cudaStreamDestroy(x.stream);
+                    x.stream = nullptr;
+                }
+        cudaEventDestroy(uploaded);
+    };
+    try {
+        sfmm::AllocMeter *meter_req = nullptr, *meter_srv = nullptr;
+        sfmm::get_thread_alloc_meters(&meter_req, &meter_srv);
+        const bool cache = sfmm::thread_block_cache();
+        std::vector<std::exception_ptr> fault(nb);
+        auto build = [&](int w) {
+            try {
+                SFMM_CUDA(cudaSetDevice(c.device));
+                sfmm::set_thread_alloc_meters(meter_req, meter_srv);
+                sfmm::set_thread_block_cache(cache);
+                for (int r = w; r < count; r += nb) {
+                    trees[r].reset(new sfmm::Tree);
+                    sfmm::Tree& t = *trees[r];
+                    t.ctx = &wc[w];
+                    t.n = items[r].n;
+                    sfmm::build_tree(t, dx.ptr + 3 * base[r], max_level, items[r].leaf, 2, 0.0);
+                }
+                SFMM_CUDA(cudaStreamSynchronize(wc[w].stream));
+            } catch (...) {
+                fault[w] = std::current_exception();
+            }
+        };
+        if (nb == 1) {
+            build(0);
+        } else {
+            std::vector<std::thread> th;
+            for (int w = 0; w < nb; ++w) th.emplace_back(build, w);
+            for (auto& x : th) x.join();
+        }
+        for (auto& f : fault)
+            if (f) std::rethrow_exception(f);
+        std::vector<const sfmm::Tree*> members;
+        for (auto& t : trees) {
+            t->ctx = &c;                                 // the forest is built on the batch's stream
+            members.push_back(t.get());
+        }
+        sfmm::build_forest(F, members);
+    } catch (...) {
+        trees.clear();
+        destroy_streams();
+        throw;
+    }
     trees.clear();
-    members.clear();
+    destroy_streams();
     {
         sfmm::Plan pl;
         // the plan's events, destroyed when the batch is done (after the sync below)

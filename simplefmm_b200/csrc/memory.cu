@@ -101,6 +101,14 @@ void set_thread_alloc_meters(AllocMeter* request, AllocMeter* server) noexcept
 
 void set_thread_block_cache(bool on) noexcept { tl_cache_on = on; }
 
+void get_thread_alloc_meters(AllocMeter** request, AllocMeter** server) noexcept
+{
+    *request = tl_meter_request;
+    *server = tl_meter_server;
+}
+
+bool thread_block_cache() noexcept { return tl_cache_on; }
+
 void* device_alloc(size_t bytes, int device, cudaStream_t s)
 {
     SFMM_REQUIRE(device >= 0 && device < 64, FMM_ERR_INVALID_ARGUMENT, "device index out of range");
