@@ -228,8 +228,12 @@ struct Tree {
 
     float build_ms = 0;
     // device time of the build's phases: keys, refinement, leaves and points,
-    // colleagues, interaction lists, near-field lists
+    // colleagues, interaction lists, near-field lists.  The single-launch
+    // refinement also numbers the leaves and fills the colleague lists: its
+    // phase then holds them, "leaves and points" only the point gather, and
+    // "colleagues" nothing.
     float phase_ms[6] = {};
+    bool single_refine = false;
 
     // a forest of independent trees (forest.cu): the member of each node; empty
     // for a single tree

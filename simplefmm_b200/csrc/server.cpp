@@ -95,7 +95,9 @@ size_t estimate_bytes(int64_t n, int p, int qdim, int leaf, int precision)
 {
     const double T = (p + 1) * (p + 2) / 2.0, T1 = (p + 2) * (p + 3) / 2.0;
     const double nodes = std::max<double>(64.0, 2.5 * double(n) / std::max(leaf, 8));
-    const double per_point = 48 + 48 + 48 + 8.0 * (qdim + 3) * 3;     // points (two frames), sort scratch, I/O
+    // points (two frames), sort scratch, I/O; colleague lists and leaf ids
+    // are first allocated for n / 8 nodes (15 B per point)
+    const double per_point = 48 + 48 + 48 + 8.0 * (qdim + 3) * 3 + 16;
     double per_node = 16.0 * qdim * (2 * T + T1) + 190 * 8 + 64;         // M, LA, LB, ilist, node arrays
     // mixed plans' tensor-core M2L (m2l_i8.cu): slot table, block lists and
     // four digits of the padded real moments per node

@@ -17,6 +17,8 @@
 // buffer and points of new leaves straight to the final order.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 
 #include "fmm_internal.cuh"
 
@@ -514,6 +516,493 @@ __global__ void k_nlist(int level, LevelTabs L, const uint64_t* __restrict__ key
     if (!kFill) count_or_ptr[f] = pos;
 }
 
+// ------------------------------------------------------------------ single-launch refinement
+// The refinement above, the colleague lists and the leaf numbering in ONE
+// cooperative launch (every block resident at once), the steps separated by
+// grid barriers instead of kernel boundaries and host reads of counts.  Per
+// level (S splitting nodes in `sp`, T tiles of at most kWTile points):
+//   A  colleagues of the level's nodes; tile counts of the splitting nodes,
+//      one partial sum per block over its contiguous range of nodes
+//   B  tile offsets (each block adds up the partials before its range); T
+//   C  digit histogram of every tile (a warp per tile, tiles in contiguous
+//      ranges per block), the block's per-digit totals, and per-node digit
+//      counts by integer atomics (exact whatever the order)
+//   D  per-digit exclusive prefixes over the tiles (the [digit][tile] scan of
+//      the level path, row by row); child counts per node, block totals
+//   E  child numbering, the children's node fields, and the stable scatter:
+//      a warp takes a tile's points in index order, 32 at a time, and places
+//      each after the earlier points of its digit (match + 8 ballots)
+// and after the last level the leaf numbering (two steps).  The partition,
+// node numbering and lists are the level path's, bit for bit.
+//
+// A level that needs more node slots than allocated ends the launch at its
+// start with kRefGrow; the host grows the node arrays and launches again from
+// that level.  Each barrier wait is bounded (%globaltimer, about two seconds,
+// and an iteration cap); a wait that runs out sets an abort flag that every
+// other waiting block sees, and the launch ends with kRefTimeout.
+constexpr int kRefThreads = 256;
+constexpr int kRefWarps = kRefThreads / 32;
+constexpr int kWTile = 1024;                  // points per tile (one warp)
+constexpr int kParts = 12;                    // partial sums per block
+constexpr unsigned long long kBarrierNs = 2000000000ull;
+
+enum { kRefDone = 0, kRefGrow = 1, kRefTimeout = 2, kRefOverflow = 3 };
+
+struct RefineState {
+    unsigned bar_count;
+    unsigned bar_gen;
+    int abort;
+    int status;
+    int level;                       // level whose splitting nodes come next
+    int S;                           // their number
+    int cur;                         // which sp / point buffers hold them
+    int need;                        // children of that level (kRefGrow)
+    long long total;                 // nodes so far
+    long long lvl_off[kKeyLevel + 3];
+    int leaf_off[kKeyLevel + 3];
+};
+
+struct RefineArgs {
+    uint64_t* key;
+    int32_t *pbeg, *pend, *parent, *child_beg, *nchild, *col, *leaf_id, *leaf_node;
+    long long cap;
+    uint64_t* pkey[2];
+    int32_t* pord[2];
+    int32_t* final_ord;
+    int32_t* sp[2];
+    int32_t *tile_off, *hist, *pre, *ncnt, *offs, *nch, *nsp, *part;
+    int smax, tmax;
+    int max_level, ppn;
+    RefineState* st;
+};
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ void st_release_u32(unsigned* p, unsigned v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid barrier (sense by generation).  Returns false when this block must
+// leave: its wait ran out or another block's did.
+__device__ bool grid_barrier(RefineState* st)
+{
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile int* abort = &st->abort;
+        if (*abort) {
+            ok = 0;
+        } else {
+            const unsigned gen = ld_acquire_u32(&st->bar_gen);
+            __threadfence();
+            if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+                atomicExch(&st->bar_count, 0u);
+                __threadfence();
+                st_release_u32(&st->bar_gen, gen + 1);
+            } else {
+                const unsigned long long t0 = global_ns();
+                unsigned spins = 0;
+                while (ld_acquire_u32(&st->bar_gen) == gen) {
+                    if (*abort || ++spins > (1u << 25) || global_ns() - t0 > kBarrierNs) {
+                        atomicExch(&st->abort, 1);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// Exclusive sum over the block of one value per thread; *tot = block total.
+__device__ int block_excl(int v, int* tot, int* sh)
+{
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int y = lane < kRefWarps ? sh[lane] : 0;
+#pragma unroll
+        for (int o = 1; o < kRefWarps; o <<= 1) {
+            const int z = __shfl_up_sync(0xffffffffu, y, o);
+            if (lane >= o) y += z;
+        }
+        if (lane < kRefWarps) sh[lane] = y;
+    }
+    __syncthreads();
+    const int before = (w ? sh[w - 1] : 0) + x - v;
+    *tot = sh[kRefWarps - 1];
+    __syncthreads();
+    return before;
+}
+
+__device__ int block_sum(int v, int* sh)
+{
+    int tot;
+    block_excl(v, &tot, sh);
+    return tot;
+}
+
+// Field f of the per-block partials: the sum over blocks before this one and
+// over all blocks.
+__device__ void parts_sums(const int32_t* part, int f, int* before, int* all, int* sh)
+{
+    int x = 0, y = 0;
+    for (int k = threadIdx.x; k < static_cast<int>(gridDim.x); k += blockDim.x) {
+        const int v = part[k * kParts + f];
+        y += v;
+        if (k < static_cast<int>(blockIdx.x)) x += v;
+    }
+    *before = block_sum(x, sh);
+    *all = block_sum(y, sh);
+}
+
+__device__ __forceinline__ int tile_count(const RefineArgs& a, const int32_t* sp, int s)
+{
+    const int g = sp[s];
+    return (a.pend[g] - a.pbeg[g] + kWTile - 1) / kWTile;
+}
+
+// first tile of the warp: binary search; later (larger) tiles: walk on
+__device__ __forceinline__ int seg_of(const int32_t* tile_off, int S, int t, int s)
+{
+    if (s < 0) return find_seg(tile_off, S, t);
+    while (s + 1 < S && tile_off[s + 1] <= t) ++s;
+    return s;
+}
+
+__global__ void __launch_bounds__(kRefThreads) k_refine(RefineArgs a)
+{
+    __shared__ int sh[kRefWarps];
+    __shared__ int s_dig[8];
+    __shared__ long long s_lvl[kKeyLevel + 3];
+    RefineState* st = a.st;
+    const int G = gridDim.x, b = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t gthreads = int64_t(G) * kRefThreads, gtid = int64_t(b) * kRefThreads + tid;
+    int level = st->level, S = st->S, cur = st->cur;
+    int64_t lo = st->lvl_off[level], total = st->total;
+    int status = kRefDone, need = 0;
+
+    for (;;) {
+        const int32_t* sp = cur ? a.sp[1] : a.sp[0];
+        int32_t* spn = cur ? a.sp[0] : a.sp[1];
+        const uint64_t* kin = cur ? a.pkey[1] : a.pkey[0];
+        uint64_t* kout = cur ? a.pkey[0] : a.pkey[1];
+        const int32_t* oin = cur ? a.pord[1] : a.pord[0];
+        int32_t* oout = cur ? a.pord[0] : a.pord[1];
+        const int child_may_split = (level + 1) < a.max_level;
+
+        // ---- A: colleagues of this level; tile counts
+        for (int64_t g = lo + gtid; g < total; g += gthreads) {
+            int32_t* my = a.col + 27 * g;
+            for (int s = 0; s < 27; ++s) my[s] = -1;
+            if (level == 0) {
+                my[13] = static_cast<int32_t>(g);
+                continue;
+            }
+            const I3 me = key_ijk(a.key[g]);
+            const int32_t* pc = a.col + 27 * int64_t(a.parent[g]);
+            for (int ps = 0; ps < 27; ++ps) {
+                const int P = pc[ps];
+                if (P < 0) continue;
+                const int cb = a.child_beg[P], nc = a.nchild[P];
+                for (int c = cb; c < cb + nc; ++c) {
+                    const I3 o = key_ijk(a.key[c]);
+                    const int dx = o.x - me.x, dy = o.y - me.y, dz = o.z - me.z;
+                    if (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1) my[slot_of(dx, dy, dz)] = c;
+                }
+            }
+        }
+        if (S == 0) break;
+        const int cs = (S + G - 1) / G, s0 = min(S, b * cs), s1 = min(S, s0 + cs);
+        {
+            int mine = 0;
+            for (int s = s0 + tid; s < s1; s += kRefThreads) {
+                mine += tile_count(a, sp, s);
+#pragma unroll
+                for (int d = 0; d < 8; ++d) a.ncnt[8 * s + d] = 0;
+            }
+            const int tot = block_sum(mine, sh);
+            if (tid == 0) a.part[b * kParts] = tot;
+        }
+        if (!grid_barrier(st)) return;
+
+        // ---- B: tile offsets
+        int T;
+        {
+            int before;
+            parts_sums(a.part, 0, &before, &T, sh);
+            if (T > a.tmax) {
+                status = kRefOverflow;
+                break;
+            }
+            int carry = before;
+            for (int base = s0; base < s1; base += kRefThreads) {
+                const int s = base + tid;
+                const int v = s < s1 ? tile_count(a, sp, s) : 0;
+                int tot;
+                const int ex = block_excl(v, &tot, sh);
+                if (s < s1) a.tile_off[s] = carry + ex;
+                carry += tot;
+            }
+        }
+        if (!grid_barrier(st)) return;
+
+        // ---- C: digit histograms
+        const int shift = 3 * (kKeyLevel - 1 - level);
+        const int ct = (T + G - 1) / G, t0 = min(T, b * ct), t1 = min(T, t0 + ct);
+        if (tid < 8) s_dig[tid] = 0;
+        __syncthreads();
+        {
+            int s = -1;
+            for (int t = t0 + warp; t < t1; t += kRefWarps) {
+                s = seg_of(a.tile_off, S, t, s);
+                const int g = sp[s];
+                const int pb = a.pbeg[g] + (t - a.tile_off[s]) * kWTile;
+                const int pe = min(a.pend[g], pb + kWTile);
+                int c = 0;                                   // lane d < 8: points of digit d
+                for (int i0 = pb; i0 < pe; i0 += 128) {
+                    int dg[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int i = i0 + 32 * u + lane;
+                        dg[u] = i < pe ? static_cast<int>((kin[i] >> shift) & 7) : 8;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u)
+#pragma unroll
+                        for (int d = 0; d < 8; ++d) {
+                            const unsigned m = __ballot_sync(0xffffffffu, dg[u] == d);
+                            if (lane == d) c += __popc(m);
+                        }
+                }
+                if (lane < 8) {
+                    a.hist[int64_t(lane) * T + t] = c;
+                    if (c) {
+                        atomicAdd(&a.ncnt[8 * s + lane], c);
+                        atomicAdd(&s_dig[lane], c);
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (tid < 8) a.part[b * kParts + 1 + tid] = s_dig[tid];
+        if (!grid_barrier(st)) return;
+
+        // ---- D: per-digit tile prefixes (warp d); node statistics
+        {
+            const int d = warp;                               // 8 warps, one per digit
+            int base = 0;
+            for (int k = lane; k < b; k += 32) base += a.part[k * kParts + 1 + d];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) base += __shfl_xor_sync(0xffffffffu, base, o);
+            for (int t = t0; t < t1; t += 32) {
+                const int tt = t + lane;
+                const int v = tt < t1 ? a.hist[int64_t(d) * T + tt] : 0;
+                int x = v;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int y = __shfl_up_sync(0xffffffffu, x, o);
+                    if (lane >= o) x += y;
+                }
+                if (tt < t1) a.pre[int64_t(d) * T + tt] = base + x - v;
+                base += __shfl_sync(0xffffffffu, x, 31);
+            }
+        }
+        {
+            int mc = 0, ms = 0;
+            for (int s = s0 + tid; s < s1; s += kRefThreads) {
+                int off = 0, nc = 0, ns = 0;
+#pragma unroll
+                for (int d = 0; d < 8; ++d) {
+                    const int c = a.ncnt[8 * s + d];
+                    a.offs[8 * s + d] = off;
+                    off += c;
+                    nc += c > 0;
+                    ns += (c > a.ppn && child_may_split);
+                }
+                a.nch[s] = nc;
+                a.nsp[s] = ns;
+                mc += nc;
+                ms += ns;
+            }
+            mc = block_sum(mc, sh);
+            ms = block_sum(ms, sh);
+            if (tid == 0) {
+                a.part[b * kParts + 9] = mc;
+                a.part[b * kParts + 10] = ms;
+            }
+        }
+        if (!grid_barrier(st)) return;
+
+        // ---- E: children and the scatter
+        int NC, NS;
+        {
+            int cbefore, sbefore;
+            parts_sums(a.part, 9, &cbefore, &NC, sh);
+            parts_sums(a.part, 10, &sbefore, &NS, sh);
+            if (total + NC > a.cap) {
+                status = kRefGrow;
+                need = NC;
+                break;
+            }
+            if (NS > a.smax) {
+                status = kRefOverflow;
+                break;
+            }
+            int cc = cbefore, sc = sbefore;
+            for (int base = s0; base < s1; base += kRefThreads) {
+                const int s = base + tid;
+                const int nc = s < s1 ? a.nch[s] : 0, ns = s < s1 ? a.nsp[s] : 0;
+                int tc, ts;
+                const int exc = block_excl(nc, &tc, sh);
+                const int exs = block_excl(ns, &ts, sh);
+                if (s < s1) {
+                    const int g = sp[s];
+                    const uint64_t k = a.key[g];
+                    const int cb = static_cast<int>(total) + cc + exc;
+                    int r = 0, rs = sc + exs;
+                    for (int d = 0; d < 8; ++d) {
+                        const int c = a.ncnt[8 * s + d];
+                        if (!c) continue;
+                        const int h = cb + r++;
+                        a.key[h] = (k << 3) | uint64_t(d);
+                        a.pbeg[h] = a.pbeg[g] + a.offs[8 * s + d];
+                        a.pend[h] = a.pbeg[h] + c;
+                        a.parent[h] = g;
+                        a.child_beg[h] = -1;
+                        a.nchild[h] = 0;
+                        if (c > a.ppn && child_may_split) spn[rs++] = h;
+                    }
+                    a.child_beg[g] = cb;
+                    a.nchild[g] = r;
+                }
+                cc += tc;
+                sc += ts;
+            }
+        }
+        {
+            int s = -1;
+            for (int t = t0 + warp; t < t1; t += kRefWarps) {
+                s = seg_of(a.tile_off, S, t, s);
+                const int g = sp[s];
+                const int f = a.tile_off[s];
+                const int pb = a.pbeg[g] + (t - f) * kWTile;
+                const int pe = min(a.pend[g], pb + kWTile);
+                int pos_d = 0, split_d = 0;                   // lane d < 8: next slot of digit d
+                if (lane < 8) {
+                    pos_d = a.pbeg[g] + a.offs[8 * s + lane] + (a.pre[int64_t(lane) * T + t] - a.pre[int64_t(lane) * T + f]);
+                    split_d = a.ncnt[8 * s + lane] > a.ppn && child_may_split;
+                }
+                const unsigned splits = __ballot_sync(0xffffffffu, split_d);
+                for (int i0 = pb; i0 < pe; i0 += 128) {
+                    uint64_t kk[4];
+                    int oo[4];
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int i = i0 + 32 * u + lane;
+                        kk[u] = i < pe ? kin[i] : 0;
+                        oo[u] = i < pe ? oin[i] : 0;
+                    }
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const bool valid = i0 + 32 * u + lane < pe;
+                        const int dg = valid ? static_cast<int>((kk[u] >> shift) & 7) : 8;
+                        const unsigned peers = __match_any_sync(0xffffffffu, dg);
+                        const int pos = __shfl_sync(0xffffffffu, pos_d, dg & 7) + __popc(peers & lt);
+                        if (valid) {
+                            if ((splits >> dg) & 1u) {
+                                kout[pos] = kk[u];
+                                oout[pos] = oo[u];
+                            } else {
+                                a.final_ord[pos] = oo[u];
+                            }
+                        }
+#pragma unroll
+                        for (int d = 0; d < 8; ++d) {
+                            const unsigned m = __ballot_sync(0xffffffffu, dg == d);
+                            if (lane == d) pos_d += __popc(m);
+                        }
+                    }
+                }
+            }
+        }
+        if (b == 0 && tid == 0) st->lvl_off[level + 2] = total + NC;
+        if (!grid_barrier(st)) return;
+        lo = total;
+        total += NC;
+        ++level;
+        S = NS;
+        cur ^= 1;
+    }
+
+    if (status == kRefDone) {
+        // ---- leaves in node order: ids, nodes, first leaf of every level
+        const int64_t cn = (total + G - 1) / G, n0 = total < b * cn ? total : b * cn, n1 = total < n0 + cn ? total : n0 + cn;
+        {
+            int mine = 0;
+            for (int64_t g = n0 + tid; g < n1; g += kRefThreads) mine += a.nchild[g] == 0;
+            const int tot = block_sum(mine, sh);
+            if (tid == 0) a.part[b * kParts + 11] = tot;
+        }
+        if (!grid_barrier(st)) return;
+        int before, nleaves;
+        parts_sums(a.part, 11, &before, &nleaves, sh);
+        if (tid <= level + 1) s_lvl[tid] = reinterpret_cast<volatile long long*>(st->lvl_off)[tid];
+        __syncthreads();
+        int carry = before;
+        for (int64_t base = n0; base < n1; base += kRefThreads) {
+            const int64_t g = base + tid;
+            const int leaf = g < n1 && a.nchild[g] == 0;
+            int tot;
+            const int id = carry + block_excl(leaf, &tot, sh);
+            if (g < n1) {
+                a.leaf_id[g] = leaf ? id : -1;
+                if (leaf) a.leaf_node[id] = static_cast<int32_t>(g);
+                for (int l = 0; l <= level; ++l)
+                    if (s_lvl[l] == g) st->leaf_off[l] = id;
+            }
+            carry += tot;
+        }
+        if (b == 0 && tid == 0) st->leaf_off[level + 1] = nleaves;
+    }
+    if (b == 0 && tid == 0) {
+        st->status = status;
+        st->level = level;
+        st->S = S;
+        st->cur = cur;
+        st->need = need;
+        st->total = total;
+    }
+}
+
 template<typename T>
 std::vector<T> to_host(const T* d, size_t n, cudaStream_t s)
 {
@@ -539,6 +1028,20 @@ void read_two(const T* d0, const T* d1, T& v0, T& v1, cudaStream_t s)
     SFMM_CUDA(cudaMemcpyAsync(&v0, d0, sizeof(T), cudaMemcpyDeviceToHost, s));
     SFMM_CUDA(cudaMemcpyAsync(&v1, d1, sizeof(T), cudaMemcpyDeviceToHost, s));
     SFMM_CUDA(cudaStreamSynchronize(s));
+}
+
+// The single-launch refinement unless SFMM_TREE_REFINE=levels asks for the
+// level-by-level launches (the tests run both), the device cannot launch
+// cooperatively, or the tile table would not fit 32-bit counts.
+bool single_launch_refinement(int64_t n, int ppn)
+{
+    const char* m = std::getenv("SFMM_TREE_REFINE");
+    if (m && std::strcmp(m, "levels") == 0) return false;
+    int dev = 0, coop = 0;
+    SFMM_CUDA(cudaGetDevice(&dev));
+    SFMM_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev));
+    const int64_t smax = std::max<int64_t>(1, n / (int64_t(ppn) + 1));
+    return coop && 8 * (n / kWTile + smax + 1) < (int64_t(1) << 31);
 }
 
 }  // namespace
@@ -656,6 +1159,101 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     }
 
     int level = 0;
+    const bool single = single_launch_refinement(n, max_ppn);
+    if (single) {
+        // one cooperative launch: all levels, the colleague lists, the leaves
+        const int64_t smax = std::max<int64_t>(1, n / (int64_t(max_ppn) + 1));
+        const int64_t tmax = n / kWTile + smax + 1;
+        int dev = 0, sms = 0, occ = 0;
+        SFMM_CUDA(cudaGetDevice(&dev));
+        SFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine, kRefThreads, 0));
+        SFMM_REQUIRE(occ > 0, FMM_ERR_UNSUPPORTED, "the refinement kernel cannot be resident");
+        const int G = static_cast<int>(std::min<int64_t>(int64_t(occ) * sms, std::max<int64_t>(1, (n + 2 * kWTile - 1) / (2 * kWTile))));
+        DevBuf<int32_t> sp0, sp1, tile_off, hist, pre, ncnt, offs, nch, nsp, part;
+        DevBuf<RefineState> dst;
+        sp0.alloc(smax, st);
+        sp1.alloc(smax, st);
+        tile_off.alloc(smax, st);
+        ncnt.alloc(8 * smax, st);
+        offs.alloc(8 * smax, st);
+        nch.alloc(smax, st);
+        nsp.alloc(smax, st);
+        hist.alloc(8 * tmax, st);
+        pre.alloc(8 * tmax, st);
+        part.alloc(size_t(kParts) * G, st);
+        dst.alloc(1, st);
+        if (S) {
+            const int32_t z = 0;
+            SFMM_CUDA(cudaMemcpyAsync(sp0.ptr, &z, 4, cudaMemcpyHostToDevice, st));
+        }
+        t.colleague.alloc(27 * cap, st);
+        t.leaf_id.alloc(cap, st);
+        t.leaf_node.alloc(cap, st);
+        RefineState h{};
+        h.S = S;
+        h.total = 1;
+        h.lvl_off[1] = 1;
+        for (;;) {
+            RefineArgs ra{};
+            ra.key = t.key.ptr;
+            ra.pbeg = t.pbeg.ptr;
+            ra.pend = t.pend.ptr;
+            ra.parent = t.parent.ptr;
+            ra.child_beg = t.child_beg.ptr;
+            ra.nchild = t.nchild.ptr;
+            ra.col = t.colleague.ptr;
+            ra.leaf_id = t.leaf_id.ptr;
+            ra.leaf_node = t.leaf_node.ptr;
+            ra.cap = static_cast<long long>(cap);
+            ra.pkey[0] = keyA.ptr;
+            ra.pkey[1] = keyB.ptr;
+            ra.pord[0] = ordA.ptr;
+            ra.pord[1] = ordB.ptr;
+            ra.final_ord = t.order.ptr;
+            ra.sp[0] = sp0.ptr;
+            ra.sp[1] = sp1.ptr;
+            ra.tile_off = tile_off.ptr;
+            ra.hist = hist.ptr;
+            ra.pre = pre.ptr;
+            ra.ncnt = ncnt.ptr;
+            ra.offs = offs.ptr;
+            ra.nch = nch.ptr;
+            ra.nsp = nsp.ptr;
+            ra.part = part.ptr;
+            ra.smax = static_cast<int>(smax);
+            ra.tmax = static_cast<int>(tmax);
+            ra.max_level = max_level;
+            ra.ppn = max_ppn;
+            ra.st = dst.ptr;
+            SFMM_CUDA(cudaMemcpyAsync(dst.ptr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+            void* params[] = {&ra};
+            SFMM_CUDA(cudaLaunchCooperativeKernel(reinterpret_cast<const void*>(k_refine), dim3(G), dim3(kRefThreads),
+                                                  params, 0, st));
+            SFMM_CHECK_LAUNCH();
+            SFMM_CUDA(cudaMemcpyAsync(&h, dst.ptr, sizeof(h), cudaMemcpyDeviceToHost, st));
+            SFMM_CUDA(cudaStreamSynchronize(st));
+            if (h.abort) throw Error(FMM_ERR_TIMEOUT, "the tree refinement gave up waiting at a grid barrier");
+            if (h.status == kRefGrow) {
+                // more node slots: keep the nodes so far and their colleagues
+                const int64_t keep = h.total;
+                grow_nodes(keep + h.need, keep);
+                t.colleague.grow(27 * cap, 27 * keep, st);
+                t.leaf_id.alloc(cap, st);
+                t.leaf_node.alloc(cap, st);
+                h.status = kRefDone;
+                continue;
+            }
+            SFMM_REQUIRE(h.status == kRefDone, FMM_ERR_UNSUPPORTED, "tree refinement: work exceeded its bounds");
+            break;
+        }
+        level = h.level;
+        total = h.total;
+        t.lvl_off.assign(h.lvl_off, h.lvl_off + level + 2);
+        t.leaf_off.assign(h.leaf_off, h.leaf_off + level + 2);
+        t.n_leaves = h.leaf_off[level + 1];
+        S = 0;
+    }
     DevBuf<int32_t> ntile, tile_off, hist, pre, cnt, offs, nch, nsp, child_base, split_base;
     while (S > 0) {
         const int child_may_split = (level + 1) < max_level;
@@ -704,10 +1302,11 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     }
     t.depth = level;
     t.n_nodes = total;
+    t.single_refine = single;
     SFMM_CUDA(cudaEventRecord(ev.e[2], st));
 
     // --- leaves (per level in key order: the reference's _i_leaf)
-    {
+    if (!single) {
         DevBuf<int32_t> flag, scan;
         flag.alloc(total, st);
         scan.alloc(total + 1, st);
@@ -745,8 +1344,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
     SFMM_CUDA(cudaEventRecord(ev.e[3], st));
 
     // --- colleagues, level by level
-    t.colleague.alloc(27 * total, st);
-    for (int l = 0; l <= t.depth; ++l) {
+    if (!single) t.colleague.alloc(27 * total, st);
+    for (int l = 0; !single && l <= t.depth; ++l) {
         const int64_t c = t.lvl_off[l + 1] - t.lvl_off[l];
         k_colleagues<<<blocks_for(c, 128), 128, 0, st>>>(t.lvl_off[l], c, l, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
                                                           t.nchild.ptr, t.colleague.ptr);
@@ -827,6 +1426,8 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
 //   leaves      points gathered into leaf order: read 24 B + 4 B index, write 24 B
 //               (twice when the frame is rotated); leaf ids 16 B per node
 //   colleagues  27 int32 per node written, parent/child fields read (12 B)
+//               (the single-launch refinement counts leaf ids and colleagues
+//               in its own phase)
 //   ilist       both passes read the 27 colleagues and 16 B of node fields per
 //               node; the entries (src, code) are written once, 8 B each
 //   near lists  both passes read the 27 colleagues per leaf's node; the ranges
@@ -841,10 +1442,11 @@ void tree_phase_bytes(const Tree& t, double* bytes6)
     for (int64_t g = 0; g < t.n_nodes; ++g)
         if (nch[g] > 0) active += double(pe[g] - pb[g]);
     const double n = double(t.n), nodes = double(t.n_nodes), L = double(t.n_leaves);
+    const double leaf_b = 16.0 * nodes, col_b = (27.0 * 4 + 12.0) * nodes;
     bytes6[0] = 60.0 * n;
-    bytes6[1] = 32.0 * active + 4.0 * n;
-    bytes6[2] = (t.box.rotated ? 76.0 : 52.0) * n + 16.0 * nodes;
-    bytes6[3] = (27.0 * 4 + 12.0) * nodes;
+    bytes6[1] = 32.0 * active + 4.0 * n + (t.single_refine ? leaf_b + col_b : 0.0);
+    bytes6[2] = (t.box.rotated ? 76.0 : 52.0) * n + (t.single_refine ? 0.0 : leaf_b);
+    bytes6[3] = t.single_refine ? 0.0 : col_b;
     bytes6[4] = 2 * (27.0 * 4 + 16.0) * nodes + 8.0 * double(t.il_nnz) + 4.0 * nodes;
     bytes6[5] = 2 * 27.0 * 4 * L + 8.0 * double(t.nr_nnz) + 4.0 * L;
 }

@@ -343,3 +343,46 @@ def test_direct_m2l_equals_rotation_on_a_medium_case(ctx):
     sp, sfl = pyoracle.error_scales(pos, q, tg)
     assert rel_err_per_target(pot_d[tg], pot_r[tg], sp) < TOL
     assert rel_err_per_target(fld_d[tg], fld_r[tg], sfl) < TOL
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_tree_bit_exact_level_launches(monkeypatch, ctx, name):
+    """The level-by-level refinement (a launch chain per level; what runs
+    where a cooperative launch is not available) forced by its test switch:
+    the reference's trees bit for bit, like the single-launch default."""
+    monkeypatch.setenv("SFMM_TREE_REFINE", "levels")
+    g = load_golden(name)
+    t = golden_tree(sf, g, ctx)
+    d = t.dump()
+    assert t.depth == int(g["DEPTH"][0])
+    if "CNODE0" not in g:
+        return
+    for k in tree_keys(g):
+        assert np.array_equal(d[k], g[k]), k
+
+
+@pytest.mark.parametrize("dist,n,ppn,max_level", [("uniform", 20000, 4, 20), ("plummer", 60000, 1, 20),
+                                                  ("gauss2", 30000, 16, 20), ("shell", 40000, 8, 5),
+                                                  ("plummer", 5000, 0, 7), ("uniform", 3000, 5000, 20)])
+def test_single_launch_refinement_equals_level_launches(monkeypatch, ctx, dist, n, ppn, max_level):
+    """The single cooperative launch (node slots grown between launches when
+    the first allocation is short: the first four cases need more than n/8
+    nodes) gives the level-by-level tree and lists bit for bit, and the same
+    potentials."""
+    pos = W.points(dist, n, 5)
+    q = W.charges(n, 5)
+    out = []
+    for mode in (None, "levels"):
+        if mode:
+            monkeypatch.setenv("SFMM_TREE_REFINE", mode)
+        t = sf.Tree(pos, max_level, ppn, ctx=ctx)
+        d = t.dump()
+        pot, fld = np.zeros(n), np.zeros((n, 3))
+        sf.Plan(t, 6, 1).evaluate(q, pot, fld)
+        out.append((t.depth, d, pot, fld))
+    (da, a, pa, fa), (db, b, pb, fb) = out
+    assert da == db
+    assert a.keys() == b.keys()
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
+    assert np.array_equal(pa, pb) and np.array_equal(fa, fb)
