@@ -377,35 +377,64 @@ __device__ inline int sorted_parent_colleagues(const int32_t* __restrict__ pc, i
 }
 
 // partition.hpp:283-297 / tree.hpp:122-174: children of the parent's
-// neighbours that exist and are not adjacent; dijk = source - target.
+// neighbours that exist and are not adjacent; dijk = source - target.  A warp
+// per node: lane a holds the parent's a-th neighbour in node order (= key
+// order, so the children come out in the row order CSRP::finish gives,
+// csr.hpp:48-56); the candidates (neighbour, child) are taken 32 at a time in
+// that order and the kept ones written contiguously (ballot + prefix).
 template<bool kFill>
 __global__ void k_ilist(int64_t off, int64_t cnt, const uint64_t* __restrict__ key, const int32_t* __restrict__ parent,
                         const int32_t* __restrict__ child_beg, const int32_t* __restrict__ nchild,
                         const int32_t* __restrict__ col, int32_t* __restrict__ count_or_ptr,
                         int32_t* __restrict__ src, int32_t* __restrict__ code)
 {
-    const int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (i >= cnt) return;
-    const int64_t g = off + i;
-    const I3 me = key_ijk(key[g]);
-    int ps[27];
-    const int m = sorted_parent_colleagues(col + 27 * int64_t(parent[g]), ps);
-    int pos = kFill ? count_or_ptr[g] : 0;
-    for (int a = 0; a < m; ++a) {
-        const int P = ps[a];
-        const int cb = child_beg[P], nc = nchild[P];
-        for (int c = cb; c < cb + nc; ++c) {
-            const I3 o = key_ijk(key[c]);
-            const int dx = o.x - me.x, dy = o.y - me.y, dz = o.z - me.z;
-            if (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1) continue;
-            if (kFill) {
-                src[pos] = c;
-                code[pos] = (dx + 3) | ((dy + 3) << 3) | ((dz + 3) << 6);
-            }
-            ++pos;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t i = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; i < cnt; i += nw) {
+        const int64_t g = off + i;
+        const I3 me = key_ijk(key[g]);
+        const int v = lane < 27 ? col[27 * int64_t(parent[g]) + lane] : -1;
+        int rank = 0;                                  // neighbours are distinct nodes
+        for (int j = 0; j < 27; ++j) {
+            const int u = __shfl_sync(full, v, j);
+            rank += u >= 0 && u < v;
         }
+        int P = -1;                                    // the lane-th neighbour in node order
+        for (int j = 0; j < 27; ++j) {
+            const int u = __shfl_sync(full, v, j), r = __shfl_sync(full, rank, j);
+            if (u >= 0 && r == lane) P = u;
+        }
+        const int m = __popc(__ballot_sync(full, v >= 0));
+        int cb = 0, nc = 0;
+        if (lane < m) {
+            cb = child_beg[P];
+            nc = nchild[P];
+        }
+        int pos = kFill ? count_or_ptr[g] : 0;
+        for (int j0 = 0; j0 < 8 * m; j0 += 32) {
+            const int j = j0 + lane, a = (j >> 3) & 31, ci = j & 7;
+            const int cbj = __shfl_sync(full, cb, a), ncj = __shfl_sync(full, nc, a);
+            bool take = false;
+            int c = 0, cd = 0;
+            if ((j >> 3) < m && ci < ncj) {
+                c = cbj + ci;
+                const I3 o = key_ijk(key[c]);
+                const int dx = o.x - me.x, dy = o.y - me.y, dz = o.z - me.z;
+                take = abs(dx) > 1 || abs(dy) > 1 || abs(dz) > 1;
+                cd = (dx + 3) | ((dy + 3) << 3) | ((dz + 3) << 6);
+            }
+            const unsigned tm = __ballot_sync(full, take);
+            if (kFill && take) {
+                const int r = pos + __popc(tm & lt);
+                src[r] = c;
+                code[r] = cd;
+            }
+            pos += __popc(tm);
+        }
+        if (!kFill && lane == 0) count_or_ptr[g] = pos;
     }
-    if (!kFill) count_or_ptr[g] = pos;
 }
 
 // Near-field source point ranges of one leaf: the point sets of its _nlist
@@ -615,14 +644,15 @@ __device__ bool grid_barrier(RefineState* st)
                 st_release_u32(&st->bar_gen, gen + 1);
             } else {
                 const unsigned long long t0 = global_ns();
-                unsigned spins = 0;
+                unsigned spins = 0, nap = 32;
                 while (ld_acquire_u32(&st->bar_gen) == gen) {
                     if (*abort || ++spins > (1u << 25) || global_ns() - t0 > kBarrierNs) {
                         atomicExch(&st->abort, 1);
                         ok = 0;
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(nap);
+                    if (nap < 256) nap *= 2;
                 }
             }
             __threadfence();
@@ -719,26 +749,29 @@ __global__ void __launch_bounds__(kRefThreads) k_refine(RefineArgs a)
         int32_t* oout = cur ? a.pord[0] : a.pord[1];
         const int child_may_split = (level + 1) < a.max_level;
 
-        // ---- A: colleagues of this level; tile counts
-        for (int64_t g = lo + gtid; g < total; g += gthreads) {
+        // ---- A: colleagues of this level (a warp per node, a lane per
+        //      neighbour of the parent); tile counts
+        for (int64_t g = lo + (gtid >> 5); g < total; g += gthreads >> 5) {
             int32_t* my = a.col + 27 * g;
-            for (int s = 0; s < 27; ++s) my[s] = -1;
-            if (level == 0) {
-                my[13] = static_cast<int32_t>(g);
-                continue;
-            }
+            if (lane < 27) my[lane] = (level == 0 && lane == 13) ? static_cast<int32_t>(g) : -1;
+            if (level == 0) continue;
+            __syncwarp();
             const I3 me = key_ijk(a.key[g]);
-            const int32_t* pc = a.col + 27 * int64_t(a.parent[g]);
-            for (int ps = 0; ps < 27; ++ps) {
-                const int P = pc[ps];
-                if (P < 0) continue;
+            const int P = lane < 27 ? a.col[27 * int64_t(a.parent[g]) + lane] : -1;
+            if (P >= 0) {
                 const int cb = a.child_beg[P], nc = a.nchild[P];
-                for (int c = cb; c < cb + nc; ++c) {
-                    const I3 o = key_ijk(a.key[c]);
+                uint64_t kc[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) kc[j] = j < nc ? a.key[cb + j] : 0;
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (j >= nc) break;
+                    const I3 o = key_ijk(kc[j]);
                     const int dx = o.x - me.x, dy = o.y - me.y, dz = o.z - me.z;
-                    if (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1) my[slot_of(dx, dy, dz)] = c;
+                    if (abs(dx) <= 1 && abs(dy) <= 1 && abs(dz) <= 1) my[slot_of(dx, dy, dz)] = cb + j;
                 }
             }
+            __syncwarp();
         }
         if (S == 0) break;
         const int cs = (S + G - 1) / G, s0 = min(S, b * cs), s1 = min(S, s0 + cs);
@@ -1363,7 +1396,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         // node's list depends only on its parent's colleagues
         const int64_t i0 = t.depth >= 2 ? t.lvl_off[2] : total, ic = total - i0;
         if (ic > 0) {
-            k_ilist<false><<<blocks_for(ic, 128), 128, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
+            k_ilist<false><<<blocks_for(32 * ic, 256, 16384), 256, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
                                                                 t.nchild.ptr, t.colleague.ptr, icnt.ptr, nullptr, nullptr);
             SFMM_CHECK_LAUNCH();
         }
@@ -1376,7 +1409,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         t.il_src.alloc(std::max<int64_t>(t.il_nnz, 1), st);
         t.il_code.alloc(std::max<int64_t>(t.il_nnz, 1), st);
         if (ic > 0) {
-            k_ilist<true><<<blocks_for(ic, 128), 128, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
+            k_ilist<true><<<blocks_for(32 * ic, 256, 16384), 256, 0, st>>>(i0, ic, t.key.ptr, t.parent.ptr, t.child_beg.ptr,
                                                                t.nchild.ptr, t.colleague.ptr, t.il_ptr.ptr, t.il_src.ptr,
                                                                t.il_code.ptr);
             SFMM_CHECK_LAUNCH();
