@@ -137,8 +137,11 @@ int fmm_tree_stats(const fmm_tree* tree, int64_t* stats5);
    by level), [2] leaves and points in leaf order, [3] same-level neighbours,
    [4] interaction lists, [5] near-field lists -- and, if bytes6 is not NULL,
    the device-memory bytes each phase must move at least once (its
-   algorithmic traffic), for achieved-bandwidth figures.  No counterpart in
-   the reference (its tree build is timed as one step). */
+   algorithmic traffic), for achieved-bandwidth figures.  The refinement runs
+   as one cooperative launch that also numbers the leaves and fills the
+   neighbour lists: [1] then holds that work, [2] only the point gather and
+   [3] nothing (0 bytes).  No counterpart in the reference (its tree build is
+   timed as one step). */
 int fmm_tree_build_phases(const fmm_tree* tree, double* ms6, double* bytes6);
 
 /* FMM3D<double, qdim, p, Vector, support_gradient>(partitioner, comm):

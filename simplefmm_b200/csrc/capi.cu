@@ -574,8 +574,9 @@ int fmm_solve_batch(fmm_context* ctx, const fmm_batch_item* items, int count, in
     SFMM_CUDA(cudaMemcpyAsync(dx.ptr, hx.data(), hx.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     SFMM_CUDA(cudaMemcpyAsync(dq.ptr, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     // member trees, each as a single solve builds it.  A build waits on the
-    // host for its level sizes, so several members are built at once: worker
-    // threads, each on a stream of its own, take every kBuilders-th member.
+    // host four times (the cube, the refinement's totals, the two list
+    // sizes), so several members are built at once: worker threads, each on a
+    // stream of its own, take every kBuilders-th member.
     constexpr int kBuilders = 4;
     const int nb = std::min(count, kBuilders);
     std::vector<std::unique_ptr<sfmm::Tree>> trees(count);

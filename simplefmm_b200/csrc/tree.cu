@@ -15,6 +15,12 @@
 // per-node child counts, then a stable scatter (warp match + inter-warp
 // prefix) that writes points of still-splitting children to the next work
 // buffer and points of new leaves straight to the final order.
+//
+// By default every level, the colleague lists and the leaf numbering run in
+// ONE cooperative launch (k_refine) whose steps are separated by grid
+// barriers; the per-level launch chain (k_ntiles ... k_scatter, k_colleagues,
+// k_leafflag / k_leafids) is the fallback for devices without cooperative
+// launch, and both give the same tree bit for bit.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -439,44 +445,50 @@ __global__ void k_ilist(int64_t off, int64_t cnt, const uint64_t* __restrict__ k
 
 // Near-field source point ranges of one leaf: the point sets of its _nlist
 // row (partition.hpp:343-366) -- leaves among every ancestor's neighbours,
-// and the whole subtree of every same-level neighbour (self included).
+// and the whole subtree of every same-level neighbour (self included).  A
+// warp per leaf, a lane per neighbour slot: ranges are kept in slot order,
+// ancestors from the parent up, then the leaf's own neighbours.
 template<bool kFill>
 __global__ void k_near(int64_t n_leaves, const int32_t* __restrict__ leaf_node, const int32_t* __restrict__ parent,
                        const int32_t* __restrict__ nchild, const int32_t* __restrict__ pbeg,
                        const int32_t* __restrict__ pend, const int32_t* __restrict__ col,
                        int32_t* __restrict__ count_or_ptr, int2* __restrict__ ranges, unsigned long long* __restrict__ pairs)
 {
-    const int64_t f = blockIdx.x * int64_t(blockDim.x) + threadIdx.x;
-    if (f >= n_leaves) return;
-    const int g = leaf_node[f];
-    int pos = kFill ? count_or_ptr[f] : 0;
-    long long npts = 0;
-    int a = parent[g];
-    while (a >= 0) {
-        const int32_t* ac = col + 27 * int64_t(a);
-        for (int s = 0; s < 27; ++s) {
-            const int c = ac[s];
-            if (c >= 0 && nchild[c] == 0) {
-                if (kFill) ranges[pos] = make_int2(pbeg[c], pend[c]);
-                npts += pend[c] - pbeg[c];
-                ++pos;
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t nw = (int64_t(gridDim.x) * blockDim.x) >> 5;
+    for (int64_t f = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; f < n_leaves; f += nw) {
+        const int g = leaf_node[f];
+        int pos = kFill ? count_or_ptr[f] : 0;
+        long long npts = 0;
+        // ancestors (take their leaf neighbours), then the leaf itself (all)
+        for (int a = parent[g], self = 0; a >= 0 || !self;) {
+            const int node = a >= 0 ? a : g;
+            const int c = lane < 27 ? col[27 * int64_t(node) + lane] : -1;
+            int b = 0, e = 0;
+            bool take = false;
+            if (c >= 0) {
+                b = pbeg[c];
+                e = pend[c];
+                take = a < 0 || nchild[c] == 0;
+            }
+            const unsigned tm = __ballot_sync(full, take);
+            if (kFill && take) ranges[pos + __popc(tm & lt)] = make_int2(b, e);
+            if (take) npts += e - b;
+            pos += __popc(tm);
+            if (a >= 0) a = parent[a];
+            else self = 1;
+        }
+        if (!kFill) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) npts += __shfl_xor_sync(full, npts, o);
+            if (lane == 0) {
+                count_or_ptr[f] = pos;
+                const long long t = pend[g] - pbeg[g];
+                atomicAdd(pairs, static_cast<unsigned long long>(t * npts - t));
             }
         }
-        a = parent[a];
-    }
-    const int32_t* gc = col + 27 * int64_t(g);
-    for (int s = 0; s < 27; ++s) {
-        const int c = gc[s];
-        if (c >= 0) {
-            if (kFill) ranges[pos] = make_int2(pbeg[c], pend[c]);
-            npts += pend[c] - pbeg[c];
-            ++pos;
-        }
-    }
-    if (!kFill) {
-        count_or_ptr[f] = pos;
-        const long long t = pend[g] - pbeg[g];
-        atomicAdd(pairs, static_cast<unsigned long long>(t * npts - t));
     }
 }
 
@@ -1202,7 +1214,9 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         SFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
         SFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_refine, kRefThreads, 0));
         SFMM_REQUIRE(occ > 0, FMM_ERR_UNSUPPORTED, "the refinement kernel cannot be resident");
-        const int G = static_cast<int>(std::min<int64_t>(int64_t(occ) * sms, std::max<int64_t>(1, (n + 2 * kWTile - 1) / (2 * kWTile))));
+        // two root tiles per block, at least 32 blocks (small trees: the colleague
+        // and list steps are chains of dependent loads, one warp per node)
+        const int G = static_cast<int>(std::min<int64_t>(int64_t(occ) * sms, std::max<int64_t>(32, (n + 2 * kWTile - 1) / (2 * kWTile))));
         DevBuf<int32_t> sp0, sp1, tile_off, hist, pre, ncnt, offs, nch, nsp, part;
         DevBuf<RefineState> dst;
         sp0.alloc(smax, st);
@@ -1426,7 +1440,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         ncnt.alloc(L, st);
         pairs.alloc(1, st);
         SFMM_CUDA(cudaMemsetAsync(pairs.ptr, 0, 8, st));
-        k_near<false><<<blocks_for(L, 128), 128, 0, st>>>(L, t.leaf_node.ptr, t.parent.ptr, t.nchild.ptr, t.pbeg.ptr,
+        k_near<false><<<blocks_for(32 * L, 256, 16384), 256, 0, st>>>(L, t.leaf_node.ptr, t.parent.ptr, t.nchild.ptr, t.pbeg.ptr,
                                                            t.pend.ptr, t.colleague.ptr, ncnt.ptr, nullptr, pairs.ptr);
         SFMM_CHECK_LAUNCH();
         t.nr_ptr.alloc(L + 1, st);
@@ -1437,7 +1451,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         require_i32_total(t.nr_nnz, "the near-field range list");
         t.near_pairs = static_cast<int64_t>(read_one(pairs.ptr, st));
         t.nr.alloc(std::max<int64_t>(t.nr_nnz, 1), st);
-        k_near<true><<<blocks_for(L, 128), 128, 0, st>>>(L, t.leaf_node.ptr, t.parent.ptr, t.nchild.ptr, t.pbeg.ptr,
+        k_near<true><<<blocks_for(32 * L, 256, 16384), 256, 0, st>>>(L, t.leaf_node.ptr, t.parent.ptr, t.nchild.ptr, t.pbeg.ptr,
                                                           t.pend.ptr, t.colleague.ptr, t.nr_ptr.ptr, t.nr.ptr, nullptr);
         SFMM_CHECK_LAUNCH();
     }
