@@ -342,6 +342,7 @@ static std::shared_ptr<PlanTables> tables_on_device(int device, int p, bool mixe
     upload(t->l2l1_code, tb1->l2l_code, st);
     upload(t->l2l1_g, tb1->l2l_g, st);
     build_m2l_fragments(*t, p, mixed, st);
+    build_unit_shift_ops(*t, p, st);
     SFMM_CUDA(cudaStreamSynchronize(st));         // other streams read it from now on
     slot = t;
     return t;

@@ -113,6 +113,7 @@ struct PlanTables {
     int rfrag_nf = 0;
     DevBuf<float> rf32, tz32, tzl32;
     int rf32_nf = 0, tz32_nf = 0;
+    DevBuf<double> sh_unit;                 // M2M / L2L maps at rho = 1 (shift.cu)
 };
 
 // Direct-M2L tables of one order on one device (shared like PlanTables).
@@ -178,6 +179,7 @@ struct Plan {
 void plan_init(Plan& pl);
 // shift.cu: set-up at plan creation, M2M into parent level lp, L2L into
 // children level lc, and the context's cuBLAS handle at context teardown
+void build_unit_shift_ops(PlanTables& tab, int p, cudaStream_t st);
 void shift_setup(Plan& pl);
 void shift_m2m(Plan& pl, const EvalArgs& a, int lp, cudaStream_t st);
 void shift_l2l(Plan& pl, const EvalArgs& a, int lc, cudaStream_t st);

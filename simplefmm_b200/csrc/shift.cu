@@ -308,10 +308,76 @@ __global__ void __launch_bounds__(32 * kShiftWarps) k_l2l_mma(L2LSide sa, L2LSid
 unsigned grid_for(int64_t n, int sms) { return static_cast<unsigned>(std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, int64_t(sms) * 16))); }
 
 // fragment counts of one level's maps
-int64_t m2m_frags(int R) { return int64_t(8) * cdiv(R, 8) * cdiv(R, 4); }
-int64_t l2l_frags(int R) { return int64_t(R) * cdiv(R, 4); }
+__host__ __device__ int64_t m2m_frags(int R) { return int64_t(8) * cdiv(R, 8) * cdiv(R, 4); }
+__host__ __device__ int64_t l2l_frags(int R) { return int64_t(R) * cdiv(R, 4); }
+
+// rho of each children level 3 .. depth (index l - 3)
+struct LevelRho {
+    double rho[kKeyLevel];
+};
+
+// A level's maps from the maps at rho = 1: every M2M / L2L term of output
+// order n(out) and input order n(in) carries rho^|n(out) - n(in)|, so entry
+// (out, in) is the unit entry times that power (the power taken as the same
+// running product the term sums use).  Zero and padding entries stay zero.
+__global__ void k_shift_scale(const double* __restrict__ unit, int64_t per_level, int nlev, LevelRho r, int RA, int RB,
+                              double* __restrict__ out)
+{
+    const int64_t fm = m2m_frags(RA), fla = l2l_frags(RA);
+    const int64_t total = per_level * nlev;
+    for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < total; i += int64_t(gridDim.x) * blockDim.x) {
+        const int lv = static_cast<int>(i / per_level);
+        const int64_t e = i - int64_t(lv) * per_level;
+        double v = unit[e];
+        if (v != 0.0) {
+            int64_t f = e >> 5;
+            const int lr = static_cast<int>(e & 31) >> 2, lc = static_cast<int>(e & 3);
+            int row, col;
+            if (f < fm) {                                   // OpM: ((oct * RT + rt) * KC + kc)
+                const int KC = cdiv(RA, 4), RT = cdiv(RA, 8);
+                const int kc = static_cast<int>(f % KC), rt = static_cast<int>((f / KC) % RT);
+                row = 8 * rt + lr;
+                col = 4 * kc + lc;
+            } else {                                        // OpL: (rt * KC + kc), rows oct * R + i
+                const bool la = f < fm + fla;
+                const int R = la ? RA : RB, KC = cdiv(R, 4);
+                f -= la ? fm : fm + fla;
+                row = (8 * static_cast<int>(f / KC) + lr) % R;
+                col = 4 * static_cast<int>(f % KC) + lc;
+            }
+            const int pw = abs(tri_order(row >> 1) - tri_order(col >> 1));
+            double s = 1.0;
+            for (int q = 0; q < pw; ++q) s *= r.rho[lv];
+            v *= s;
+        }
+        out[i] = v;
+    }
+}
 
 }  // namespace
+
+// The shift maps at rho = 1 for order p (OpM, OpLA, OpLB in the fragment
+// order of one level), built once per (device, p) with the term sums.
+void build_unit_shift_ops(PlanTables& tab, int p, cudaStream_t st)
+{
+    const int T = (p + 1) * (p + 2) / 2, T1 = (p + 2) * (p + 3) / 2, RA = 2 * T, RB = 2 * T1;
+    const int64_t per_level = (m2m_frags(RA) + l2l_frags(RA) + l2l_frags(RB)) * 32;
+    tab.sh_unit.alloc(per_level, st);
+    SFMM_CUDA(cudaMemsetAsync(tab.sh_unit.ptr, 0, size_t(per_level) * sizeof(double), st));
+    double* op = tab.sh_unit.ptr;
+    const size_t shm = (32 + 2 * (T1 + 1)) * sizeof(double);
+    k_shift_ops<true><<<8 * RA, 128, shm, st>>>(tab.m2m_ptr.ptr, tab.m2m_code.ptr, tab.m2m_g.ptr,
+                                                reinterpret_cast<const cplx*>(tab.echild.ptr), p, 1.0, op);
+    SFMM_CHECK_LAUNCH();
+    k_shift_ops<false><<<8 * RA, 128, shm, st>>>(tab.l2l_ptr.ptr, tab.l2l_code.ptr, tab.l2l_g.ptr,
+                                                 reinterpret_cast<const cplx*>(tab.eparent.ptr), p, 1.0,
+                                                 op + m2m_frags(RA) * 32);
+    SFMM_CHECK_LAUNCH();
+    k_shift_ops<false><<<8 * RB, 128, shm, st>>>(tab.l2l1_ptr.ptr, tab.l2l1_code.ptr, tab.l2l1_g.ptr,
+                                                 reinterpret_cast<const cplx*>(tab.eparent1.ptr), p + 1, 1.0,
+                                                 op + (m2m_frags(RA) + l2l_frags(RA)) * 32);
+    SFMM_CHECK_LAUNCH();
+}
 
 void shift_setup(Plan& pl)
 {
@@ -320,7 +386,7 @@ void shift_setup(Plan& pl)
     if (t.depth < 3) return;
     Context& c = *t.ctx;
     cudaStream_t st = c.stream;
-    const int p = pl.p, RA = 2 * pl.T, RB = 2 * pl.T1;
+    const int RA = 2 * pl.T, RB = 2 * pl.T1;
     // parents of levels 2 .. depth - 1 with children: compact slots
     const int64_t base = t.lvl_off[2], n = t.lvl_off[t.depth] - base;
     DevBuf<int32_t> flag;
@@ -341,26 +407,16 @@ void shift_setup(Plan& pl)
     SFMM_CUDA(cudaMemcpyAsync(pl.sh_S.data(), S.ptr, (t.depth + 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     SFMM_CUDA(cudaStreamSynchronize(st));
     // maps per children level 3 .. depth, fragment order: OpM (RA x 8RA),
-    // OpLA (8RA x RA), OpLB (8RB x RB); zero padding rows / columns
+    // OpLA (8RA x RA), OpLB (8RB x RB); zero padding rows / columns; each
+    // the order's maps at rho = 1 scaled to the level's rho
     const int64_t per_level = (m2m_frags(RA) + l2l_frags(RA) + l2l_frags(RB)) * 32;
-    pl.sh_ops.alloc(size_t(per_level) * (t.depth - 2), st);
-    SFMM_CUDA(cudaMemsetAsync(pl.sh_ops.ptr, 0, size_t(per_level) * (t.depth - 2) * sizeof(double), st));
-    for (int l = 3; l <= t.depth; ++l) {
-        double* op = pl.sh_ops.ptr + per_level * (l - 3);
-        const double rho = std::sqrt(0.75) * t.box.width / double(1 << l);
-        const size_t shm = (32 + 2 * (pl.T1 + 1)) * sizeof(double);
-        k_shift_ops<true><<<8 * RA, 128, shm, st>>>(pl.tab->m2m_ptr.ptr, pl.tab->m2m_code.ptr, pl.tab->m2m_g.ptr,
-                                                    reinterpret_cast<const cplx*>(pl.tab->echild.ptr), p, rho, op);
-        SFMM_CHECK_LAUNCH();
-        k_shift_ops<false><<<8 * RA, 128, shm, st>>>(pl.tab->l2l_ptr.ptr, pl.tab->l2l_code.ptr, pl.tab->l2l_g.ptr,
-                                                     reinterpret_cast<const cplx*>(pl.tab->eparent.ptr), p, rho,
-                                                     op + m2m_frags(RA) * 32);
-        SFMM_CHECK_LAUNCH();
-        k_shift_ops<false><<<8 * RB, 128, shm, st>>>(pl.tab->l2l1_ptr.ptr, pl.tab->l2l1_code.ptr, pl.tab->l2l1_g.ptr,
-                                                     reinterpret_cast<const cplx*>(pl.tab->eparent1.ptr), p + 1, rho,
-                                                     op + (m2m_frags(RA) + l2l_frags(RA)) * 32);
-        SFMM_CHECK_LAUNCH();
-    }
+    const int nlev = t.depth - 2;
+    pl.sh_ops.alloc(size_t(per_level) * nlev, st);
+    LevelRho r{};
+    for (int l = 3; l <= t.depth; ++l) r.rho[l - 3] = std::sqrt(0.75) * t.box.width / double(1 << l);
+    k_shift_scale<<<grid_for(per_level * nlev, c.sm_count), 256, 0, st>>>(pl.tab->sh_unit.ptr, per_level, nlev, r, RA,
+                                                                          RB, pl.sh_ops.ptr);
+    SFMM_CHECK_LAUNCH();
     const size_t smem = size_t(8 * kL2LTiles) * shift_ld(4 * cdiv(RB, 4)) * sizeof(double);
     SFMM_REQUIRE(smem + 2 * sizeof(ShiftTile) <= 227 * 1024, FMM_ERR_UNSUPPORTED, "shift operands exceed shared memory");
     allow_max_smem(k_m2m_mma);

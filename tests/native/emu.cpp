@@ -443,3 +443,31 @@ extern "C" int emu_check_term_codes(int p)
     check(tb.l2l_code);
     return bad;
 }
+
+// Every M2M / L2L term of order p carries the rho power |n(out) - n(in)|,
+// the order difference of its output and input coefficients.  The plan
+// set-up relies on it: a level's shift maps are the maps at rho = 1 with
+// entry (out, in) scaled by rho^|n(out) - n(in)|.  Returns the number of
+// terms that break it.
+extern "C" int emu_check_term_powers(int p)
+{
+    const HostTables tb = make_tables(p);
+    auto order = [](int t) {
+        int n = 0;
+        while ((n + 1) * (n + 2) / 2 <= t) ++n;
+        return n;
+    };
+    int bad = 0;
+    auto check = [&](const std::vector<int>& ptr, const std::vector<int>& codes) {
+        for (size_t o = 0; o + 1 < ptr.size(); ++o)
+            for (int e = ptr[o]; e < ptr[o + 1]; ++e) {
+                int pw, q, in;
+                bool cj;
+                unpack_term(codes[e], &pw, &q, &in, &cj);
+                if (pw != std::abs(order(static_cast<int>(o)) - order(in))) ++bad;
+            }
+    };
+    check(tb.m2m_ptr, tb.m2m_code);
+    check(tb.l2l_ptr, tb.l2l_code);
+    return bad;
+}

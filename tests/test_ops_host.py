@@ -130,3 +130,12 @@ def test_shift_term_codes_hold_every_order(emu):
     emu.emu_check_term_codes.restype = C.c_int
     for p in range(0, 18):
         assert emu.emu_check_term_codes(p) == 0, p
+
+
+def test_shift_terms_scale_by_order_difference(emu):
+    """Every M2M / L2L term's rho power is the order difference of its output
+    and input coefficients, for every order the shifts run at: the plan
+    builds each level's shift maps by scaling the maps at rho = 1."""
+    emu.emu_check_term_powers.restype = C.c_int
+    for p in range(0, 18):
+        assert emu.emu_check_term_powers(p) == 0, p
