@@ -318,6 +318,61 @@ def run_reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+def small_solves_bench(args):
+    """Costs of small solves (the serving regime), Plummer points, leaf 64,
+    p = args.p, potential + field, FP64, host arrays: for each size the
+    median over 9 repetitions (after 3) of the wall time of the tree build,
+    the plan set-up and the evaluation, and the device time of the build
+    (fmm_tree_build_phases summed); then the per-solve wall time of a plain
+    solve, a batch of one and a batch of eight copies (fmm_solve_batch)."""
+    import simplefmm_b200 as sf
+    from simplefmm_b200 import workloads as W
+
+    ctx = sf.Context(0)
+    reps, skip = 12, 3
+    single = {}
+    for n in (2000, 10000, 50000, 400000):
+        pos, q = W.points("plummer", n, 3), W.charges(n, 3)
+        rows = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            tree = sf.Tree(pos, 20, LEAF, ctx=ctx)
+            t1 = time.perf_counter()
+            plan = sf.Plan(tree, args.p, 1)
+            t2 = time.perf_counter()
+            plan.evaluate(q, np.zeros(n), np.zeros((n, 3)))
+            t3 = time.perf_counter()
+            ph = tree.build_phases()
+            rows.append(((t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3, sum(v[0] for v in ph.values()), ph))
+            plan.close()
+            tree.close()
+        med = lambda k: round(statistics.median(r[k] for r in rows[skip:]), 4)  # noqa: E731
+        single[n] = {"build_wall_ms": med(0), "plan_wall_ms": med(1), "evaluate_wall_ms": med(2),
+                     "build_device_ms": med(3),
+                     "build_phases_ms": {k: round(statistics.median(r[4][k][0] for r in rows[skip:]), 4)
+                                         for k in rows[0][4]}}
+    batch = {}
+    for n in (2000, 10000, 50000):
+        pos, q = W.points("plummer", n, 3), W.charges(n, 3)
+        res = {}
+        for mode, count in (("plain", 1), ("batch1", 1), ("batch8", 8)):
+            ts = []
+            for _ in range(15):
+                t0 = time.perf_counter()
+                if mode == "plain":
+                    tree = sf.Tree(pos, 20, LEAF, ctx=ctx)
+                    sf.Plan(tree, args.p, 1).evaluate(q, np.zeros(n), np.zeros((n, 3)))
+                    tree.close()
+                else:
+                    sf.solve_batch([(pos, q)] * count, args.p, ctx=ctx)
+                ts.append((time.perf_counter() - t0) * 1e3)
+            res[mode + "_ms_per_solve"] = round(statistics.median(ts[3:]) / count, 4)
+        batch[n] = res
+    print(json.dumps({"metric": "small-solve costs (wall ms, host arrays)", "p": args.p, "leaf": LEAF,
+                      "distribution": "plummer", "single": single, "per_solve": batch,
+                      "batch_graphs": sf.batch_graph_stats(ctx)}), flush=True)
+
+
 def workload_config(args, n: int, world: int) -> dict:
     par = f"shard x{world} (one solve, NCCL all-reduce)" if getattr(args, "shard", False) and world > 1 else f"replicas x{world}"
     leaf = getattr(args, "leaf", LEAF)
@@ -436,6 +491,9 @@ def main():
     ap.add_argument("--no-mixed", action="store_true", help="skip timing the mixed-precision form beside the FP64 step")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--serve", action="store_true", help="serving-stream benchmark instead of the solve benchmark")
+    ap.add_argument("--small", action="store_true",
+                    help="small-solve costs instead of the solve benchmark: tree build, plan set-up and evaluation "
+                         "of single solves, and the per-solve time of batches (fmm_solve_batch)")
     ap.add_argument("--shard", action="store_true",
                     help="with --gpus N > 1: one solve split over the N ranks (fmm_plan_set_shard, NCCL all-reduce of "
                          "moments, locals and outputs; strong scaling) instead of N independent replicas")
@@ -449,6 +507,9 @@ def main():
         return
     if args.serve:
         serve_bench(args)
+        return
+    if args.small:
+        small_solves_bench(args)
         return
 
     import torch
