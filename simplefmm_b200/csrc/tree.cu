@@ -598,6 +598,7 @@ struct RefineState {
     int S;                           // their number
     int cur;                         // which sp / point buffers hold them
     int need;                        // children of that level (kRefGrow)
+    int gate;                        // set by nothing: the wait of the stall test
     long long total;                 // nodes so far
     long long lvl_off[kKeyLevel + 3];
     int leaf_off[kKeyLevel + 3];
@@ -614,6 +615,7 @@ struct RefineArgs {
     int32_t *tile_off, *hist, *pre, *ncnt, *offs, *nch, *nsp, *part;
     int smax, tmax;
     int max_level, ppn;
+    int stall;                       // test switch: block 0 waits on `gate` (never set)
     RefineState* st;
 };
 
@@ -748,6 +750,21 @@ __global__ void __launch_bounds__(kRefThreads) k_refine(RefineArgs a)
     const int lane = tid & 31, warp = tid >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t gthreads = int64_t(G) * kRefThreads, gtid = int64_t(b) * kRefThreads + tid;
+    if (a.stall && b == 0) {
+        // test of the bounded waits: block 0 never reaches the first barrier;
+        // its thread 0 waits on a flag nothing sets, then raises the abort
+        // that ends every other block's barrier wait
+        if (tid == 0) {
+            const unsigned long long t0 = global_ns();
+            unsigned spins = 0;
+            while (!*reinterpret_cast<volatile int*>(&st->gate)) {
+                if (++spins > (1u << 25) || global_ns() - t0 > kBarrierNs) break;
+                __nanosleep(256);
+            }
+            atomicExch(&st->abort, 1);
+        }
+        return;
+    }
     int level = st->level, S = st->S, cur = st->cur;
     int64_t lo = st->lvl_off[level], total = st->total;
     int status = kRefDone, need = 0;
@@ -1237,6 +1254,10 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         t.colleague.alloc(27 * cap, st);
         t.leaf_id.alloc(cap, st);
         t.leaf_node.alloc(cap, st);
+        // SFMM_TREE_TEST_STALL=1: the test of the bounded waits (the build
+        // then fails with FMM_ERR_TIMEOUT after about two seconds)
+        const char* stall_env = std::getenv("SFMM_TREE_TEST_STALL");
+        const int stall_test = stall_env && std::strcmp(stall_env, "1") == 0;
         RefineState h{};
         h.S = S;
         h.total = 1;
@@ -1272,6 +1293,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
             ra.tmax = static_cast<int>(tmax);
             ra.max_level = max_level;
             ra.ppn = max_ppn;
+            ra.stall = stall_test;
             ra.st = dst.ptr;
             SFMM_CUDA(cudaMemcpyAsync(dst.ptr, &h, sizeof(h), cudaMemcpyHostToDevice, st));
             void* params[] = {&ra};

@@ -386,3 +386,26 @@ def test_single_launch_refinement_equals_level_launches(monkeypatch, ctx, dist, 
     for k in a:
         assert np.array_equal(a[k], b[k]), k
     assert np.array_equal(pa, pb) and np.array_equal(fa, fb)
+
+
+def test_refinement_wait_runs_out_and_reports(monkeypatch, ctx):
+    """The single-launch refinement's bounded waits, run out on purpose: with
+    its test switch one block waits on a flag that nothing sets, so the other
+    blocks' grid-barrier waits end through the abort flag.  The build fails
+    with FMM_ERR_TIMEOUT after about two seconds, and the same context then
+    builds the tree as before."""
+    import time
+
+    pos = W.points("plummer", 20000, 7)
+    ref = sf.Tree(pos, 20, 64, ctx=ctx).dump()
+    monkeypatch.setenv("SFMM_TREE_TEST_STALL", "1")
+    t0 = time.perf_counter()
+    with pytest.raises(sf.FMMError) as e:
+        sf.Tree(pos, 20, 64, ctx=ctx)
+    assert e.value.status == 7                      # FMM_ERR_TIMEOUT
+    assert time.perf_counter() - t0 < 30
+    monkeypatch.delenv("SFMM_TREE_TEST_STALL")
+    d = sf.Tree(pos, 20, 64, ctx=ctx).dump()
+    assert d.keys() == ref.keys()
+    for k in ref:
+        assert np.array_equal(d[k], ref[k]), k
