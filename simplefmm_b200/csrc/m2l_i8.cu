@@ -248,34 +248,68 @@ __global__ void __launch_bounds__(kI8FillThreads) k_i8_fill(int64_t nrb, int tpb
 }
 
 // ------------------------------------------------------------------ per evaluation
-// alpha_l = max |M~| / gamma_n over the level's nodes (warp per node and component)
+// Per-block tables of the moment scales, s_l^n (s_l = 2^l / width) and
+// gamma_n, each entry the same expression a per-element evaluation would use.
+struct I8Scales {
+    double pw[kKeyLevel + 1][kI8MaxOrder + 1];    // pow(s_l, n)
+    double sa[kKeyLevel + 1][kI8MaxOrder + 1];    // pow(s_l, n) / gamma_n
+    double gm[kI8MaxOrder + 1];                   // gamma_n
+};
+
+__device__ void fill_scales(const EvalArgs& a, I8Scales& t)
+{
+    const int np = a.p + 1;
+    for (int i = threadIdx.x; i < (a.depth + 1) * np; i += blockDim.x) {
+        const int l = i / np, n = i % np;
+        const double s = double(1 << l) / a.box->width;
+        t.pw[l][n] = pow(s, double(n));
+        t.sa[l][n] = pow(s, double(n)) / i8_gamma(n);
+        if (l == 0) t.gm[n] = i8_gamma(n);
+    }
+    __syncthreads();
+}
+
+// alpha_l = max |M~| / gamma_n over the level's nodes (warp per node and
+// component).  A warp keeps the running maximum of its current (tree, level)
+// and issues one atomic when that changes, not one per node.
 __global__ void k_i8_alpha(EvalArgs a, uint32_t* __restrict__ alpha_bits)
 {
+    __shared__ I8Scales sc;
+    fill_scales(a, sc);
     const int lane = threadIdx.x & 31, qd = a.qdim, T = a.T;
     const int64_t g0 = a.lvl_off[2], g1 = a.lvl_off[a.depth + 1];
     const int64_t rows = (g1 - g0) * qd;
+    int key = -1;
+    float run = 0.f;
     for (int64_t w = (blockIdx.x * int64_t(blockDim.x) + threadIdx.x) >> 5; w < rows; w += (int64_t(gridDim.x) * blockDim.x) >> 5) {
         const int64_t g = g0 + w / qd;
         const int l = level_of(a, g);
-        const double s = double(1 << l) / a.box->width;
         float mx = 0.f;
         for (int t = lane; t < T; t += 32) {
             int n, m;
             tri_nm(t, n, m);
             const cplx v = a.M[(g * qd + w % qd) * T + t];
-            const double sc = pow(s, double(n)) / i8_gamma(n);
-            mx = fmaxf(mx, __double2float_ru(fmax(fabs(v.re), fabs(v.im)) * sc));
+            mx = fmaxf(mx, __double2float_ru(fmax(fabs(v.re), fabs(v.im)) * sc.sa[l][n]));
         }
         for (int o = 16; o; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         const int tr = a.node_tree ? a.node_tree[g] : 0;
-        if (lane == 0 && mx > 0.f) atomicMax(alpha_bits + tr * (kKeyLevel + 2) + l, __float_as_uint(mx));
+        const int k = tr * (kKeyLevel + 2) + l;
+        if (k != key) {
+            if (lane == 0 && key >= 0 && run > 0.f) atomicMax(alpha_bits + key, __float_as_uint(run));
+            key = k;
+            run = 0.f;
+        }
+        run = fmaxf(run, mx);
     }
+    if (lane == 0 && key >= 0 && run > 0.f) atomicMax(alpha_bits + key, __float_as_uint(run));
 }
 
 // moment digits of every node of levels >= 2 (warp per node and component)
 template<int ND>
 __global__ void k_i8_mdigits(EvalArgs a, int KS, const uint32_t* __restrict__ alpha_bits, int8_t* __restrict__ md)
 {
+    __shared__ I8Scales sc;
+    fill_scales(a, sc);
     const int lane = threadIdx.x & 31, qd = a.qdim, T = a.T, p = a.p, KP = 32 * KS;
     const int64_t g0 = a.lvl_off[2], g1 = a.lvl_off[a.depth + 1];
     const int64_t rows = (g1 - g0) * qd;
@@ -285,7 +319,6 @@ __global__ void k_i8_mdigits(EvalArgs a, int KS, const uint32_t* __restrict__ al
         const int l = level_of(a, g);
         const int tr = a.node_tree ? a.node_tree[g] : 0;
         const double al = double(__uint_as_float(alpha_bits[tr * (kKeyLevel + 2) + l]));
-        const double s = double(1 << l) / a.box->width;
         int8_t* dst = md + (g * qd + c) * int64_t(KS) * (32 * ND);
         for (int k = lane; k < KP; k += 32) {
             int8_t d[ND] = {};
@@ -293,7 +326,7 @@ __global__ void k_i8_mdigits(EvalArgs a, int KS, const uint32_t* __restrict__ al
                 int n, m, im;
                 real_nm(k, n, m, im);
                 const cplx v = a.M[(g * qd + c) * T + n * (n + 1) / 2 + m];
-                split_digits<ND>((im ? v.im : v.re) * pow(s, double(n)) / i8_gamma(n) / al, d);
+                split_digits<ND>((im ? v.im : v.re) * sc.pw[l][n] / sc.gm[n] / al, d);
             }
             int8_t* o = dst + (k / 32) * (32 * ND) + (k % 32);
 #pragma unroll
