@@ -51,13 +51,26 @@ __global__ void k_gather_q(const double* __restrict__ Q, const int32_t* __restri
     }
 }
 
-// P2M (fmm.hpp:524-556): warp per leaf of level >= 2, lanes over points,
-// one warp-sum per coefficient.
+// P2M (fmm.hpp:524-556): warp per leaf of level >= 2, lanes over points.
+// The lanes' terms q_b S_n^m go through a per-warp staging block of
+// kP2MStage values: each lane writes its terms, then two lanes per value add
+// the 32 lanes' entries (16 each and one shuffle) into the coefficient.  That
+// is about four instructions per term and lane, against a five-step warp sum.
+constexpr int kP2MStage = 16;                   // values staged per reduction
+constexpr int kP2MLd = 33;                      // doubles per staged value (32 lanes + pad)
+constexpr size_t kP2MStageBytes = size_t(kP2MStage) * kP2MLd * sizeof(double) + kP2MStage * sizeof(int);
+
 __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
 {
     extern __shared__ double smem[];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    cplx* acc = reinterpret_cast<cplx*>(smem) + w * a.qdim * a.T;
+    const size_t per_warp = size_t(a.qdim) * a.T * sizeof(cplx) + kP2MStageBytes;
+    char* wbase = reinterpret_cast<char*>(smem) + w * per_warp;
+    cplx* acc = reinterpret_cast<cplx*>(wbase);
+    double* accd = reinterpret_cast<double*>(wbase);
+    double* stage = reinterpret_cast<double*>(wbase + size_t(a.qdim) * a.T * sizeof(cplx));
+    int* sidx = reinterpret_cast<int*>(stage + kP2MStage * kP2MLd);
+    const int j = lane & 15, h = lane >> 4;
     const int64_t nfar = a.n_leaves - a.far_leaf0;
     for (int64_t f = blockIdx.x * int64_t(nw) + w; f < nfar; f += int64_t(gridDim.x) * nw) {
         const int g = a.leaf_node[a.far_leaf0 + f];
@@ -78,16 +91,36 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
             double q[3] = {0, 0, 0};
             if (on)
                 for (int b = 0; b < a.qdim; ++b) q[b] = a.qs[b * a.n + i];
+            int cnt = 0;                                  // staged values (the same in every lane)
+            auto flush = [&](int nv) {
+                __syncwarp();
+                double sum = 0.0;
+                if (j < nv) {
+                    const double* col = stage + j * kP2MLd + h * 16;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) sum += col[u];
+                }
+                sum += __shfl_xor_sync(0xffffffffu, sum, 16);
+                if (h == 0 && j < nv) accd[sidx[j]] += sum;
+                __syncwarp();
+            };
             for_each_harmonic(a.p, x, y, z, c_harm, [&](int n, int m, cplx s) {
                 const int t = tri(n, m);
                 for (int b = 0; b < a.qdim; ++b) {
-                    const double re = warp_sum(q[b] * s.re), im = warp_sum(q[b] * s.im);
+                    stage[cnt * kP2MLd + lane] = q[b] * s.re;
+                    stage[(cnt + 1) * kP2MLd + lane] = q[b] * s.im;
                     if (lane == 0) {
-                        acc[b * a.T + t].re += re;
-                        acc[b * a.T + t].im += im;
+                        sidx[cnt] = 2 * (b * a.T + t);
+                        sidx[cnt + 1] = 2 * (b * a.T + t) + 1;
+                    }
+                    cnt += 2;
+                    if (cnt == kP2MStage) {
+                        flush(kP2MStage);
+                        cnt = 0;
                     }
                 }
             });
+            if (cnt) flush(cnt);
         }
         __syncwarp();
         cplx* M = a.M + int64_t(g) * a.qdim * a.T;
@@ -558,7 +591,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field, cudaEv
     const bool far = t.depth >= 2;
     if (far) {
         const int64_t nfar = t.n_leaves - a.far_leaf0;
-        const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx);
+        const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx) + kP2MStageBytes;
         const int w_p2m = warps_for(0, sm_p2m_w);
         allow_smem(k_p2m, sm_p2m_w * w_p2m);
         k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
@@ -683,7 +716,7 @@ void plan_evaluate_stage(Plan& pl, const double* Q, double* pot, double* field, 
         launch_p2p(a, sms, side);
         SFMM_CUDA(cudaEventRecord(pl.join, side));
         if (far) {
-            const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx);
+            const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx) + kP2MStageBytes;
             const int w_p2m = warps_for(0, sm_p2m_w);
             allow_smem(k_p2m, sm_p2m_w * w_p2m);
             k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
