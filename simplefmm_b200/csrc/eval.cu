@@ -227,6 +227,7 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_l2l(EvalArgs a, int lc, int6
 // locals (potential: LA; field: minus grad of LB for scalar charges, curl
 // of LB for vector charges) are formed in shared memory, then lanes
 // evaluate them at the leaf's points.
+template<int KM>
 __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
 {
     extern __shared__ double smem[];
@@ -262,15 +263,18 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_l2p(EvalArgs a)
         __syncwarp();
         const int b0 = a.pbeg[g], b1 = a.pend[g];
         for (int i = b0 + lane; i < b1; i += 32) {
-            double u[6] = {0, 0, 0, 0, 0, 0};
+            // KM = K, a compile-time bound: the sums stay in registers
+            double u[KM];
+#pragma unroll
+            for (int k = 0; k < KM; ++k) u[k] = 0.0;
             for_each_harmonic(a.p, a.fx[i] - c[0], a.fy[i] - c[1], a.fz[i] - c[2], c_harm, [&](int n, int m, cplx s) {
                 const int t = tri(n, m);
                 const double wt = m == 0 ? 1.0 : 2.0;
 #pragma unroll
-                for (int k = 0; k < 6; ++k)
-                    if (k < K) u[k] += wt * (loc[k * T + t].re * s.re + loc[k * T + t].im * s.im);
+                for (int k = 0; k < KM; ++k) u[k] += wt * (loc[k * T + t].re * s.re + loc[k * T + t].im * s.im);
             });
-            for (int k = 0; k < K; ++k) a.out[int64_t(k) * a.n + i] += u[k];
+#pragma unroll
+            for (int k = 0; k < KM; ++k) a.out[int64_t(k) * a.n + i] += u[k];
         }
         __syncwarp();
     }
@@ -304,6 +308,26 @@ void allow_smem(KernelT k, size_t smem)
 {
     SFMM_REQUIRE(smem <= g_smem_optin, FMM_ERR_UNSUPPORTED, "kernel working set exceeds shared memory");
     allow_max_smem(k);
+}
+
+template<int KM>
+void launch_l2p_k(const EvalArgs& a, int64_t nfar, int w, size_t smem, cudaStream_t st)
+{
+    allow_smem(k_l2p<KM>, smem);
+    k_l2p<KM><<<blocks_for(nfar, w, 65535), w * 32, smem, st>>>(a);
+}
+
+// L2P for K output components: qdim (potential) + 3 (field), so 1, 3, 4 or 6
+void launch_l2p(const EvalArgs& a, int K, int64_t nfar, int w, size_t smem, cudaStream_t st)
+{
+    switch (K) {
+    case 1: launch_l2p_k<1>(a, nfar, w, smem, st); break;
+    case 3: launch_l2p_k<3>(a, nfar, w, smem, st); break;
+    case 4: launch_l2p_k<4>(a, nfar, w, smem, st); break;
+    case 6: launch_l2p_k<6>(a, nfar, w, smem, st); break;
+    default: SFMM_REQUIRE(false, FMM_ERR_UNSUPPORTED, "L2P: unexpected number of output components");
+    }
+    SFMM_CHECK_LAUNCH();
 }
 
 }  // namespace
@@ -630,9 +654,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field, cudaEv
         }
         const size_t sm_l2p_w = size_t(K) * T * sizeof(cplx);
         const int w_l2p = warps_for(0, sm_l2p_w);
-        allow_smem(k_l2p, sm_l2p_w * w_l2p);
-        k_l2p<<<blocks_for(nfar, w_l2p, 65535), w_l2p * 32, sm_l2p_w * w_l2p, st>>>(a);
-        SFMM_CHECK_LAUNCH();
+        launch_l2p(a, K, nfar, w_l2p, sm_l2p_w * w_l2p, st);
     } else {
         SFMM_CUDA(cudaEventRecord(pl.ev[1], st));
         near_field();
@@ -767,9 +789,7 @@ void plan_evaluate_stage(Plan& pl, const double* Q, double* pot, double* field, 
         }
         const size_t sm_l2p_w = size_t(K) * T * sizeof(cplx);
         const int w_l2p = warps_for(0, sm_l2p_w);
-        allow_smem(k_l2p, sm_l2p_w * w_l2p);
-        k_l2p<<<blocks_for(nfar, w_l2p, 65535), w_l2p * 32, sm_l2p_w * w_l2p, st>>>(a);
-        SFMM_CHECK_LAUNCH();
+        launch_l2p(a, K, nfar, w_l2p, sm_l2p_w * w_l2p, st);
     }
     SFMM_CUDA(cudaStreamWaitEvent(st, pl.join, 0));
     k_finalize<<<blocks_for(t.n, 256, 8192), 256, 0, st>>>(a, pot, field);
