@@ -60,6 +60,7 @@ constexpr int kP2MStage = 16;                   // values staged per reduction
 constexpr int kP2MLd = 33;                      // doubles per staged value (32 lanes + pad)
 constexpr size_t kP2MStageBytes = size_t(kP2MStage) * kP2MLd * sizeof(double) + kP2MStage * sizeof(int);
 
+template<int QD>
 __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
 {
     extern __shared__ double smem[];
@@ -88,9 +89,9 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
             const int i = base + lane;
             const bool on = i < b1;
             const double x = on ? a.fx[i] - c[0] : 0, y = on ? a.fy[i] - c[1] : 0, z = on ? a.fz[i] - c[2] : 0;
-            double q[3] = {0, 0, 0};
-            if (on)
-                for (int b = 0; b < a.qdim; ++b) q[b] = a.qs[b * a.n + i];
+            double q[QD];                                 // QD = qdim: the charges stay in registers
+#pragma unroll
+            for (int b = 0; b < QD; ++b) q[b] = on ? a.qs[b * a.n + i] : 0.0;
             int cnt = 0;                                  // staged values (the same in every lane)
             auto flush = [&](int nv) {
                 __syncwarp();
@@ -106,7 +107,8 @@ __global__ void __launch_bounds__(kMaxWarps * 32) k_p2m(EvalArgs a)
             };
             for_each_harmonic(a.p, x, y, z, c_harm, [&](int n, int m, cplx s) {
                 const int t = tri(n, m);
-                for (int b = 0; b < a.qdim; ++b) {
+#pragma unroll
+                for (int b = 0; b < QD; ++b) {
                     stage[cnt * kP2MLd + lane] = q[b] * s.re;
                     stage[(cnt + 1) * kP2MLd + lane] = q[b] * s.im;
                     if (lane == 0) {
@@ -310,6 +312,27 @@ void allow_smem(KernelT k, size_t smem)
     allow_max_smem(k);
 }
 
+// P2M for one, two or three charge components
+void launch_p2m(const EvalArgs& a, int64_t nfar, int w, size_t smem, cudaStream_t st)
+{
+    switch (a.qdim) {
+    case 1:
+        allow_smem(k_p2m<1>, smem);
+        k_p2m<1><<<blocks_for(nfar, w, 65535), w * 32, smem, st>>>(a);
+        break;
+    case 2:
+        allow_smem(k_p2m<2>, smem);
+        k_p2m<2><<<blocks_for(nfar, w, 65535), w * 32, smem, st>>>(a);
+        break;
+    case 3:
+        allow_smem(k_p2m<3>, smem);
+        k_p2m<3><<<blocks_for(nfar, w, 65535), w * 32, smem, st>>>(a);
+        break;
+    default: SFMM_REQUIRE(false, FMM_ERR_UNSUPPORTED, "P2M: charges have 1, 2 or 3 components");
+    }
+    SFMM_CHECK_LAUNCH();
+}
+
 template<int KM>
 void launch_l2p_k(const EvalArgs& a, int64_t nfar, int w, size_t smem, cudaStream_t st)
 {
@@ -317,11 +340,13 @@ void launch_l2p_k(const EvalArgs& a, int64_t nfar, int w, size_t smem, cudaStrea
     k_l2p<KM><<<blocks_for(nfar, w, 65535), w * 32, smem, st>>>(a);
 }
 
-// L2P for K output components: qdim (potential) + 3 (field), so 1, 3, 4 or 6
+// L2P for K output components: qdim (potential) + 3 (field, qdim 1 or 3),
+// so 1, 2, 3, 4 or 6
 void launch_l2p(const EvalArgs& a, int K, int64_t nfar, int w, size_t smem, cudaStream_t st)
 {
     switch (K) {
     case 1: launch_l2p_k<1>(a, nfar, w, smem, st); break;
+    case 2: launch_l2p_k<2>(a, nfar, w, smem, st); break;
     case 3: launch_l2p_k<3>(a, nfar, w, smem, st); break;
     case 4: launch_l2p_k<4>(a, nfar, w, smem, st); break;
     case 6: launch_l2p_k<6>(a, nfar, w, smem, st); break;
@@ -617,9 +642,7 @@ void plan_evaluate(Plan& pl, const double* Q, double* pot, double* field, cudaEv
         const int64_t nfar = t.n_leaves - a.far_leaf0;
         const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx) + kP2MStageBytes;
         const int w_p2m = warps_for(0, sm_p2m_w);
-        allow_smem(k_p2m, sm_p2m_w * w_p2m);
-        k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
-        SFMM_CHECK_LAUNCH();
+        launch_p2m(a, nfar, w_p2m, sm_p2m_w * w_p2m, st);
         const size_t head = (32 + 2 * 4 * (2 * kMaxOrder + 1)) * sizeof(double);
         const size_t sm_m2m_w = 2 * size_t(qd) * T * sizeof(cplx);
         const int w_m2m = warps_for(head, sm_m2m_w);
@@ -740,9 +763,7 @@ void plan_evaluate_stage(Plan& pl, const double* Q, double* pot, double* field, 
         if (far) {
             const size_t sm_p2m_w = size_t(qd) * T * sizeof(cplx) + kP2MStageBytes;
             const int w_p2m = warps_for(0, sm_p2m_w);
-            allow_smem(k_p2m, sm_p2m_w * w_p2m);
-            k_p2m<<<blocks_for(nfar, w_p2m, 65535), w_p2m * 32, sm_p2m_w * w_p2m, st>>>(a);
-            SFMM_CHECK_LAUNCH();
+            launch_p2m(a, nfar, w_p2m, sm_p2m_w * w_p2m, st);
         }
         return;
     }

@@ -409,3 +409,19 @@ def test_refinement_wait_runs_out_and_reports(monkeypatch, ctx):
     assert d.keys() == ref.keys()
     for k in ref:
         assert np.array_equal(d[k], ref[k]), k
+
+
+def test_two_component_charges_equal_two_single_solves(ctx):
+    """N = 2 charges (potential only, as FMM3D<double, 2>::rinv gives): each
+    output component equals the solve of that component's charges alone, to
+    FP64 rounding (the M2L tiles group columns differently)."""
+    n = 20000
+    pos = W.points("plummer", n, 11)
+    q2 = np.ascontiguousarray(np.stack([W.charges(n, 11), W.charges(n, 12)], axis=1))
+    t = sf.Tree(pos, 20, 64, ctx=ctx)
+    u2 = np.zeros((n, 2))
+    sf.Plan(t, 8, 2).rinv(q2, u2)
+    for b in range(2):
+        u1 = np.zeros(n)
+        sf.Plan(t, 8, 1).rinv(np.ascontiguousarray(q2[:, b]), u1)
+        assert np.max(np.abs(u2[:, b] - u1)) <= 1e-12 * np.max(np.abs(u1)), b
