@@ -214,6 +214,7 @@ __global__ void __launch_bounds__(kI8FillThreads) k_i8_fill(int64_t nrb, int tpb
                                                            int32_t* __restrict__ nused)
 {
     extern __shared__ int32_t tab[];                     // [216][tpb]
+    __shared__ int slot_on[kI8Slots];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = kI8FillThreads / 32;
     for (int64_t rb = blockIdx.x; rb < nrb; rb += gridDim.x) {
         const int info = rb_info[rb];
@@ -231,15 +232,23 @@ __global__ void __launch_bounds__(kI8FillThreads) k_i8_fill(int64_t nrb, int tpb
         }
         __syncthreads();
         for (int e = threadIdx.x; e < kI8Slots * tpb; e += kI8FillThreads) slot_src[rb * kI8Slots * tpb + e] = tab[e];
+        // the slots that occur: a flag per slot (warps over slots), then warp 0
+        // lists them in slot order (ballot + prefix)
+        for (int sl = warp; sl < kI8Slots; sl += nw) {
+            bool any = false;
+            for (int t = lane; t < ntg; t += 32) any |= tab[sl * tpb + t] >= 0;
+            const bool occ = __any_sync(0xffffffffu, any);
+            if (lane == 0) slot_on[sl] = occ;
+        }
+        __syncthreads();
         if (warp == 0) {
             int cnt = 0;
-            for (int sl = 0; sl < kI8Slots; ++sl) {
-                bool any = false;
-                for (int t = lane; t < ntg; t += 32) any |= tab[sl * tpb + t] >= 0;
-                if (__any_sync(0xffffffffu, any)) {
-                    if (lane == 0) used[rb * kI8Slots + cnt] = sl;
-                    ++cnt;
-                }
+            for (int s0 = 0; s0 < kI8Slots; s0 += 32) {
+                const int sl = s0 + lane;
+                const bool occ = sl < kI8Slots && slot_on[sl];
+                const unsigned m = __ballot_sync(0xffffffffu, occ);
+                if (occ) used[rb * kI8Slots + cnt + __popc(m & ((1u << lane) - 1u))] = sl;
+                cnt += __popc(m);
             }
             if (lane == 0) nused[rb] = cnt;
         }
