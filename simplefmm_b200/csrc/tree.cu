@@ -78,15 +78,39 @@ __global__ void k_minmax(const double* __restrict__ xyz, int64_t n, BoxDev b, do
     }
 }
 
-// box.hpp:96-106 evaluated with the same double operations.
-__global__ void k_box_final(const double* __restrict__ partial, int nb, BoxDev b, BoxDev* out)
+// box.hpp:96-106 evaluated with the same double operations, after the block
+// partials are reduced by the whole block (min / max: exact in any order).
+constexpr int kBoxFinalThreads = 256;
+__global__ void __launch_bounds__(kBoxFinalThreads) k_box_final(const double* __restrict__ partial, int nb, BoxDev b,
+                                                                BoxDev* out)
 {
-    if (threadIdx.x != 0) return;
     double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    for (int k = 0; k < nb; ++k)
+    for (int k = threadIdx.x; k < nb; k += blockDim.x)
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
             lo[a] = fmin(lo[a], partial[6 * k + a]);
             hi[a] = fmax(hi[a], partial[6 * k + 3 + a]);
+        }
+    __shared__ double s[6][kBoxFinalThreads / 32];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], o));
+            hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], o));
+        }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) {
+            s[a][w] = lo[a];
+            s[3 + a][w] = hi[a];
+        }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int k = 1; k < static_cast<int>(blockDim.x >> 5); ++k)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = fmin(lo[a], s[a][k]);
+            hi[a] = fmax(hi[a], s[3 + a][k]);
         }
     double dl[3], c[3];
     for (int a = 0; a < 3; ++a) {
@@ -1161,7 +1185,7 @@ void build_tree(Tree& t, const double* xyz, int max_level, int max_ppn, int vert
         t.d_box.alloc(1, st);
         k_minmax<<<nb, 256, 0, st>>>(xyz, n, b, partial.ptr);
         SFMM_CHECK_LAUNCH();
-        k_box_final<<<1, 32, 0, st>>>(partial.ptr, nb, b, t.d_box.ptr);
+        k_box_final<<<1, kBoxFinalThreads, 0, st>>>(partial.ptr, nb, b, t.d_box.ptr);
         SFMM_CHECK_LAUNCH();
     }
 
