@@ -1107,7 +1107,8 @@ T read_one(const T* d, cudaStream_t s)
     return v;
 }
 
-// Two device values read back with one synchronisation.
+// Two device values read back together: the stream drains once, for the first
+// copy; the second follows it directly.
 template<typename T>
 void read_two(const T* d0, const T* d1, T& v0, T& v1, cudaStream_t s)
 {
